@@ -1,0 +1,250 @@
+// The flat C bridge declared in include/bh_b200.h.
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include <bh_b200.h>
+#include <bohrium/bh_component.hpp>
+#include <bohrium/bh_main_memory.hpp>
+
+using namespace std;
+using namespace bohrium;
+
+namespace {
+thread_local string g_last_error;
+
+template <typename F>
+int guarded(F &&f) {
+    try {
+        f();
+        g_last_error.clear();
+        return 0;
+    } catch (const std::exception &e) {
+        g_last_error = e.what();
+    } catch (...) {
+        g_last_error = "unknown error";
+    }
+    return -1;
+}
+} // namespace
+
+struct bhb_runtime {
+    unique_ptr<ConfigParser> config;
+    component::ComponentFace child;
+    string message;
+};
+
+struct bhb_ir {
+    unique_ptr<BhIR> ir;
+};
+
+namespace {
+BhIR *decode(const int64_t *w, int64_t n, bh_base *const *syncs, int64_t nsyncs, uint64_t nrepeats, bh_base *cond,
+             const int64_t *slides, int64_t nslide) {
+    vector<bh_instruction> list;
+    int64_t i = 0;
+    auto need = [&](int64_t k) {
+        if (i + k > n) throw runtime_error("bhb: truncated instruction encoding");
+    };
+    while (i < n) {
+        need(5);
+        bh_instruction instr;
+        instr.opcode = w[i];
+        const int64_t nop = w[i + 1];
+        const int64_t ctype = w[i + 2];
+        if (nop < 0 || nop > 8) throw runtime_error("bhb: bad operand count");
+        if (ctype >= 0) {
+            if (ctype >= BH_NUM_TYPES) throw runtime_error("bhb: bad constant type");
+            instr.constant.type = static_cast<bh_type>(ctype);
+            memcpy(&instr.constant.value, &w[i + 3], 16);
+        } else {
+            instr.constant.type = bh_type::BOOL;
+            memset(&instr.constant.value, 0, 16);
+        }
+        i += 5;
+        for (int64_t o = 0; o < nop; ++o) {
+            need(1);
+            bh_view v;
+            v.base = reinterpret_cast<bh_base *>(w[i++]);
+            if (v.base != nullptr) {
+                need(2);
+                v.start = w[i];
+                v.ndim = w[i + 1];
+                i += 2;
+                if (v.ndim < 0 || v.ndim > BH_MAXDIM) throw runtime_error("bhb: bad ndim");
+                need(2 * v.ndim);
+                v.shape.resize(static_cast<size_t>(v.ndim));
+                v.stride.resize(static_cast<size_t>(v.ndim));
+                for (int64_t d = 0; d < v.ndim; ++d) v.shape[d] = w[i + d];
+                for (int64_t d = 0; d < v.ndim; ++d) v.stride[d] = w[i + v.ndim + d];
+                i += 2 * v.ndim;
+            }
+            instr.operand.push_back(v);
+        }
+        if (instr.opcode <= BH_MAX_OPCODE_ID) {
+            const int expect = bh_opcode_nop(instr.opcode);
+            if (expect < 0) throw runtime_error("bhb: unknown opcode " + to_string(instr.opcode));
+            if (expect != static_cast<int>(nop))
+                throw runtime_error(string("bhb: ") + bh_opcode_text(instr.opcode) + " expects " + to_string(expect) +
+                                    " operands");
+        }
+        list.push_back(std::move(instr));
+    }
+    // Sliding views
+    int64_t j = 0;
+    while (j < nslide) {
+        const int64_t ii = slides[j], oo = slides[j + 1], nd = slides[j + 2];
+        j += 3;
+        if (ii < 0 || ii >= static_cast<int64_t>(list.size()) || oo < 0 ||
+            oo >= static_cast<int64_t>(list[ii].operand.size()))
+            throw runtime_error("bhb: bad slide target");
+        bh_view &v = list[ii].operand[oo];
+        for (int64_t d = 0; d < nd; ++d) {
+            bh_slide_dim sd{slides[j], slides[j + 1], slides[j + 2], slides[j + 3], slides[j + 4], slides[j + 5]};
+            v.slides.dims.push_back(sd);
+            j += 6;
+        }
+        const int64_t nr = slides[j++];
+        for (int64_t r = 0; r < nr; ++r) {
+            v.slides.resets[slides[j]] = make_pair(slides[j + 1], int64_t{0});
+            j += 2;
+        }
+    }
+    set<bh_base *> s(syncs, syncs + nsyncs);
+    return new BhIR(std::move(list), std::move(s), nrepeats, cond);
+}
+} // namespace
+
+extern "C" {
+
+const char *bhb_last_error(void) { return g_last_error.c_str(); }
+
+bhb_runtime *bhb_runtime_create(const char *config_path, const char *stack_name) {
+    bhb_runtime *rt = nullptr;
+    guarded([&] {
+        // Components below the bridge locate the config themselves, as in the reference.
+        if (config_path && config_path[0]) setenv("BH_CONFIG", config_path, 1);
+        if (stack_name && stack_name[0]) setenv("BH_STACK", stack_name, 1);
+        unique_ptr<bhb_runtime> r(new bhb_runtime());
+        r->config.reset(new ConfigParser(-1));
+        const string child = r->config->getChildLibraryPath();
+        if (child.empty()) throw runtime_error("bhb_runtime_create: the stack is empty");
+        r->child = component::ComponentFace(child, 0);
+        rt = r.release();
+    });
+    return rt;
+}
+
+void bhb_runtime_destroy(bhb_runtime *rt) {
+    guarded([&] { delete rt; });
+}
+
+bh_base *bhb_base_create(int dtype, int64_t nelem) {
+    bh_base *b = nullptr;
+    guarded([&] {
+        if (dtype < 0 || dtype >= BH_NUM_TYPES) throw runtime_error("bhb_base_create: bad dtype");
+        if (nelem < 0) throw runtime_error("bhb_base_create: negative size");
+        b = new bh_base(nelem, static_cast<bh_type>(dtype));
+    });
+    return b;
+}
+
+void bhb_base_destroy(bh_base *base) { delete base; }
+int bhb_base_dtype(const bh_base *base) { return static_cast<int>(base->dtype()); }
+int64_t bhb_base_nelem(const bh_base *base) { return base->nelem(); }
+
+void *bhb_data_get(bhb_runtime *rt, bh_base *base, int copy2host, int force_alloc, int nullify) {
+    void *ret = nullptr;
+    guarded([&] { ret = rt->child.getMemoryPointer(*base, copy2host != 0, force_alloc != 0, nullify != 0); });
+    return ret;
+}
+
+int bhb_data_set(bhb_runtime *rt, bh_base *base, int host_ptr, void *data) {
+    return guarded([&] { rt->child.setMemoryPointer(base, host_ptr != 0, data); });
+}
+
+void *bhb_host_alloc(bhb_runtime *rt, int64_t nbytes) {
+    void *ret = nullptr;
+    guarded([&] {
+        const string r = rt->child.message("host_alloc " + to_string(nbytes));
+        ret = reinterpret_cast<void *>(strtoull(r.c_str(), nullptr, 10));
+        if (ret == nullptr) ret = malloc(static_cast<size_t>(nbytes));
+        if (ret == nullptr) throw bad_alloc();
+    });
+    return ret;
+}
+
+int bhb_data_copy_in(bhb_runtime *rt, bh_base *base, const void *src, int64_t nbytes) {
+    return guarded([&] {
+        if (nbytes != base->nbytes()) throw runtime_error("bhb_data_copy_in: size mismatch");
+        void *p = rt->child.getMemoryPointer(*base, true, true, false);
+        if (nbytes > 0) memcpy(p, src, static_cast<size_t>(nbytes));
+    });
+}
+
+bhb_ir *bhb_ir_create(const int64_t *words, int64_t nwords, bh_base *const *syncs, int64_t nsyncs, uint64_t nrepeats,
+                      bh_base *repeat_condition, const int64_t *slides, int64_t nslide_words) {
+    bhb_ir *ret = nullptr;
+    guarded([&] {
+        unique_ptr<bhb_ir> r(new bhb_ir());
+        r->ir.reset(decode(words, nwords, syncs, nsyncs, nrepeats, repeat_condition, slides, nslide_words));
+        ret = r.release();
+    });
+    return ret;
+}
+
+void bhb_ir_destroy(bhb_ir *ir) { delete ir; }
+
+int bhb_ir_execute(bhb_runtime *rt, bhb_ir *ir) {
+    return guarded([&] { rt->child.execute(ir->ir.get()); });
+}
+
+int bhb_execute(bhb_runtime *rt, const int64_t *words, int64_t nwords, bh_base *const *syncs, int64_t nsyncs,
+                uint64_t nrepeats, bh_base *repeat_condition, const int64_t *slides, int64_t nslide_words) {
+    return guarded([&] {
+        unique_ptr<BhIR> ir(decode(words, nwords, syncs, nsyncs, nrepeats, repeat_condition, slides, nslide_words));
+        rt->child.execute(ir.get());
+    });
+}
+
+const char *bhb_message(bhb_runtime *rt, const char *msg) {
+    const int r = guarded([&] { rt->message = rt->child.message(msg); });
+    return r == 0 ? rt->message.c_str() : nullptr;
+}
+
+int bhb_extmethod(bhb_runtime *rt, const char *name, int64_t opcode) {
+    return guarded([&] {
+        if (opcode <= BH_MAX_OPCODE_ID) throw runtime_error("bhb_extmethod: opcode must be > BH_MAX_OPCODE_ID");
+        rt->child.extmethod(name, opcode);
+    });
+}
+
+void *bhb_get_device_context(bhb_runtime *rt) {
+    void *r = nullptr;
+    guarded([&] { r = rt->child.getDeviceContext(); });
+    return r;
+}
+
+int bhb_set_device_context(bhb_runtime *rt, void *ctx) {
+    return guarded([&] { rt->child.setDeviceContext(ctx); });
+}
+
+double bhb_last_execute_ms(bhb_runtime *rt) {
+    double ms = 0;
+    guarded([&] {
+        const string r = rt->child.message("CUDA: last execute ms");
+        ms = r.empty() ? 0.0 : strtod(r.c_str(), nullptr);
+    });
+    return ms;
+}
+
+} // extern "C"
+
+// Access to the decoded BhIR of a bhb_ir handle (used by in-tree components' test hooks).
+extern "C" void *bhb_ir_bhir(bhb_ir *ir) { return ir ? static_cast<void *>(ir->ir.get()) : nullptr; }
+extern "C" void bhb_set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+
+// Host data pointer of a base (valid after a sync; NULL when the base has no host storage).
+extern "C" void *bhb_base_data(const bh_base *base) { return const_cast<void *>(base->getDataPtr()); }

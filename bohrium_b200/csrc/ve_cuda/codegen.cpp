@@ -1,0 +1,1074 @@
+// Kernel source generation; see codegen.hpp for the schedules.
+//
+// Operation semantics (one C statement per bytecode, NumPy rules for signed integer division and
+// remainder, reductions as `acc = acc op x`, accumulates as `out[i] = out[i-1] op in[i]`) follow
+// core/jitk/instruction.cpp:58-544 of the reference; temporaries and scalar replacement of
+// reduction outputs follow core/jitk/engines/engine.cpp:84-249.
+#include <algorithm>
+#include <cassert>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <set>
+#include <sstream>
+#include <stdexcept>
+#include "codegen.hpp"
+
+using namespace std;
+using bohrium::jitk::Block;
+using bohrium::jitk::InstrPtr;
+using bohrium::jitk::LoopB;
+
+namespace bohrium {
+namespace cuda {
+
+const char *sched_name(Sched s) {
+    switch (s) {
+        case Sched::FLAT: return "flat";
+        case Sched::GRID_REDUCE: return "grid_reduce";
+        case Sched::OUTER_REDUCE: return "outer_reduce";
+        case Sched::SCAN1D: return "scan1d";
+        case Sched::SERIAL: return "serial";
+    }
+    return "?";
+}
+
+int64_t LaunchUnit::work_items() const {
+    switch (sched) {
+        case Sched::FLAT: {
+            const int64_t per = static_cast<int64_t>(kThreads) * V;
+            return rows * ((cols + per - 1) / per);
+        }
+        case Sched::GRID_REDUCE: return (cols + kReduceTile - 1) / kReduceTile;
+        case Sched::OUTER_REDUCE: return (rows * cols + kThreads - 1) / kThreads;
+        case Sched::SCAN1D: return (cols + kScanChunk - 1) / kScanChunk;
+        case Sched::SERIAL: return 1;
+    }
+    return 1;
+}
+
+string cuda_type(bh_type t) {
+    switch (t) {
+        case bh_type::BOOL: return "bool";
+        case bh_type::INT8: return "signed char";
+        case bh_type::INT16: return "short";
+        case bh_type::INT32: return "int";
+        case bh_type::INT64: return "long long";
+        case bh_type::UINT8: return "unsigned char";
+        case bh_type::UINT16: return "unsigned short";
+        case bh_type::UINT32: return "unsigned int";
+        case bh_type::UINT64: return "unsigned long long";
+        case bh_type::FLOAT32: return "float";
+        case bh_type::FLOAT64: return "double";
+        case bh_type::COMPLEX64: return "bh_c64";
+        case bh_type::COMPLEX128: return "bh_c128";
+        case bh_type::R123: return "bh_r123";
+    }
+    throw runtime_error("cuda_type(): unknown type");
+}
+
+namespace {
+
+// ------------------------------------------------------------------------------- kernel prelude
+// Common device helpers: Philox2x32-10 (the counter-based generator behind BH_RANDOM, restated
+// from Salmon et al., "Parallel Random Numbers: As Easy as 1, 2, 3", SC'11: ten rounds of
+// (hi, lo) = M * x0; x0' = hi ^ k ^ x1; x1' = lo with the key bumped by W between rounds), warp
+// shuffles for every element type and a small complex type.
+const char *kPrelude = R"CUDA(
+typedef long long bh_i64;
+typedef unsigned long long bh_u64;
+struct bh_r123 { bh_u64 start, key; };
+struct bh_c64 { float re, im; };
+struct bh_c128 { double re, im; };
+
+__device__ __forceinline__ bh_u64 bh_random123(bh_u64 start, bh_u64 key, bh_u64 index) {
+    const bh_u64 c = start + index;
+    unsigned x0 = (unsigned)c, x1 = (unsigned)(c >> 32), k = (unsigned)key;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const unsigned hi = __umulhi(0xD256D193u, x0);
+        const unsigned lo = 0xD256D193u * x0;
+        x0 = hi ^ k ^ x1;
+        x1 = lo;
+        k += 0x9E3779B9u;
+    }
+    return ((bh_u64)x1 << 32) | (bh_u64)x0;
+}
+
+template <typename T> __device__ __forceinline__ T bh_shfl_xor(T v, int m) {
+    if (sizeof(T) == 8) {
+        long long x; memcpy(&x, &v, 8);
+        x = __shfl_xor_sync(0xffffffffu, x, m);
+        T r; memcpy(&r, &x, 8); return r;
+    } else {
+        int x = 0; memcpy(&x, &v, sizeof(T));
+        x = __shfl_xor_sync(0xffffffffu, x, m);
+        T r; memcpy(&r, &x, sizeof(T)); return r;
+    }
+}
+
+__device__ __forceinline__ bh_i64 bh_floordiv_i64(bh_i64 a, bh_i64 b) { return a / b; }
+)CUDA";
+
+// ---------------------------------------------------------------------------- operation emitting
+bool is_float(bh_type t) { return t == bh_type::FLOAT32 || t == bh_type::FLOAT64; }
+
+// Name of a math function for element type `t` (float uses the f-suffixed variant, as C's
+// <tgmath.h> does for the reference's generated C code).
+string fn(const char *name, bh_type t) { return t == bh_type::FLOAT32 ? string(name) + "f" : string(name); }
+
+string sign_expr(const string &x) { return "((" + x + " > 0) - (0 > " + x + "))"; }
+
+// The combine expression of a reduction: `acc op x`.
+string reduce_expr(bh_opcode op, const string &acc, const string &x) {
+    switch (op) {
+        case BH_ADD_REDUCE: return acc + " + " + x;
+        case BH_MULTIPLY_REDUCE: return acc + " * " + x;
+        case BH_MINIMUM_REDUCE: return acc + " < " + x + " ? " + acc + " : " + x;
+        case BH_MAXIMUM_REDUCE: return acc + " > " + x + " ? " + acc + " : " + x;
+        case BH_LOGICAL_AND_REDUCE: return acc + " && " + x;
+        case BH_LOGICAL_OR_REDUCE: return acc + " || " + x;
+        case BH_LOGICAL_XOR_REDUCE: return "!" + acc + " != !" + x;
+        case BH_BITWISE_AND_REDUCE: return acc + " & " + x;
+        case BH_BITWISE_OR_REDUCE: return acc + " | " + x;
+        case BH_BITWISE_XOR_REDUCE: return acc + " ^ " + x;
+        default: throw runtime_error(string("reduce_expr(): not a reduction: ") + bh_opcode_text(op));
+    }
+}
+
+// One statement computing `instr` given its operand expressions (ops[0] is the output lvalue).
+string op_statement(const bh_instruction &instr, const vector<string> &ops) {
+    const bh_opcode op = instr.opcode;
+    const bh_type t0 = instr.operand_type(0);
+    const bh_type t1 = instr.operand.size() > 1 ? instr.operand_type(1) : t0;
+    for (size_t i = 0; i < instr.operand.size(); ++i)
+        if (bh_type_is_complex(instr.operand_type(static_cast<int>(i))))
+            throw runtime_error(string("complex element types are not supported by the CUDA engine: ") +
+                                bh_opcode_text(op));
+    const string &o = ops[0];
+    auto un = [&](const char *f) { return o + " = " + fn(f, t1) + "(" + ops[1] + ");"; };
+    auto bin = [&](const char *sym) { return o + " = " + ops[1] + " " + sym + " " + ops[2] + ";"; };
+    if (bh_opcode_is_reduction(op)) return o + " = " + reduce_expr(op, o, ops[1]) + ";";
+    switch (op) {
+        case BH_ADD: return bin("+");
+        case BH_SUBTRACT: return bin("-");
+        case BH_MULTIPLY: return bin("*");
+        case BH_DIVIDE:
+            if (bh_type_is_signed_integer(t0)) {
+                const string &a = ops[1], &b = ops[2];
+                return o + " = ((" + a + " > 0) != (" + b + " > 0) && (" + a + " % " + b + ") != 0) ? (" + a +
+                       " / " + b + " - 1) : (" + a + " / " + b + ");";
+            }
+            return bin("/");
+        case BH_POWER:
+            if (bh_type_is_integer(t0) || t0 == bh_type::BOOL)
+                return o + " = pow((double)" + ops[1] + ", (double)" + ops[2] + ");";
+            return o + " = " + fn("pow", t0) + "(" + ops[1] + ", " + ops[2] + ");";
+        case BH_ABSOLUTE:
+            if (t1 == bh_type::BOOL || bh_type_is_unsigned_integer(t1)) return o + " = " + ops[1] + ";";
+            if (is_float(t1)) return un("fabs");
+            if (t1 == bh_type::INT64) return o + " = llabs(" + ops[1] + ");";
+            return o + " = abs((int)" + ops[1] + ");";
+        case BH_GREATER: return bin(">");
+        case BH_GREATER_EQUAL: return bin(">=");
+        case BH_LESS: return bin("<");
+        case BH_LESS_EQUAL: return bin("<=");
+        case BH_EQUAL: return bin("==");
+        case BH_NOT_EQUAL: return bin("!=");
+        case BH_LOGICAL_AND: return bin("&&");
+        case BH_LOGICAL_OR: return bin("||");
+        case BH_LOGICAL_XOR: return o + " = !" + ops[1] + " != !" + ops[2] + ";";
+        case BH_LOGICAL_NOT: return o + " = !" + ops[1] + ";";
+        case BH_MAXIMUM: return o + " = " + ops[1] + " > " + ops[2] + " ? " + ops[1] + " : " + ops[2] + ";";
+        case BH_MINIMUM: return o + " = " + ops[1] + " < " + ops[2] + " ? " + ops[1] + " : " + ops[2] + ";";
+        case BH_BITWISE_AND: return bin("&");
+        case BH_BITWISE_OR: return bin("|");
+        case BH_BITWISE_XOR: return bin("^");
+        case BH_INVERT:
+            if (t0 == bh_type::BOOL) return o + " = !" + ops[1] + ";";
+            return o + " = ~" + ops[1] + ";";
+        case BH_LEFT_SHIFT: return bin("<<");
+        case BH_RIGHT_SHIFT: return bin(">>");
+        case BH_COS: return un("cos");
+        case BH_SIN: return un("sin");
+        case BH_TAN: return un("tan");
+        case BH_COSH: return un("cosh");
+        case BH_SINH: return un("sinh");
+        case BH_TANH: return un("tanh");
+        case BH_ARCSIN: return un("asin");
+        case BH_ARCCOS: return un("acos");
+        case BH_ARCTAN: return un("atan");
+        case BH_ARCSINH: return un("asinh");
+        case BH_ARCCOSH: return un("acosh");
+        case BH_ARCTANH: return un("atanh");
+        case BH_ARCTAN2: return o + " = " + fn("atan2", t1) + "(" + ops[1] + ", " + ops[2] + ");";
+        case BH_EXP: return un("exp");
+        case BH_EXP2: return un("exp2");
+        case BH_EXPM1: return un("expm1");
+        case BH_LOG: return un("log");
+        case BH_LOG2: return un("log2");
+        case BH_LOG10: return un("log10");
+        case BH_LOG1P: return un("log1p");
+        case BH_SQRT: return un("sqrt");
+        case BH_CEIL: return un("ceil");
+        case BH_TRUNC: return un("trunc");
+        case BH_FLOOR: return un("floor");
+        case BH_RINT: return un("rint");
+        case BH_MOD:
+            if (is_float(t0)) return o + " = " + fn("fmod", t0) + "(" + ops[1] + ", " + ops[2] + ");";
+            return bin("%");
+        case BH_REMAINDER: {
+            const string &a = ops[1], &b = ops[2];
+            if (is_float(t0)) return o + " = " + a + " - " + fn("floor", t0) + "(" + a + " / " + b + ") * " + b + ";";
+            if (bh_type_is_unsigned_integer(t0)) return bin("%");
+            return o + " = ((" + a + " > 0) == (" + b + " > 0) || (" + a + " % " + b + ") == 0) ? (" + a + " % " +
+                   b + ") : (" + a + " % " + b + ") + " + b + ";";
+        }
+        case BH_ISNAN:
+            return is_float(t1) ? o + " = isnan(" + ops[1] + ");" : o + " = false;";
+        case BH_ISINF:
+            return is_float(t1) ? o + " = isinf(" + ops[1] + ");" : o + " = false;";
+        case BH_ISFINITE:
+            return is_float(t1) ? o + " = isfinite(" + ops[1] + ");" : o + " = true;";
+        case BH_IDENTITY: return o + " = " + ops[1] + ";";
+        case BH_SIGN: return o + " = " + sign_expr(ops[1]) + ";";
+        case BH_RANGE: return o + " = " + ops[1] + ";";
+        case BH_RANDOM: return o + " = " + ops[1] + ";";
+        case BH_GATHER: return o + " = " + ops[1] + ";";
+        case BH_SCATTER: return o + " = " + ops[1] + ";";
+        case BH_COND_SCATTER: return "if (" + ops[2] + ") { " + o + " = " + ops[1] + "; }";
+        case BH_ADD_ACCUMULATE: return o + " = " + ops[1] + " + " + ops[2] + ";";
+        case BH_MULTIPLY_ACCUMULATE: return o + " = " + ops[1] + " * " + ops[2] + ";";
+        default: break;
+    }
+    throw runtime_error(string("Instruction not supported by the CUDA engine: ") + bh_opcode_text(op));
+}
+
+// Literal CUDA expression of a constant (used for identities folded into accumulator init).
+string constant_literal(const bh_constant &c) {
+    stringstream ss;
+    ss.precision(17);
+    switch (c.type) {
+        case bh_type::BOOL: ss << (c.value.bool8 ? "true" : "false"); break;
+        case bh_type::INT8: ss << "((signed char)" << static_cast<int>(c.value.int8) << ")"; break;
+        case bh_type::INT16: ss << "((short)" << c.value.int16 << ")"; break;
+        case bh_type::INT32: ss << "((int)" << c.value.int32 << ")"; break;
+        case bh_type::INT64:
+            // INT64_MIN+1 and friends: write through the unsigned bit pattern to avoid overflowing literals.
+            ss << "((long long)" << static_cast<uint64_t>(c.value.int64) << "ULL)";
+            break;
+        case bh_type::UINT8: ss << "((unsigned char)" << static_cast<unsigned>(c.value.uint8) << "u)"; break;
+        case bh_type::UINT16: ss << "((unsigned short)" << c.value.uint16 << "u)"; break;
+        case bh_type::UINT32: ss << c.value.uint32 << "u"; break;
+        case bh_type::UINT64: ss << c.value.uint64 << "ULL"; break;
+        case bh_type::FLOAT32: {
+            uint32_t bits;
+            memcpy(&bits, &c.value.float32, 4);
+            ss << "__int_as_float(" << static_cast<int32_t>(bits) << ")";
+            break;
+        }
+        case bh_type::FLOAT64: {
+            int64_t bits;
+            memcpy(&bits, &c.value.float64, 8);
+            ss << "__longlong_as_double(" << static_cast<uint64_t>(bits) << "LL)";
+            break;
+        }
+        default: throw runtime_error("constant_literal(): unsupported constant type");
+    }
+    return ss.str();
+}
+
+// ------------------------------------------------------------------------------- view identity
+// Views compared like the reference's IgnoreOneDim_less (base, start and the (shape, stride) of
+// dimensions larger than one); used to find scalar-replaced reduction outputs.
+struct ViewKey {
+    const bh_base *base;
+    int64_t start;
+    vector<pair<int64_t, int64_t>> dims;
+    explicit ViewKey(const bh_view &v) : base(v.base), start(v.start) {
+        for (int64_t i = 0; i < v.ndim; ++i)
+            if (v.shape[i] > 1) dims.emplace_back(v.shape[i], v.stride[i]);
+    }
+    bool operator<(const ViewKey &o) const { return tie(base, start, dims) < tie(o.base, o.start, o.dims); }
+};
+
+// ------------------------------------------------------------------------------- unit symbols
+struct Symbols {
+    vector<bh_base *> params;
+    map<const bh_base *, int> param_id;
+    map<const bh_base *, int> base_id; // every base (params and temporaries)
+    set<const bh_base *> temps;
+    set<const bh_base *> always_array;
+    map<bh_view, int> view_id; // exact view -> offset/stride slot
+    vector<bh_view> views;
+    map<const LoopB *, int> loop_id;
+    vector<const LoopB *> loops;
+    map<const bh_instruction *, int> const_id;
+    vector<const bh_instruction *> consts;
+
+    int base_index(const bh_base *b) {
+        auto it = base_id.find(b);
+        if (it != base_id.end()) return it->second;
+        const int id = static_cast<int>(base_id.size());
+        base_id[b] = id;
+        return id;
+    }
+};
+
+void collect_loops(const LoopB &l, Symbols &s) {
+    if (l.rank >= 0 && !s.loop_id.count(&l)) {
+        s.loop_id[&l] = static_cast<int>(s.loops.size());
+        s.loops.push_back(&l);
+    }
+    for (const Block &b : l._block_list)
+        if (!b.isInstr()) collect_loops(b.getLoop(), s);
+}
+
+// Build the symbols of a unit made of `items` (instruction and loop blocks, in order).
+// `folded` instructions are identities turned into accumulator initialisation (no constant slot).
+Symbols build_symbols(const vector<const Block *> &items, const set<const bh_instruction *> &folded) {
+    Symbols s;
+    vector<InstrPtr> instrs;
+    set<bh_base *> temps, frees;
+    for (const Block *b : items) {
+        if (b->isInstr()) {
+            instrs.push_back(b->getInstr());
+        } else {
+            jitk::all_instr(b->getLoop(), instrs);
+            const auto t = b->getLoop().getAllTemps();
+            temps.insert(t.begin(), t.end());
+            const auto f = b->getLoop().getAllFrees();
+            frees.insert(f.begin(), f.end());
+            collect_loops(b->getLoop(), s);
+        }
+    }
+    for (const InstrPtr &instr : instrs) {
+        if (bh_opcode_is_accumulate(instr->opcode)) {
+            s.always_array.insert(instr->operand[0].base);
+        } else if (instr->opcode == BH_GATHER) {
+            s.always_array.insert(instr->operand[1].base);
+        } else if (instr->opcode == BH_SCATTER || instr->opcode == BH_COND_SCATTER) {
+            s.always_array.insert(instr->operand[0].base);
+        }
+    }
+    for (const bh_base *t : temps)
+        if (!s.always_array.count(t)) s.temps.insert(t);
+    for (const InstrPtr &instr : instrs) {
+        for (const bh_view &v : instr->getViews()) {
+            s.base_index(v.base);
+            if (!s.temps.count(v.base) && !s.param_id.count(v.base)) {
+                s.param_id[v.base] = static_cast<int>(s.params.size());
+                s.params.push_back(v.base);
+            }
+            // Views of temporaries are registered too: BH_RANGE/BH_RANDOM use their index.
+            if (!s.view_id.count(v)) {
+                s.view_id[v] = static_cast<int>(s.views.size());
+                s.views.push_back(v);
+            }
+        }
+        if (instr->has_constant() && !bh_opcode_is_sweep(instr->opcode) && !folded.count(instr.get())) {
+            s.const_id[instr.get()] = static_cast<int>(s.consts.size());
+            s.consts.push_back(instr.get());
+        }
+    }
+    return s;
+}
+
+// ------------------------------------------------------------------------------------ emitter
+struct Scope {
+    const Scope *parent = nullptr;
+    set<const bh_base *> tmps;
+    map<ViewKey, string> repl; // scalar-replaced views
+    bool is_tmp(const bh_base *b) const { return tmps.count(b) || (parent && parent->is_tmp(b)); }
+    const string *replaced(const bh_view &v) const {
+        auto it = repl.find(ViewKey(v));
+        if (it != repl.end()) return &it->second;
+        return parent ? parent->replaced(v) : nullptr;
+    }
+};
+
+class Emitter {
+public:
+    Symbols &sym;
+    ostream &out;
+    const CodegenOptions &opt;
+    // Views replaced by accumulators owned by the schedule (no write-back by the emitter).
+    map<ViewKey, string> external_acc;
+
+    Emitter(Symbols &s, ostream &o, const CodegenOptions &op) : sym(s), out(o), opt(op) {}
+
+    void indent(int n) { out << string(static_cast<size_t>(n), ' '); }
+
+    // Local temporaries of `loop` in symbol order (deterministic source text).
+    vector<const bh_base *> sorted_temps(const LoopB &loop) {
+        vector<const bh_base *> ret;
+        for (const bh_base *b : loop.getLocalTemps())
+            if (sym.base_id.count(b)) ret.push_back(b);
+        sort(ret.begin(), ret.end(), [&](const bh_base *a, const bh_base *b) { return sym.base_id.at(a) < sym.base_id.at(b); });
+        return ret;
+    }
+
+    string index_expr(const bh_view &v, int hidden_axis = BH_MAXDIM, pair<int, int> axis_offset = {-1, 0}) {
+        const int vid = sym.view_id.at(v);
+        stringstream ss;
+        ss << "(p.v" << vid << "_o";
+        if (!v.is_scalar()) {
+            for (int64_t i = 0; i < v.ndim; ++i) {
+                int t = static_cast<int>(i);
+                if (t >= hidden_axis) ++t;
+                if (axis_offset.first == t) {
+                    ss << " + (i" << t << " == 0 ? 0 : i" << t << " + (" << axis_offset.second << "))";
+                } else {
+                    ss << " + i" << t;
+                }
+                ss << " * p.v" << vid << "_s" << i;
+            }
+        }
+        ss << ")";
+        return ss.str();
+    }
+
+    string array_ref(const bh_view &v, int hidden_axis = BH_MAXDIM, pair<int, int> axis_offset = {-1, 0}) {
+        const string idx = index_expr(v, hidden_axis, axis_offset);
+        const int pid = sym.param_id.at(v.base);
+        if (opt.bounds_check) {
+            return "a" + to_string(pid) + "[bh_check(" + idx + ", p.nelem" + to_string(pid) + ", p.err)]";
+        }
+        return "a" + to_string(pid) + "[" + idx + "]";
+    }
+
+    string name(const bh_view &v, const Scope &s, int hidden_axis = BH_MAXDIM) {
+        if (s.is_tmp(v.base)) return "t" + to_string(sym.base_index(v.base));
+        auto ext = external_acc.find(ViewKey(v));
+        if (ext != external_acc.end()) return ext->second;
+        if (const string *r = s.replaced(v)) return *r;
+        return array_ref(v, hidden_axis);
+    }
+
+    bool is_array(const bh_view &v, const Scope &s) {
+        return !(s.is_tmp(v.base) || s.replaced(v) || external_acc.count(ViewKey(v)));
+    }
+
+    string const_ref(const bh_instruction &instr) { return "p.c" + to_string(sym.const_id.at(&instr)); }
+
+    void write_instr(const bh_instruction &instr, const Scope &s, int ind) {
+        if (bh_opcode_is_system(instr.opcode) || instr.operand.empty()) return;
+        vector<string> ops;
+        if (instr.opcode == BH_RANGE) {
+            ops.push_back(name(instr.operand[0], s));
+            ops.push_back("(bh_u64)" + index_expr(instr.operand[0]));
+        } else if (instr.opcode == BH_RANDOM) {
+            ops.push_back(name(instr.operand[0], s));
+            const int cid = sym.const_id.at(&instr);
+            ops.push_back("bh_random123(p.c" + to_string(cid) + "_start, p.c" + to_string(cid) + "_key, (bh_u64)" +
+                          index_expr(instr.operand[0]) + ")");
+        } else if (instr.opcode == BH_GATHER) {
+            ops.push_back(name(instr.operand[0], s));
+            const bh_view &in = instr.operand[1];
+            ops.push_back("a" + to_string(sym.param_id.at(in.base)) + "[p.v" + to_string(sym.view_id.at(in)) +
+                          "_o + (bh_i64)" + name(instr.operand[2], s) + "]");
+        } else if (instr.opcode == BH_SCATTER || instr.opcode == BH_COND_SCATTER) {
+            const bh_view &outv = instr.operand[0];
+            ops.push_back("a" + to_string(sym.param_id.at(outv.base)) + "[p.v" + to_string(sym.view_id.at(outv)) +
+                          "_o + (bh_i64)" + name(instr.operand[2], s) + "]");
+            ops.push_back(name(instr.operand[1], s));
+            if (instr.opcode == BH_COND_SCATTER) ops.push_back(name(instr.operand[3], s));
+        } else if (bh_opcode_is_accumulate(instr.opcode)) {
+            ops.push_back(name(instr.operand[0], s));
+            ops.push_back(array_ref(instr.operand[0], BH_MAXDIM, {instr.sweep_axis(), -1}));
+            ops.push_back(name(instr.operand[1], s));
+        } else if (bh_opcode_is_reduction(instr.opcode)) {
+            // The constant operand of a reduction is its axis, not a value.
+            const bh_view &v = instr.operand[0];
+            if (instr.operand[1].ndim > 1 && is_array(v, s)) {
+                ops.push_back(array_ref(v, instr.sweep_axis()));
+            } else {
+                ops.push_back(name(v, s));
+            }
+            ops.push_back(name(instr.operand[1], s));
+        } else {
+            for (size_t o = 0; o < instr.operand.size(); ++o) {
+                const bh_view &v = instr.operand[o];
+                if (v.isConstant()) {
+                    ops.push_back(const_ref(instr));
+                } else if (o == 0 && bh_opcode_is_reduction(instr.opcode) && instr.operand[1].ndim > 1 &&
+                           is_array(v, s)) {
+                    ops.push_back(array_ref(v, instr.sweep_axis()));
+                } else {
+                    ops.push_back(name(v, s));
+                }
+            }
+        }
+        indent(ind);
+        out << op_statement(instr, ops) << "\n";
+    }
+
+    // Emit the body of `loop` (its temporaries, accumulators of swept children, instructions and
+    // serial sub-loops). Loop heads of `loop` itself are written by the caller.
+    void write_body(const LoopB &loop, Scope &scope, int ind) {
+        // Temporaries local to this loop become registers.
+        for (const bh_base *b : sorted_temps(loop)) {
+            if (sym.temps.count(b) && !scope.is_tmp(b)) {
+                scope.tmps.insert(b);
+                indent(ind);
+                out << cuda_type(b->dtype()) << " t" << sym.base_index(b) << ";\n";
+            }
+        }
+        // Outputs of reductions over the innermost axis of a child loop live in registers here.
+        vector<pair<const bh_view *, const bh_instruction *>> replaced_here;
+        for (const Block &b1 : loop._block_list) {
+            if (b1.isInstr()) continue;
+            for (const InstrPtr &instr : jitk::all_local_instr(b1.getLoop())) {
+                if (bh_opcode_is_reduction(instr->opcode) && jitk::sweeping_innermost_axis(instr)) {
+                    const bh_view &v = instr->operand[0];
+                    if (scope.is_tmp(v.base) || scope.replaced(v) || external_acc.count(ViewKey(v)) ||
+                        sym.always_array.count(v.base))
+                        continue;
+                    const string nm = "s" + to_string(sym.base_index(v.base)) + "_" + to_string(replaced_here.size()) +
+                                      "_r" + to_string(loop.rank + 1);
+                    scope.repl[ViewKey(v)] = nm;
+                    replaced_here.emplace_back(&v, instr.get());
+                    indent(ind);
+                    out << cuda_type(v.base->dtype()) << " " << nm << ";\n";
+                }
+            }
+        }
+        for (const Block &b : loop._block_list) {
+            if (b.isInstr()) {
+                write_instr(*b.getInstr(), scope, ind);
+            } else {
+                const LoopB &sub = b.getLoop();
+                if (sub.isSystemOnly()) continue;
+                indent(ind);
+                out << "for (bh_i64 i" << sub.rank << " = 0; i" << sub.rank << " < p.n"
+                    << sym.loop_id.at(&sub) << "; ++i" << sub.rank << ") {\n";
+                Scope inner;
+                inner.parent = &scope;
+                write_body(sub, inner, ind + 4);
+                indent(ind);
+                out << "}\n";
+            }
+        }
+        // Write the scalar-replaced reduction outputs back (temporaries stay registers).
+        for (const auto &rp : replaced_here) {
+            const bh_view &v = *rp.first;
+            if (scope.is_tmp(v.base)) continue;
+            indent(ind);
+            out << array_ref(v, rp.second->sweep_axis()) << " = " << scope.repl.at(ViewKey(v)) << ";\n";
+            scope.repl.erase(ViewKey(v));
+        }
+    }
+};
+
+// ------------------------------------------------------------------------------ param struct
+struct ParamLayout {
+    vector<ParamField> fields;
+    stringstream decl; // members of `struct P`
+    void add(const ParamField &f, const string &ctype, const string &name) {
+        fields.push_back(f);
+        decl << "    alignas(8) " << ctype << " " << name << ";\n";
+    }
+};
+
+void add_common_fields(Symbols &sym, ParamLayout &pl, const CodegenOptions &opt) {
+    for (size_t i = 0; i < sym.params.size(); ++i) {
+        ParamField f{ParamField::PTR};
+        f.base = sym.params[i];
+        pl.add(f, cuda_type(sym.params[i]->dtype()) + "* __restrict__", "a" + to_string(i));
+    }
+    for (size_t i = 0; i < sym.views.size(); ++i) {
+        const bh_view &v = sym.views[i];
+        ParamField f{ParamField::I64};
+        f.i64 = v.start;
+        pl.add(f, "bh_i64", "v" + to_string(i) + "_o");
+        for (int64_t d = 0; d < v.ndim; ++d) {
+            f.i64 = v.stride[d];
+            pl.add(f, "bh_i64", "v" + to_string(i) + "_s" + to_string(d));
+        }
+    }
+    for (size_t i = 0; i < sym.loops.size(); ++i) {
+        ParamField f{ParamField::I64};
+        f.i64 = sym.loops[i]->size;
+        pl.add(f, "bh_i64", "n" + to_string(i));
+    }
+    for (size_t i = 0; i < sym.consts.size(); ++i) {
+        const bh_instruction *instr = sym.consts[i];
+        if (instr->constant.type == bh_type::R123) {
+            ParamField f{ParamField::R123_START};
+            f.c = instr->constant;
+            pl.add(f, "bh_u64", "c" + to_string(i) + "_start");
+            f.kind = ParamField::R123_KEY;
+            pl.add(f, "bh_u64", "c" + to_string(i) + "_key");
+        } else {
+            if (bh_type_is_complex(instr->constant.type))
+                throw runtime_error("complex constants are not supported by the CUDA engine");
+            ParamField f{ParamField::CONST};
+            f.c = instr->constant;
+            pl.add(f, cuda_type(instr->constant.type), "c" + to_string(i));
+        }
+    }
+    if (opt.bounds_check) {
+        for (size_t i = 0; i < sym.params.size(); ++i) {
+            ParamField f{ParamField::I64};
+            f.i64 = sym.params[i]->nelem();
+            pl.add(f, "bh_i64", "nelem" + to_string(i));
+        }
+        ParamField f{ParamField::SCRATCH};
+        f.i64 = -1; // the engine's error record
+        pl.add(f, "unsigned long long*", "err");
+    }
+}
+
+string bounds_check_helper() {
+    return R"CUDA(
+__device__ __forceinline__ bh_i64 bh_check(bh_i64 idx, bh_i64 n, unsigned long long *err) {
+    if (idx < 0 || idx >= n) { atomicCAS(err, 0ULL, (unsigned long long)idx | 0x8000000000000000ULL); return 0; }
+    return idx;
+}
+)CUDA";
+}
+
+uint64_t fnv1a(const string &s) {
+    uint64_t h = 1469598103934665603ULL;
+    for (unsigned char c : s) {
+        h ^= c;
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+
+void finish_source(LaunchUnit &u, const string &params_decl, const string &body, const CodegenOptions &opt) {
+    stringstream src;
+    src << kPrelude;
+    if (opt.bounds_check) src << bounds_check_helper();
+    src << "struct P {\n" << params_decl << "};\n";
+    src << body;
+    const string without_name = src.str();
+    stringstream nm;
+    nm << "bh_" << sched_name(u.sched) << "_" << hex << fnv1a(without_name);
+    u.name = nm.str();
+    string s = without_name;
+    const string placeholder = "__KERNEL_NAME__";
+    for (size_t pos = s.find(placeholder); pos != string::npos; pos = s.find(placeholder))
+        s.replace(pos, placeholder.size(), u.name);
+    u.source = s;
+}
+
+// Unpack the pointer fields into local restrict pointers.
+string pointer_locals(const Symbols &sym) {
+    stringstream ss;
+    for (size_t i = 0; i < sym.params.size(); ++i)
+        ss << "    " << cuda_type(sym.params[i]->dtype()) << "* __restrict__ a" << i << " = p.a" << i << ";\n";
+    return ss.str();
+}
+
+int64_t unit_bytes(const Symbols &sym) {
+    int64_t b = 0;
+    for (const bh_view &v : sym.views) b += v.shape.prod() * bh_type_size(v.base->dtype());
+    return b;
+}
+
+// ------------------------------------------------------------------------------------ schedules
+LaunchUnit lower_serial(const vector<const Block *> &items, const CodegenOptions &opt) {
+    LaunchUnit u;
+    u.sched = Sched::SERIAL;
+    // The kernel is a loop of rank -1: wrap the items in a pseudo loop so temporaries and
+    // scalar replacement are handled uniformly.
+    LoopB pseudo{-1, 1};
+    for (const Block *b : items) pseudo._block_list.push_back(*b);
+    pseudo.metadataUpdate();
+    vector<const Block *> pitems;
+    for (const Block &b : pseudo._block_list) pitems.push_back(&b);
+    Symbols sym = build_symbols(pitems, {});
+    ParamLayout pl2;
+    add_common_fields(sym, pl2, opt);
+    stringstream body;
+    Emitter em(sym, body, opt);
+    body << "extern \"C\" __global__ void __launch_bounds__(32) __KERNEL_NAME__(const __grid_constant__ P p) {\n";
+    body << "    if (blockIdx.x != 0 || threadIdx.x != 0) return;\n";
+    body << pointer_locals(sym);
+    Scope scope;
+    em.write_body(pseudo, scope, 4);
+    body << "}\n";
+    u.fields = pl2.fields;
+    u.algorithmic_bytes = unit_bytes(sym);
+    finish_source(u, pl2.decl.str(), body.str(), opt);
+    return u;
+}
+
+// FLAT: `loop` has P >= 1 leading parallel ranks.
+LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) {
+    LaunchUnit u;
+    u.sched = Sched::FLAT;
+    const Block holder(loop);
+    const vector<const Block *> items = {&holder};
+    Symbols sym = build_symbols(items, {});
+    const LoopB &L = holder.getLoop();
+    const vector<const LoopB *> chain = jitk::get_first_loop_blocks(L);
+    const LoopB &inner = *chain[P - 1];
+    const bool innermost = inner.isInnermost();
+    u.V = innermost ? opt.flat_v : 1;
+    ParamLayout pl;
+    add_common_fields(sym, pl, opt);
+    ParamField f{ParamField::I64};
+    pl.add(f, "bh_i64", "rows");
+    pl.add(f, "bh_i64", "chunks");
+    pl.add(f, "bh_i64", "work");
+    int64_t rows = 1;
+    for (unsigned r = 0; r + 1 < P; ++r) rows *= chain[r]->size;
+    u.rows = rows;
+    u.cols = inner.size;
+    const int64_t per = static_cast<int64_t>(kThreads) * u.V;
+    const int64_t chunks = (u.cols + per - 1) / per;
+    pl.fields[pl.fields.size() - 3].i64 = rows;
+    pl.fields[pl.fields.size() - 2].i64 = chunks;
+    pl.fields[pl.fields.size() - 1].i64 = rows * chunks;
+
+    stringstream body;
+    Emitter em(sym, body, opt);
+    body << "extern \"C\" __global__ void __launch_bounds__(" << kThreads
+         << ") __KERNEL_NAME__(const __grid_constant__ P p) {\n";
+    body << pointer_locals(sym);
+    body << "    for (bh_i64 w = blockIdx.x; w < p.work; w += gridDim.x) {\n";
+    body << "        const bh_i64 row = w / p.chunks;\n";
+    body << "        const bh_i64 chunk = w - row * p.chunks;\n";
+    body << "        bh_i64 rem = row;\n";
+    for (int r = static_cast<int>(P) - 2; r >= 0; --r) {
+        const int lid = sym.loop_id.at(chain[r]);
+        if (r == 0) {
+            body << "        const bh_i64 i0 = rem;\n";
+        } else {
+            body << "        const bh_i64 i" << r << " = rem % p.n" << lid << "; rem /= p.n" << lid << ";\n";
+        }
+    }
+    body << "        (void)rem;\n";
+    body << "        const bh_i64 cbase = chunk * " << per << " + threadIdx.x;\n";
+    body << "#pragma unroll\n";
+    body << "        for (int j = 0; j < " << u.V << "; ++j) {\n";
+    body << "            const bh_i64 i" << (P - 1) << " = cbase + j * " << kThreads << ";\n";
+    body << "            if (i" << (P - 1) << " >= p.n" << sym.loop_id.at(&inner) << ") break;\n";
+    Scope scope;
+    // Temporaries declared on the threaded chain above the innermost threaded loop.
+    for (unsigned r = 0; r + 1 < P; ++r) {
+        for (const bh_base *b : em.sorted_temps(*chain[r])) {
+            if (sym.temps.count(b) && !scope.is_tmp(b)) {
+                scope.tmps.insert(b);
+                body << "            " << cuda_type(b->dtype()) << " t" << sym.base_index(b) << ";\n";
+            }
+        }
+    }
+    em.write_body(inner, scope, 12);
+    body << "        }\n    }\n}\n";
+    u.fields = pl.fields;
+    u.algorithmic_bytes = unit_bytes(sym);
+    u.elements = rows * u.cols;
+    finish_source(u, pl.decl.str(), body.str(), opt);
+    return u;
+}
+
+// CTA-wide deterministic tree reduction of `v` (fixed xor-shuffle butterfly, then warp 0).
+string block_reduce_fn(const string &ctype, const string &fname, bh_opcode op, const string &identity) {
+    stringstream ss;
+    ss << "__device__ __forceinline__ " << ctype << " " << fname << "(" << ctype << " v, " << ctype << " *sm) {\n";
+    ss << "#pragma unroll\n";
+    ss << "    for (int m = 16; m >= 1; m >>= 1) { const " << ctype << " o = bh_shfl_xor(v, m); v = "
+       << reduce_expr(op, "v", "o") << "; }\n";
+    ss << "    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n";
+    ss << "    if (lane == 0) sm[warp] = v;\n";
+    ss << "    __syncthreads();\n";
+    ss << "    if (warp == 0) {\n";
+    ss << "        v = lane < " << (kThreads / 32) << " ? sm[lane] : " << identity << ";\n";
+    ss << "#pragma unroll\n";
+    ss << "        for (int m = 16; m >= 1; m >>= 1) { const " << ctype << " o = bh_shfl_xor(v, m); v = "
+       << reduce_expr(op, "v", "o") << "; }\n";
+    ss << "    }\n";
+    ss << "    __syncthreads();\n";
+    ss << "    return v;\n}\n";
+    return ss.str();
+}
+
+// GRID_REDUCE: `loop` is a 1-D innermost loop whose rank-0 sweeps are reductions to scalars.
+// `identities` are the kernel-level identity instructions of those reductions (folded).
+LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identities, const CodegenOptions &opt) {
+    LaunchUnit u;
+    u.sched = Sched::GRID_REDUCE;
+    u.V = kReduceV;
+    const Block holder(loop);
+    set<const bh_instruction *> folded;
+    for (const InstrPtr &i : identities) folded.insert(i.get());
+    Symbols sym = build_symbols({&holder}, folded);
+    const LoopB &L = holder.getLoop();
+    // Reductions of this loop, ordered by origin id.
+    vector<InstrPtr> reds(L._sweeps.begin(), L._sweeps.end());
+    sort(reds.begin(), reds.end(), [](const InstrPtr &a, const InstrPtr &b) { return a->origin_id < b->origin_id; });
+    u.nred = static_cast<int>(reds.size());
+    ParamLayout pl;
+    add_common_fields(sym, pl, opt);
+    ParamField f{ParamField::I64};
+    u.cols = L.size;
+    const int64_t ntiles = (L.size + kReduceTile - 1) / kReduceTile;
+    f.i64 = ntiles;
+    pl.add(f, "bh_i64", "ntiles");
+    ParamField fs{ParamField::SCRATCH};
+    pl.add(fs, "unsigned char*", "scratch");
+    ParamField fc{ParamField::COUNTER};
+    pl.add(fc, "unsigned int*", "counter");
+
+    stringstream helpers, body;
+    Emitter em(sym, body, opt);
+    // Each reduction gets an accumulator per thread and a slot per tile in the scratch buffer.
+    vector<string> ctypes, idents, accs;
+    int64_t scratch_off = 0;
+    vector<int64_t> offs;
+    for (size_t k = 0; k < reds.size(); ++k) {
+        const InstrPtr &r = reds[k];
+        const bh_type t = r->operand[0].base->dtype();
+        ctypes.push_back(cuda_type(t));
+        idents.push_back(constant_literal(jitk::sweep_identity(r->opcode, t)));
+        accs.push_back("tacc" + to_string(k));
+        offs.push_back(scratch_off);
+        scratch_off += 8; // per tile
+        helpers << block_reduce_fn(ctypes[k], "bh_block_reduce" + to_string(k), r->opcode, idents[k]);
+        em.external_acc[ViewKey(r->operand[0])] = accs[k];
+    }
+    u.scratch_bytes_per_tile = scratch_off;
+    body << helpers.str();
+    body << "extern \"C\" __global__ void __launch_bounds__(" << kThreads
+         << ") __KERNEL_NAME__(const __grid_constant__ P p) {\n";
+    body << pointer_locals(sym);
+    body << "    __shared__ unsigned long long sm_raw[" << (kThreads / 32) << "];\n";
+    body << "    __shared__ bool am_last;\n";
+    for (size_t k = 0; k < reds.size(); ++k)
+        body << "    " << ctypes[k] << "* part" << k << " = (" << ctypes[k] << "*)(p.scratch + p.ntiles * " << offs[k]
+             << ");\n";
+    body << "    for (bh_i64 tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {\n";
+    for (size_t k = 0; k < reds.size(); ++k) body << "        " << ctypes[k] << " " << accs[k] << " = " << idents[k] << ";\n";
+    body << "#pragma unroll\n";
+    body << "        for (int j = 0; j < " << kReduceV << "; ++j) {\n";
+    body << "            const bh_i64 i0 = tile * " << kReduceTile << " + j * " << kThreads << " + threadIdx.x;\n";
+    body << "            if (i0 >= p.n" << sym.loop_id.at(&L) << ") break;\n";
+    Scope scope;
+    em.write_body(L, scope, 12);
+    body << "        }\n";
+    for (size_t k = 0; k < reds.size(); ++k) {
+        body << "        " << accs[k] << " = bh_block_reduce" << k << "(" << accs[k] << ", (" << ctypes[k]
+             << "*)sm_raw);\n";
+        body << "        if (threadIdx.x == 0) part" << k << "[tile] = " << accs[k] << ";\n";
+    }
+    body << "    }\n";
+    body << "    __threadfence();\n";
+    body << "    __syncthreads();\n";
+    body << "    if (threadIdx.x == 0) am_last = atomicAdd(p.counter, 1u) == gridDim.x - 1;\n";
+    body << "    __syncthreads();\n";
+    body << "    if (!am_last) return;\n";
+    body << "    __threadfence();\n";
+    for (size_t k = 0; k < reds.size(); ++k) {
+        const InstrPtr &r = reds[k];
+        body << "    {\n";
+        body << "        " << ctypes[k] << " acc = " << idents[k] << ";\n";
+        body << "        for (bh_i64 t = threadIdx.x; t < p.ntiles; t += " << kThreads << ") {\n";
+        body << "            const " << ctypes[k] << " x = ((volatile " << ctypes[k] << "*)part" << k << ")[t];\n";
+        body << "            acc = " << reduce_expr(r->opcode, "acc", "x") << ";\n";
+        body << "        }\n";
+        body << "        acc = bh_block_reduce" << k << "(acc, (" << ctypes[k] << "*)sm_raw);\n";
+        if (!sym.temps.count(r->operand[0].base)) {
+            body << "        if (threadIdx.x == 0) " << em.array_ref(r->operand[0]) << " = acc;\n";
+        }
+        body << "    }\n";
+    }
+    body << "    if (threadIdx.x == 0) *p.counter = 0u;\n";
+    body << "}\n";
+    u.fields = pl.fields;
+    u.algorithmic_bytes = unit_bytes(sym);
+    u.elements = L.size;
+    finish_source(u, pl.decl.str(), body.str(), opt);
+    return u;
+}
+
+// OUTER_REDUCE: rank 0 sweeps (reductions) with a single parallel sub-nest and no instructions
+// directly at rank 0. Threads own points of the sub-nest and loop over the reduced axis in order.
+bool outer_reduce_applicable(const LoopB &L) {
+    if (L._sweeps.empty()) return false;
+    for (const InstrPtr &s : L._sweeps)
+        if (!bh_opcode_is_reduction(s->opcode)) return false;
+    if (!jitk::all_local_instr(L).empty()) return false;
+    if (L._block_list.size() != 1 || L._block_list[0].isInstr()) return false;
+    const LoopB &sub = L._block_list[0].getLoop();
+    const unsigned P = static_cast<unsigned>(jitk::parallel_ranks(sub, 64).first);
+    if (P == 0) return false;
+    // Every sweep must be inside the threaded chain's innermost loop or below it, and the whole
+    // sub-nest must be free of deeper sweeps over the threaded ranks (guaranteed by P).
+    return true;
+}
+
+LaunchUnit lower_outer_reduce(const LoopB &loop, const vector<const Block *> &identity_loops,
+                              const CodegenOptions &opt) {
+    LaunchUnit u;
+    u.sched = Sched::OUTER_REDUCE;
+    const Block holder(loop);
+    set<const bh_instruction *> folded;
+    for (const Block *b : identity_loops)
+        for (const InstrPtr &i : jitk::all_instr(*b)) folded.insert(i.get());
+    Symbols sym = build_symbols({&holder}, folded);
+    const LoopB &L = holder.getLoop();
+    const LoopB &sub = L._block_list[0].getLoop();
+    const unsigned P = static_cast<unsigned>(jitk::parallel_ranks(sub, 64).first);
+    const vector<const LoopB *> chain = jitk::get_first_loop_blocks(sub);
+    const LoopB &inner = *chain[P - 1];
+    ParamLayout pl;
+    add_common_fields(sym, pl, opt);
+    int64_t rows = 1;
+    for (unsigned r = 0; r + 1 < P; ++r) rows *= chain[r]->size;
+    u.rows = rows;
+    u.cols = inner.size;
+    ParamField f{ParamField::I64};
+    f.i64 = rows * inner.size;
+    pl.add(f, "bh_i64", "points");
+    vector<InstrPtr> reds(L._sweeps.begin(), L._sweeps.end());
+    sort(reds.begin(), reds.end(), [](const InstrPtr &a, const InstrPtr &b) { return a->origin_id < b->origin_id; });
+
+    stringstream body;
+    Emitter em(sym, body, opt);
+    body << "extern \"C\" __global__ void __launch_bounds__(" << kThreads
+         << ") __KERNEL_NAME__(const __grid_constant__ P p) {\n";
+    body << pointer_locals(sym);
+    body << "    for (bh_i64 pt = (bh_i64)blockIdx.x * " << kThreads << " + threadIdx.x; pt < p.points; pt += (bh_i64)gridDim.x * "
+         << kThreads << ") {\n";
+    // Decompose the point into the sub-nest's threaded indices (ranks 1..P).
+    body << "        bh_i64 rem = pt;\n";
+    for (int r = static_cast<int>(P) - 1; r >= 0; --r) {
+        const int rank = r + 1;
+        const int lid = sym.loop_id.at(chain[r]);
+        if (r == 0) {
+            body << "        const bh_i64 i" << rank << " = rem;\n";
+        } else {
+            body << "        const bh_i64 i" << rank << " = rem % p.n" << lid << "; rem /= p.n" << lid << ";\n";
+        }
+    }
+    // Accumulators of the rank-0 reductions, initialised with the identity.
+    Scope scope;
+    for (size_t k = 0; k < reds.size(); ++k) {
+        const bh_type t = reds[k]->operand[0].base->dtype();
+        const string nm = "oacc" + to_string(k);
+        body << "        " << cuda_type(t) << " " << nm << " = "
+             << constant_literal(jitk::sweep_identity(reds[k]->opcode, t)) << ";\n";
+        em.external_acc[ViewKey(reds[k]->operand[0])] = nm;
+    }
+    for (unsigned r = 0; r + 1 < P; ++r) {
+        for (const bh_base *b : em.sorted_temps(*chain[r])) {
+            if (sym.temps.count(b) && !scope.is_tmp(b)) {
+                scope.tmps.insert(b);
+                body << "        " << cuda_type(b->dtype()) << " t" << sym.base_index(b) << ";\n";
+            }
+        }
+    }
+    body << "        for (bh_i64 i0 = 0; i0 < p.n" << sym.loop_id.at(&L) << "; ++i0) {\n";
+    Scope s0;
+    s0.parent = &scope;
+    for (const bh_base *b : em.sorted_temps(L)) {
+        if (sym.temps.count(b) && !s0.is_tmp(b)) {
+            s0.tmps.insert(b);
+            body << "            " << cuda_type(b->dtype()) << " t" << sym.base_index(b) << ";\n";
+        }
+    }
+    em.write_body(inner, s0, 12);
+    body << "        }\n";
+    for (size_t k = 0; k < reds.size(); ++k) {
+        if (sym.temps.count(reds[k]->operand[0].base)) continue;
+        body << "        " << em.array_ref(reds[k]->operand[0], 0) << " = oacc" << k << ";\n";
+    }
+    body << "    }\n}\n";
+    u.fields = pl.fields;
+    u.algorithmic_bytes = unit_bytes(sym);
+    u.elements = rows * inner.size * L.size;
+    finish_source(u, pl.decl.str(), body.str(), opt);
+    return u;
+}
+
+bool is_foldable_identity(const Block &b) {
+    if (!b.isInstr()) return false;
+    const bh_instruction &i = *b.getInstr();
+    return i.opcode == BH_IDENTITY && i.operand.size() == 2 && i.operand[1].isConstant();
+}
+
+bool identity_loop(const Block &b) {
+    if (b.isInstr()) return false;
+    const auto instrs = jitk::all_instr(b);
+    return instrs.size() == 1 && instrs[0]->opcode == BH_IDENTITY && instrs[0]->operand[1].isConstant();
+}
+
+} // namespace
+
+vector<LaunchUnit> lower_kernel(const LoopB &kernel, const CodegenOptions &opt) {
+    vector<const Block *> items;
+    for (const Block &b : kernel._block_list)
+        if (!b.isSystemOnly()) items.push_back(&b);
+    if (items.empty()) return {};
+
+    vector<LaunchUnit> units;
+    vector<InstrPtr> pending_identities;     // kernel-level scalar identities
+    vector<const Block *> pending_id_loops;  // kernel-level identity loops
+    bool serial = false;
+    for (size_t idx = 0; idx < items.size() && !serial; ++idx) {
+        const Block &b = *items[idx];
+        if (b.isInstr()) {
+            if (is_foldable_identity(b)) {
+                pending_identities.push_back(b.getInstr());
+                continue;
+            }
+            serial = true;
+            break;
+        }
+        const LoopB &L = b.getLoop();
+        if (identity_loop(b) && idx + 1 < items.size()) {
+            pending_id_loops.push_back(&b);
+            continue;
+        }
+        const unsigned P = static_cast<unsigned>(jitk::parallel_ranks(L, 64).first);
+        if (P >= 1) {
+            if (!pending_identities.empty()) {
+                serial = true;
+                break;
+            }
+            for (const Block *il : pending_id_loops) {
+                const unsigned Pi = static_cast<unsigned>(jitk::parallel_ranks(il->getLoop(), 64).first);
+                units.push_back(lower_flat(il->getLoop(), Pi, opt));
+            }
+            pending_id_loops.clear();
+            units.push_back(lower_flat(L, P, opt));
+            continue;
+        }
+        bool all_reduce = !L._sweeps.empty();
+        for (const InstrPtr &s : L._sweeps) all_reduce = all_reduce && bh_opcode_is_reduction(s->opcode);
+        if (all_reduce && L.isInnermost() && pending_id_loops.empty()) {
+            // Every folded identity must belong to one of this loop's reductions.
+            set<ViewKey> outs;
+            for (const InstrPtr &s : L._sweeps) outs.insert(ViewKey(s->operand[0]));
+            bool ok = true;
+            for (const InstrPtr &i : pending_identities) ok = ok && outs.count(ViewKey(i->operand[0]));
+            if (ok) {
+                units.push_back(lower_grid_reduce(L, pending_identities, opt));
+                pending_identities.clear();
+                continue;
+            }
+        }
+        if (all_reduce && outer_reduce_applicable(L) && pending_identities.empty()) {
+            set<ViewKey> outs;
+            for (const InstrPtr &s : L._sweeps) outs.insert(ViewKey(s->operand[0]));
+            bool ok = true;
+            for (const Block *il : pending_id_loops) ok = ok && outs.count(ViewKey(jitk::all_instr(*il)[0]->operand[0]));
+            if (ok) {
+                units.push_back(lower_outer_reduce(L, pending_id_loops, opt));
+                pending_id_loops.clear();
+                continue;
+            }
+        }
+        serial = true;
+    }
+    if (!serial && (!pending_identities.empty() || !pending_id_loops.empty())) serial = true;
+    if (serial) return {lower_serial(items, opt)};
+    return units;
+}
+
+} // namespace cuda
+} // namespace bohrium

@@ -1,0 +1,79 @@
+// Lowering of fused kernels (jitk::LoopB, rank -1) to sm_100a CUDA source.
+//
+// The reference emits one generic SIMT loop nest per kernel (core/jitk/engines/engine.cpp:84-336,
+// ve/cuda/engine_cuda.cpp:243-274) with fixed 128-thread blocks, hard-coded loop sizes and a CPU
+// offload for blocks that sweep their outermost axis (include/bohrium/jitk/engines/engine_gpu.hpp:
+// 140-142). Here every fused loop nest is lowered to one of a few launch schedules:
+//
+//   FLAT          the leading parallel ranks form a (rows x cols) index space processed by a
+//                 grid-stride persistent kernel, V elements per thread along the innermost
+//                 parallel rank; deeper ranks are serial loops inside the thread.
+//   GRID_REDUCE   a 1-D nest that reduces its only axis (maps fused with sum/max/... to a scalar):
+//                 fixed tiles of TILE = 256 x 8 elements, a per-tile CTA tree, then the last CTA
+//                 folds the tile partials in tile order. The summation order depends only on the
+//                 element count, never on the grid size, so batched and plain launches agree bit
+//                 for bit.
+//   OUTER_REDUCE  a nest that reduces its outermost axis into an array: threads own the output
+//                 elements (the inner parallel ranks) and loop over the reduced axis.
+//   SCAN1D        a 1-D nest whose outermost axis is an accumulate (cumulative sum/product):
+//                 chunked three-phase scan (chunk totals, serial exclusive scan of the totals,
+//                 re-scan with carry).
+//   SERIAL        anything else: one thread runs the nest in program order (always correct).
+//
+// All loop sizes, view offsets/strides and constants are kernel parameters, so one compiled
+// kernel serves every array size and sliding offset; the generated source depends only on the
+// block structure and element types.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+#include "../jitk/block.hpp"
+
+namespace bohrium {
+namespace cuda {
+
+enum class Sched { FLAT, GRID_REDUCE, OUTER_REDUCE, SCAN1D, SERIAL };
+const char *sched_name(Sched s);
+
+constexpr int kThreads = 256;      // threads per CTA for every schedule
+constexpr int kReduceV = 8;        // elements per thread per tile in GRID_REDUCE
+constexpr int64_t kReduceTile = kThreads * kReduceV;
+constexpr int64_t kScanChunk = 4096; // elements per chunk in SCAN1D
+
+// One 8-byte slot (or two for 16-byte constants) of the kernel parameter struct.
+struct ParamField {
+    enum Kind { PTR, I64, CONST, R123_START, R123_KEY, SCRATCH, COUNTER } kind;
+    bh_base *base = nullptr; // PTR
+    int64_t i64 = 0;         // I64
+    bh_constant c{};         // CONST / R123_*
+};
+
+struct LaunchUnit {
+    std::string name;   // kernel function name (derived from the source hash)
+    std::string source; // complete CUDA source
+    Sched sched = Sched::FLAT;
+    int V = 1;          // elements per thread along the innermost parallel rank (FLAT)
+    std::vector<ParamField> fields;
+    int64_t rows = 1, cols = 1; // FLAT / OUTER_REDUCE index space; GRID_REDUCE/SCAN1D: cols = length
+    int nred = 0;               // GRID_REDUCE: number of reductions
+    int64_t scratch_bytes_per_tile = 0; // GRID_REDUCE: bytes of partials per tile (all reductions)
+    int64_t work_items() const;
+    // Bytes of arrays read/written by this unit (algorithmic, temporaries excluded).
+    int64_t algorithmic_bytes = 0;
+    int64_t elements = 0;
+};
+
+struct CodegenOptions {
+    bool bounds_check = false; // emit index checks that record violations instead of accessing
+    int flat_v = 4;            // elements per thread in FLAT
+};
+
+// Lower one kernel (as produced by jitk::get_kernel_list) into launch units executed in order.
+std::vector<LaunchUnit> lower_kernel(const jitk::LoopB &kernel, const CodegenOptions &opt);
+
+// CUDA element type name (the "long long" family is used for 64-bit integers).
+std::string cuda_type(bh_type t);
+
+} // namespace cuda
+} // namespace bohrium

@@ -1,0 +1,725 @@
+// B200 vector engine: memory, compilation, launching and the flush loop.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <stdexcept>
+#include <sys/stat.h>
+#include <unistd.h>
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <nvrtc.h>
+#include <bohrium/bh_main_memory.hpp>
+#include "engine.hpp"
+
+using namespace std;
+using namespace bohrium::jitk;
+
+namespace bohrium {
+namespace cuda {
+
+// ---------------------------------------------------------------------------------- errors
+namespace {
+void check(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) throw runtime_error(string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+void check_nvrtc(nvrtcResult r, const char *what) {
+    if (r != NVRTC_SUCCESS) throw runtime_error(string("NVRTC error in ") + what + ": " + nvrtcGetErrorString(r));
+}
+double seconds_since(chrono::steady_clock::time_point t0) {
+    return chrono::duration<double>(chrono::steady_clock::now() - t0).count();
+}
+uint64_t fnv1a(const void *data, size_t n, uint64_t h = 1469598103934665603ULL) {
+    const unsigned char *p = static_cast<const unsigned char *>(data);
+    for (size_t i = 0; i < n; ++i) {
+        h ^= p[i];
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+// Cheap 64-bit mixing for structural hashes.
+struct Hasher {
+    uint64_t h = 0x9E3779B97F4A7C15ULL;
+    void add(uint64_t v) {
+        v ^= v >> 33;
+        v *= 0xff51afd7ed558ccdULL;
+        v ^= v >> 33;
+        h = (h ^ v) * 0x100000001b3ULL + 0x9E3779B97F4A7C15ULL;
+    }
+};
+} // namespace
+
+// Driver entry points, fetched through the runtime so the library loads without libcuda.so
+// (the machine that builds it has no GPU driver).
+struct DeviceApi {
+    CUresult (*cuModuleLoadData)(CUmodule *, const void *) = nullptr;
+    CUresult (*cuModuleGetFunction)(CUfunction *, CUmodule, const char *) = nullptr;
+    CUresult (*cuLaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
+                               CUstream, void **, void **) = nullptr;
+    CUresult (*cuOccupancyMaxActiveBlocksPerMultiprocessor)(int *, CUfunction, int, size_t) = nullptr;
+    CUresult (*cuGetErrorString)(CUresult, const char **) = nullptr;
+
+    template <typename F>
+    void get(const char *name, F &fp) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        check(cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q), name);
+        if (p == nullptr || q != cudaDriverEntryPointSuccess) throw runtime_error(string("driver symbol not found: ") + name);
+        fp = reinterpret_cast<F>(p);
+    }
+    DeviceApi() {
+        get("cuModuleLoadData", cuModuleLoadData);
+        get("cuModuleGetFunction", cuModuleGetFunction);
+        get("cuLaunchKernel", cuLaunchKernel);
+        get("cuOccupancyMaxActiveBlocksPerMultiprocessor", cuOccupancyMaxActiveBlocksPerMultiprocessor);
+        get("cuGetErrorString", cuGetErrorString);
+    }
+    void ck(CUresult r, const char *what) const {
+        if (r != CUDA_SUCCESS) {
+            const char *s = "?";
+            if (cuGetErrorString) cuGetErrorString(r, &s);
+            throw runtime_error(string("CUDA driver error in ") + what + ": " + s);
+        }
+    }
+};
+
+// ------------------------------------------------------------------------------------- engine
+EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
+    const ConfigParser &cfg = comp.config;
+    prof = cfg.defaultGet<bool>("prof", false);
+    verbose = cfg.defaultGet<bool>("verbose", false);
+    fmad = cfg.defaultGet<bool>("fmad", false);
+    batch_mode = cfg.defaultGet<string>("batch", "off");
+    cg_opt.bounds_check = cfg.defaultGet<bool>("bounds_check", false);
+    cg_opt.flat_v = cfg.defaultGet<int>("elements_per_thread", 4);
+    // The GPU reduces over the outermost axis natively, so sweeps may fuse with maps at rank 0.
+    fusion_config = jitk::FusionConfig(cfg, false);
+    cache_dir = cfg.defaultGet<string>("cache_dir", "");
+    if (cache_dir == "NONE") cache_dir.clear();
+    _device = cfg.defaultGet<int>("device_number", 0);
+
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        throw runtime_error("Error: no devices supporting CUDA");
+    }
+    check(cudaSetDevice(_device), "cudaSetDevice");
+    check(cudaFree(nullptr), "context init");
+    cudaDeviceProp prop;
+    check(cudaGetDeviceProperties(&prop, _device), "cudaGetDeviceProperties");
+    _sm_count = prop.multiProcessorCount;
+    api.reset(new DeviceApi());
+    cudaStream_t s;
+    check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+    _stream = s;
+    // Keep freed device memory in the pool (exact reuse across flushes).
+    cudaMemPool_t pool;
+    check(cudaDeviceGetDefaultMemPool(&pool, _device), "cudaDeviceGetDefaultMemPool");
+    uint64_t threshold = UINT64_MAX;
+    const int64_t limit_pct = cfg.defaultGet<int64_t>("malloc_cache_limit", 90);
+    if (limit_pct < 0 || limit_pct > 100) throw runtime_error("config: `malloc_cache_limit` must be between 0 and 100");
+    threshold = static_cast<uint64_t>(static_cast<double>(prop.totalGlobalMem) * (limit_pct / 100.0));
+    check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold), "cudaMemPoolSetAttribute");
+    check(cudaMalloc(&counters, 4096 * sizeof(unsigned int)), "cudaMalloc(counters)");
+    check(cudaMemset(counters, 0, 4096 * sizeof(unsigned int)), "cudaMemset(counters)");
+    check(cudaMalloc(&err_record, sizeof(unsigned long long)), "cudaMalloc(err)");
+    check(cudaMemset(err_record, 0, sizeof(unsigned long long)), "cudaMemset(err)");
+    if (!cache_dir.empty()) mkdir(cache_dir.c_str(), 0755);
+}
+
+EngineCUDA::~EngineCUDA() {
+    try {
+        cudaStreamSynchronize(static_cast<cudaStream_t>(_stream));
+        for (auto &kv : buffers)
+            if (kv.second.ptr) cudaFree(kv.second.ptr);
+        if (scratch) cudaFree(scratch);
+        if (counters) cudaFree(counters);
+        if (err_record) cudaFree(err_record);
+        cudaStreamDestroy(static_cast<cudaStream_t>(_stream));
+    } catch (...) {
+    }
+}
+
+void EngineCUDA::synchronize() { check(cudaStreamSynchronize(static_cast<cudaStream_t>(_stream)), "cudaStreamSynchronize"); }
+
+// ------------------------------------------------------------------------------------- memory
+void EngineCUDA::copyToDevice(bh_base *base) {
+    if (buffers.count(base)) return;
+    DevBuf b;
+    b.nbytes = base->nbytes();
+    if (b.nbytes > 0) {
+        check(cudaMallocAsync(&b.ptr, static_cast<size_t>(b.nbytes), static_cast<cudaStream_t>(_stream)),
+              "cudaMallocAsync");
+        if (base->getDataPtr() != nullptr) {
+            check(cudaMemcpyAsync(b.ptr, base->getDataPtr(), static_cast<size_t>(b.nbytes), cudaMemcpyHostToDevice,
+                                  static_cast<cudaStream_t>(_stream)),
+                  "cudaMemcpyAsync(H2D)");
+            _stats.bytes_h2d += static_cast<uint64_t>(b.nbytes);
+        }
+    }
+    buffers[base] = b;
+}
+
+void *EngineCUDA::getBuffer(bh_base *base) {
+    copyToDevice(base);
+    return buffers.at(base).ptr;
+}
+
+void EngineCUDA::delBuffer(bh_base *base) {
+    auto it = buffers.find(base);
+    if (it == buffers.end()) return;
+    if (it->second.ptr) {
+        if (it->second.external) {
+            synchronize();
+            cudaFree(it->second.ptr);
+        } else {
+            check(cudaFreeAsync(it->second.ptr, static_cast<cudaStream_t>(_stream)), "cudaFreeAsync");
+        }
+    }
+    buffers.erase(it);
+    host_stale.erase(base);
+}
+
+void EngineCUDA::free_base(bh_base *base) {
+    delBuffer(base);
+    void *p = base->getDataPtr();
+    if (p == nullptr) return;
+    auto it = pinned.find(p);
+    if (it != pinned.end()) {
+        // Copies from page-locked memory are asynchronous: wait before releasing it.
+        synchronize();
+        cudaFreeHost(p);
+        pinned.erase(it);
+        base->resetDataPtr(nullptr);
+    } else {
+        // Copies from pageable memory are staged before cudaMemcpyAsync returns.
+        bh_data_free(base);
+    }
+}
+
+void *EngineCUDA::host_alloc(int64_t nbytes) {
+    void *p = nullptr;
+    check(cudaMallocHost(&p, static_cast<size_t>(max<int64_t>(nbytes, 1))), "cudaMallocHost");
+    pinned.insert(p);
+    return p;
+}
+
+void EngineCUDA::record_execute_begin() {
+    if (!ev_begin) {
+        cudaEvent_t a, b;
+        check(cudaEventCreate(&a), "cudaEventCreate");
+        check(cudaEventCreate(&b), "cudaEventCreate");
+        ev_begin = a;
+        ev_end = b;
+    }
+    check(cudaEventRecord(static_cast<cudaEvent_t>(ev_begin), static_cast<cudaStream_t>(_stream)), "cudaEventRecord");
+}
+
+void EngineCUDA::record_execute_end() {
+    check(cudaEventRecord(static_cast<cudaEvent_t>(ev_end), static_cast<cudaStream_t>(_stream)), "cudaEventRecord");
+}
+
+double EngineCUDA::last_execute_ms() {
+    if (!ev_begin) return 0.0;
+    check(cudaEventSynchronize(static_cast<cudaEvent_t>(ev_end)), "cudaEventSynchronize");
+    float ms = 0;
+    check(cudaEventElapsedTime(&ms, static_cast<cudaEvent_t>(ev_begin), static_cast<cudaEvent_t>(ev_end)),
+          "cudaEventElapsedTime");
+    return ms;
+}
+
+void EngineCUDA::copyToHost(const set<bh_base *> &bases, bool evict) {
+    bool any = false;
+    for (bh_base *base : bases) {
+        auto it = buffers.find(base);
+        if (it == buffers.end()) continue;
+        if (host_stale.count(base) || base->getDataPtr() == nullptr) {
+            bh_data_malloc(base);
+            if (it->second.nbytes > 0) {
+                check(cudaMemcpyAsync(base->getDataPtr(), it->second.ptr, static_cast<size_t>(it->second.nbytes),
+                                      cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(_stream)),
+                      "cudaMemcpyAsync(D2H)");
+                _stats.bytes_d2h += static_cast<uint64_t>(it->second.nbytes);
+                any = true;
+            }
+            host_stale.erase(base);
+        }
+    }
+    if (any) synchronize();
+    if (evict)
+        for (bh_base *base : bases) delBuffer(base);
+}
+
+void EngineCUDA::copyAllBasesToHost() {
+    set<bh_base *> all;
+    for (auto &kv : buffers) all.insert(kv.first);
+    copyToHost(all, true);
+}
+
+void *EngineCUDA::getMemoryPointer(bh_base &base, bool copy2host, bool force_alloc, bool nullify) {
+    if (copy2host) {
+        // The caller may write to the host data: the host copy becomes the master copy.
+        copyToHost({&base}, true);
+        if (force_alloc) bh_data_malloc(&base);
+        void *ret = base.getDataPtr();
+        if (nullify) base.resetDataPtr(nullptr);
+        return ret;
+    }
+    return getBuffer(&base);
+}
+
+void EngineCUDA::setMemoryPointer(bh_base *base, bool host_ptr, void *mem) {
+    if (host_ptr) {
+        delBuffer(base);
+        if (base->getDataPtr() != nullptr && base->getDataPtr() != mem) bh_data_free(base);
+        base->resetDataPtr(mem);
+    } else {
+        delBuffer(base);
+        DevBuf b;
+        b.ptr = mem;
+        b.nbytes = base->nbytes();
+        b.external = true;
+        buffers[base] = b;
+        host_stale.insert(base);
+    }
+}
+
+void *EngineCUDA::ensure_scratch(int64_t bytes) {
+    if (bytes <= scratch_bytes) return scratch;
+    const int64_t nb = max<int64_t>(bytes, max<int64_t>(scratch_bytes * 2, 1 << 20));
+    if (scratch) check(cudaFreeAsync(scratch, static_cast<cudaStream_t>(_stream)), "cudaFreeAsync(scratch)");
+    check(cudaMallocAsync(&scratch, static_cast<size_t>(nb), static_cast<cudaStream_t>(_stream)), "cudaMallocAsync(scratch)");
+    scratch_bytes = nb;
+    return scratch;
+}
+
+// ------------------------------------------------------------------------------- compilation
+void *EngineCUDA::function_for(const LaunchUnit &u) {
+    const uint64_t h = fnv1a(u.source.data(), u.source.size());
+    auto it = functions.find(h);
+    if (it != functions.end()) {
+        ++_stats.kernel_cache_hits;
+        return it->second;
+    }
+    ++_stats.kernel_cache_misses;
+    const auto t0 = chrono::steady_clock::now();
+    int nvrtc_major = 0, nvrtc_minor = 0;
+    nvrtcVersion(&nvrtc_major, &nvrtc_minor);
+    vector<string> opts = {"-arch=sm_100a", "-std=c++17", fmad ? "--fmad=true" : "--fmad=false", "-lineinfo"};
+    string key = u.source;
+    for (const string &o : opts) key += o;
+    key += to_string(nvrtc_major) + "." + to_string(nvrtc_minor);
+    const uint64_t disk_hash = fnv1a(key.data(), key.size());
+    vector<char> cubin;
+    string path;
+    if (!cache_dir.empty()) {
+        stringstream ss;
+        ss << cache_dir << "/" << hex << disk_hash << ".cubin";
+        path = ss.str();
+        ifstream in(path, ios::binary);
+        if (in) {
+            cubin.assign(istreambuf_iterator<char>(in), istreambuf_iterator<char>());
+            if (!cubin.empty()) ++_stats.disk_cache_hits;
+        }
+    }
+    if (cubin.empty()) {
+        nvrtcProgram prog;
+        check_nvrtc(nvrtcCreateProgram(&prog, u.source.c_str(), (u.name + ".cu").c_str(), 0, nullptr, nullptr),
+                    "nvrtcCreateProgram");
+        vector<const char *> copts;
+        for (const string &o : opts) copts.push_back(o.c_str());
+        const nvrtcResult r = nvrtcCompileProgram(prog, static_cast<int>(copts.size()), copts.data());
+        if (r != NVRTC_SUCCESS) {
+            size_t logsz = 0;
+            nvrtcGetProgramLogSize(prog, &logsz);
+            string log(logsz, '\0');
+            nvrtcGetProgramLog(prog, &log[0]);
+            nvrtcDestroyProgram(&prog);
+            throw runtime_error("NVRTC compilation of " + u.name + " failed:\n" + log + "\n--- source ---\n" + u.source);
+        }
+        size_t n = 0;
+        check_nvrtc(nvrtcGetCUBINSize(prog, &n), "nvrtcGetCUBINSize");
+        cubin.resize(n);
+        check_nvrtc(nvrtcGetCUBIN(prog, cubin.data()), "nvrtcGetCUBIN");
+        nvrtcDestroyProgram(&prog);
+        if (!path.empty()) {
+            const string tmp = path + ".tmp" + to_string(getpid());
+            ofstream out(tmp, ios::binary);
+            out.write(cubin.data(), static_cast<streamsize>(cubin.size()));
+            out.close();
+            rename(tmp.c_str(), path.c_str());
+        }
+    }
+    CUmodule mod;
+    api->ck(api->cuModuleLoadData(&mod, cubin.data()), "cuModuleLoadData");
+    CUfunction f;
+    api->ck(api->cuModuleGetFunction(&f, mod, u.name.c_str()), "cuModuleGetFunction");
+    functions[h] = reinterpret_cast<void *>(f);
+    int occ = 0;
+    const int threads = u.sched == Sched::SERIAL ? 32 : kThreads;
+    api->ck(api->cuOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, threads, 0), "cuOccupancy");
+    occupancy[reinterpret_cast<void *>(f)] = max(occ, 1);
+    _stats.time_compile += seconds_since(t0);
+    if (verbose) cerr << "[ve_cuda] compiled " << u.name << "\n" << u.source << endl;
+    return reinterpret_cast<void *>(f);
+}
+
+// ------------------------------------------------------------------------------------ launch
+vector<uint8_t> EngineCUDA::pack_params(const LaunchUnit &u) {
+    vector<uint8_t> buf(u.fields.size() * 8, 0);
+    int64_t scratch_need = 0;
+    if (u.sched == Sched::GRID_REDUCE) scratch_need = u.work_items() * u.scratch_bytes_per_tile;
+    if (u.sched == Sched::SCAN1D) scratch_need = u.work_items() * 16;
+    void *scr = scratch_need > 0 ? ensure_scratch(scratch_need) : scratch;
+    for (size_t i = 0; i < u.fields.size(); ++i) {
+        const ParamField &f = u.fields[i];
+        uint8_t *slot = &buf[i * 8];
+        switch (f.kind) {
+            case ParamField::PTR: {
+                void *p = getBuffer(f.base);
+                memcpy(slot, &p, 8);
+                break;
+            }
+            case ParamField::I64: memcpy(slot, &f.i64, 8); break;
+            case ParamField::CONST: memcpy(slot, &f.c.value, static_cast<size_t>(bh_type_size(f.c.type))); break;
+            case ParamField::R123_START: memcpy(slot, &f.c.value.r123.start, 8); break;
+            case ParamField::R123_KEY: memcpy(slot, &f.c.value.r123.key, 8); break;
+            case ParamField::SCRATCH: {
+                void *p = f.i64 == -1 ? static_cast<void *>(err_record) : scr;
+                memcpy(slot, &p, 8);
+                break;
+            }
+            case ParamField::COUNTER: {
+                void *p = counters;
+                memcpy(slot, &p, 8);
+                break;
+            }
+        }
+    }
+    return buf;
+}
+
+void EngineCUDA::launch(const LaunchUnit &u, const vector<uint8_t> &params, const string *) {
+    void *fv = function_for(u);
+    CUfunction f = reinterpret_cast<CUfunction>(fv);
+    const int64_t work = u.work_items();
+    int64_t grid = 1;
+    unsigned threads = kThreads;
+    if (u.sched == Sched::SERIAL) {
+        threads = 32;
+    } else {
+        const int64_t resident = static_cast<int64_t>(_sm_count) * occupancy[fv];
+        grid = max<int64_t>(1, min<int64_t>(work, resident));
+    }
+    if (work == 0) return;
+    void *args[] = {const_cast<uint8_t *>(params.data())};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (prof) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, static_cast<cudaStream_t>(_stream));
+    }
+    api->ck(api->cuLaunchKernel(f, static_cast<unsigned>(grid), 1, 1, threads, 1, 1, 0,
+                                static_cast<CUstream>(_stream), args, nullptr),
+            "cuLaunchKernel");
+    ++_stats.launches;
+    if (u.sched == Sched::SERIAL) ++_stats.serial_units;
+    if (prof) {
+        cudaEventRecord(e1, static_cast<cudaStream_t>(_stream));
+        cudaEventSynchronize(e1);
+        UnitRecord r;
+        r.name = u.name;
+        r.sched = u.sched;
+        r.elements = u.elements;
+        r.bytes = u.algorithmic_bytes;
+        cudaEventElapsedTime(&r.ms, e0, e1);
+        _stats.records.push_back(r);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+}
+
+void EngineCUDA::check_error_record() {
+    if (!cg_opt.bounds_check) return;
+    unsigned long long v = 0;
+    check(cudaMemcpyAsync(&v, err_record, sizeof(v), cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(_stream)),
+          "cudaMemcpyAsync(err)");
+    synchronize();
+    if (v != 0) {
+        check(cudaMemset(err_record, 0, sizeof(v)), "cudaMemset(err)");
+        last_error_index = v & 0x7fffffffffffffffULL;
+        throw runtime_error("bounds check: a generated kernel indexed element " + to_string(last_error_index) +
+                            " outside its array");
+    }
+}
+
+// ------------------------------------------------------------------------------- fuse cache
+namespace {
+// Structural hash of an instruction list: opcodes, sweep axes, the constant slot, and for every
+// view its base (numbered by first appearance), dtype, start (unless sliding), shape and stride.
+uint64_t hash_instr_list(const vector<bh_instruction *> &instr_list, vector<bh_base *> &base_ids) {
+    Hasher h;
+    unordered_map<const bh_base *, uint64_t> ids;
+    for (const bh_instruction *instr : instr_list) {
+        h.add(static_cast<uint64_t>(instr->opcode));
+        h.add(static_cast<uint64_t>(instr->sweep_axis()));
+        h.add(instr->constructor ? 1 : 0);
+        for (const bh_view &v : instr->operand) {
+            if (v.isConstant()) {
+                h.add(0xC0115747ULL);
+                continue;
+            }
+            auto it = ids.find(v.base);
+            uint64_t id;
+            if (it == ids.end()) {
+                id = ids.size();
+                ids[v.base] = id;
+                base_ids.push_back(v.base);
+            } else {
+                id = it->second;
+            }
+            h.add(id);
+            h.add(static_cast<uint64_t>(v.base->dtype()));
+            h.add(static_cast<uint64_t>(v.base->nelem()));
+            if (!v.hasSlide()) h.add(static_cast<uint64_t>(v.start));
+            h.add(static_cast<uint64_t>(v.ndim));
+            for (int64_t d = 0; d < v.ndim; ++d) {
+                h.add(static_cast<uint64_t>(v.shape[d]));
+                h.add(static_cast<uint64_t>(v.stride[d]));
+            }
+        }
+    }
+    h.add(instr_list.size());
+    return h.h;
+}
+
+void rebase(Block &block, const map<bh_base *, bh_base *> &cached2new,
+            const unordered_map<int64_t, const bh_instruction *> &origin) {
+    if (block.isInstr()) {
+        bh_instruction instr(*block.getInstr());
+        auto it = origin.find(instr.origin_id);
+        if (it == origin.end()) throw runtime_error("fuse cache: unknown origin id");
+        const bh_instruction *o = it->second;
+        for (size_t i = 0; i < instr.operand.size(); ++i) {
+            bh_view &v = instr.operand[i];
+            if (v.isConstant()) {
+                if (!bh_opcode_is_sweep(instr.opcode)) instr.constant = o->constant;
+            } else {
+                if (v.hasSlide()) v.start = o->operand[i].start;
+                v.base = cached2new.at(v.base);
+            }
+        }
+        instr.constructor = o->constructor;
+        block.setInstr(instr);
+    } else {
+        LoopB &loop = block.getLoop();
+        for (Block &b : loop._block_list) rebase(b, cached2new, origin);
+        set<bh_base *> frees;
+        for (bh_base *b : loop._frees) frees.insert(cached2new.at(b));
+        loop._frees = std::move(frees);
+        loop.metadataUpdate();
+    }
+}
+} // namespace
+
+vector<LoopB> EngineCUDA::kernels_for(vector<bh_instruction *> &instr_list) {
+    const auto t0 = chrono::steady_clock::now();
+    int64_t oc = 0;
+    for (bh_instruction *i : instr_list) i->origin_id = oc++;
+    vector<bh_base *> base_ids;
+    // Frees are part of the structure too (they decide contraction).
+    const uint64_t key = hash_instr_list(instr_list, base_ids);
+    vector<LoopB> kernels;
+    auto it = fuse_cache.find(key);
+    if (it != fuse_cache.end() && it->second.base_ids.size() == base_ids.size()) {
+        ++_stats.fuse_cache_hits;
+        map<bh_base *, bh_base *> cached2new;
+        for (size_t i = 0; i < base_ids.size(); ++i) cached2new[it->second.base_ids[i]] = base_ids[i];
+        unordered_map<int64_t, const bh_instruction *> origin;
+        for (const bh_instruction *i : instr_list) origin[i->origin_id] = i;
+        vector<Block> blocks = it->second.block_list;
+        for (Block &b : blocks) rebase(b, cached2new, origin);
+        kernels = get_kernel_list(instr_list, fusion_config, &blocks);
+    } else {
+        ++_stats.fuse_cache_misses;
+        vector<Block> blocks;
+        kernels = get_kernel_list(instr_list, fusion_config, nullptr, &blocks);
+        fuse_cache[key] = FusePayload{std::move(blocks), base_ids};
+    }
+    _stats.time_fusion += seconds_since(t0);
+    return kernels;
+}
+
+void EngineCUDA::setConstructorFlag(vector<bh_instruction *> &instr_list) {
+    // Arrays already on the device or with host data are not constructed by this flush.
+    set<const bh_base *> constructed;
+    for (auto &kv : buffers) constructed.insert(kv.first);
+    for (bh_instruction *instr : instr_list) {
+        instr->constructor = false;
+        for (size_t o = 0; o < instr->operand.size(); ++o) {
+            const bh_view &v = instr->operand[o];
+            if (v.isConstant()) continue;
+            if (o == 0 && !constructed.count(v.base) && v.base->getDataPtr() == nullptr) instr->constructor = true;
+            constructed.insert(v.base);
+        }
+    }
+}
+
+void EngineCUDA::run_kernels(const vector<LoopB> &kernels) {
+    for (const LoopB &kernel : kernels) {
+        ++_stats.kernels;
+        if (!kernel.isSystemOnly()) {
+            const auto tc = chrono::steady_clock::now();
+            const vector<LaunchUnit> units = lower_kernel(kernel, cg_opt);
+            _stats.time_codegen += seconds_since(tc);
+            for (const LaunchUnit &u : units) {
+                const vector<uint8_t> params = pack_params(u);
+                launch(u, params);
+            }
+            // Everything written by the kernel is newer on the device.
+            for (const InstrPtr &instr : all_instr(kernel)) {
+                if (!instr->operand.empty() && !instr->operand[0].isConstant()) host_stale.insert(instr->operand[0].base);
+            }
+        }
+        for (bh_base *base : kernel.getAllFrees()) free_base(base);
+    }
+}
+
+void EngineCUDA::handleExecution(BhIR *bhir) {
+    const auto t0 = chrono::steady_clock::now();
+    set<bh_base *> frees;
+    vector<bh_instruction *> instr_list = remove_non_computed_system_instr(bhir->instr_list, frees);
+    for (bh_base *base : frees) free_base(base);
+    setConstructorFlag(instr_list);
+    const vector<LoopB> kernels = kernels_for(instr_list);
+    run_kernels(kernels);
+    copyToHost(bhir->getSyncs(), false);
+    check_error_record();
+    _stats.time_exec_host += seconds_since(t0);
+}
+
+void EngineCUDA::handleExtmethod(BhIR *bhir) {
+    vector<bh_instruction> instr_list;
+    for (bh_instruction &instr : bhir->instr_list) {
+        auto ext = comp.extmethods.find(instr.opcode);
+        auto childext = comp.child_extmethods.find(instr.opcode);
+        if (ext != comp.extmethods.end() || childext != comp.child_extmethods.end()) {
+            BhIR b(std::move(instr_list), bhir->getSyncs());
+            handleExecution(&b);
+            instr_list.clear();
+            if (ext != comp.extmethods.end()) {
+                ext->second.execute(&instr, this);
+                for (const bh_view &v : instr.operand)
+                    if (!v.isConstant() && &v == &instr.operand[0]) host_stale.insert(v.base);
+            } else {
+                set<bh_base *> bases = instr.get_bases();
+                copyToHost(bases, true);
+                vector<bh_instruction> child_list{instr};
+                BhIR cb(std::move(child_list), bhir->getSyncs());
+                comp.child.execute(&cb);
+            }
+        } else {
+            instr_list.push_back(instr);
+        }
+    }
+    bhir->instr_list = instr_list;
+}
+
+namespace {
+// Slide views between repeats of flush-and-repeat (include/bohrium/jitk/engines/dyn_view.hpp:21-67).
+void slide_views(BhIR *bhir) {
+    for (bh_instruction &instr : bhir->instr_list) {
+        for (bh_view &view : instr.operand) {
+            if (!view.hasSlide()) continue;
+            for (const bh_slide_dim &dim : view.slides.dims) {
+                if (dim.step_delay == 1 || (view.slides.iteration_counter % dim.step_delay == dim.step_delay - 1)) {
+                    if (dim.stride) {
+                        int64_t change = dim.offset_change * dim.stride;
+                        const int64_t max_rel_idx = dim.stride * dim.shape;
+                        int64_t rel_idx = view.start % (dim.stride * dim.shape);
+                        rel_idx += change;
+                        if (rel_idx < 0) {
+                            change += max_rel_idx;
+                        } else if (rel_idx >= max_rel_idx) {
+                            change -= max_rel_idx;
+                        }
+                        view.start += change;
+                        auto it = view.slides.resets.find(dim.rank);
+                        if (it != view.slides.resets.end()) {
+                            const int64_t reset_at = it->second.first;
+                            int64_t &changes_since_reset = it->second.second;
+                            changes_since_reset += change;
+                            if (view.slides.iteration_counter > 0 &&
+                                (view.slides.iteration_counter / dim.step_delay) % reset_at == reset_at - 1) {
+                                view.start -= changes_since_reset;
+                                changes_since_reset = 0;
+                                view.shape[dim.rank] -= reset_at * dim.shape_change;
+                            }
+                        }
+                    }
+                    view.shape[dim.rank] += dim.shape_change;
+                    if (view.shape[dim.rank] < 0) view.shape[dim.rank] = 0;
+                }
+            }
+            view.slides.iteration_counter += 1;
+        }
+    }
+}
+} // namespace
+
+void EngineCUDA::execute(BhIR *bhir) {
+    ++_stats.flushes;
+    bh_base *cond = bhir->getRepeatCondition();
+    for (uint64_t i = 0; i < bhir->getNRepeats(); ++i) {
+        handleExtmethod(bhir);
+        handleExecution(bhir);
+        if (cond != nullptr) {
+            copyToHost({cond}, false);
+            if (cond->getDataPtr() != nullptr && !static_cast<bool *>(cond->getDataPtr())[0]) break;
+        }
+        slide_views(bhir);
+    }
+}
+
+// ------------------------------------------------------------------------------------ reports
+string EngineCUDA::info() const {
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, _device);
+    int nv_major = 0, nv_minor = 0;
+    nvrtcVersion(&nv_major, &nv_minor);
+    stringstream ss;
+    ss << "----\nCUDA (B200 engine):\n";
+    ss << "  Device: " << prop.name << " (SM " << prop.major << "." << prop.minor << ", " << prop.multiProcessorCount
+       << " SMs)\n";
+    ss << "  Memory: " << prop.totalGlobalMem / 1024 / 1024 << " MB\n";
+    ss << "  JIT: NVRTC " << nv_major << "." << nv_minor << " -arch=sm_100a" << (fmad ? "" : " --fmad=false") << "\n";
+    ss << "  Cache dir: " << (cache_dir.empty() ? "NONE" : cache_dir) << "\n";
+    ss << "  Batch mode: " << batch_mode << "\n";
+    return ss.str();
+}
+
+string EngineCUDA::statistics() const {
+    stringstream ss;
+    ss << "flushes: " << _stats.flushes << "\nkernels: " << _stats.kernels << "\nlaunches: " << _stats.launches
+       << "\ngrouped_launches: " << _stats.grouped_launches << "\ngraph_replays: " << _stats.graph_replays
+       << "\nserial_units: " << _stats.serial_units << "\nfuse_cache_hits: " << _stats.fuse_cache_hits
+       << "\nfuse_cache_misses: " << _stats.fuse_cache_misses << "\nkernel_cache_hits: " << _stats.kernel_cache_hits
+       << "\nkernel_cache_misses: " << _stats.kernel_cache_misses << "\ndisk_cache_hits: " << _stats.disk_cache_hits
+       << "\nbytes_h2d: " << _stats.bytes_h2d << "\nbytes_d2h: " << _stats.bytes_d2h
+       << "\ntime_fusion: " << _stats.time_fusion << "\ntime_codegen: " << _stats.time_codegen
+       << "\ntime_compile: " << _stats.time_compile << "\ntime_exec_host: " << _stats.time_exec_host << "\n";
+    if (!_stats.records.empty()) {
+        ss << "units:\n";
+        for (const UnitRecord &r : _stats.records)
+            ss << "  - {name: " << r.name << ", sched: " << sched_name(r.sched) << ", elements: " << r.elements
+               << ", bytes: " << r.bytes << ", ms: " << r.ms << "}\n";
+    }
+    return ss.str();
+}
+
+void EngineCUDA::resetStatistics() { _stats = Stats(); }
+
+} // namespace cuda
+} // namespace bohrium

@@ -1,0 +1,27 @@
+// The Bohrium Internal Representation: one flushed batch of instructions.
+// Fields follow include/bohrium/bh_ir.hpp:30-107 of the reference. Boost serialisation is not
+// provided; a flat wire encoding for foreign callers is declared in include/bh_b200.h.
+#pragma once
+
+#include <cstdint>
+#include <set>
+#include <vector>
+#include <bohrium/bh_instruction.hpp>
+
+class BhIR {
+public:
+    std::vector<bh_instruction> instr_list;
+    std::set<bh_base *> _syncs;
+    uint64_t _nrepeats;
+    // Repeat while this single BH_BOOL element is true (nullptr: no condition).
+    bh_base *_repeat_condition;
+
+    BhIR(std::vector<bh_instruction> instr_list, std::set<bh_base *> syncs, uint64_t nrepeats = 1,
+         bh_base *repeat_condition = nullptr)
+        : instr_list(std::move(instr_list)), _syncs(std::move(syncs)), _nrepeats(nrepeats),
+          _repeat_condition(repeat_condition) {}
+
+    const std::set<bh_base *> getSyncs() const { return _syncs; }
+    uint64_t getNRepeats() const { return _nrepeats; }
+    bh_base *getRepeatCondition() { return _repeat_condition; }
+};
