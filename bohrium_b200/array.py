@@ -59,8 +59,10 @@ class BhArray:
         return int(np.prod(self.shape, dtype=np.int64)) if self.shape else 1
 
     def view(self) -> ir.View:
+        # Zero-dimensional arrays travel as one-element 1-D views, as the reference's bridge sends
+        # them (bridge/npbackend/src/bharray.c:41-45).
         if self.ndim == 0:
-            return ir.View(self.base, self.start, (), ())
+            return ir.View(self.base, self.start, (1,), (1,))
         return ir.View(self.base, self.start, self.shape, self.strides)
 
     def _root(self):

@@ -662,10 +662,43 @@ string pointer_locals(const Symbols &sym) {
     return ss.str();
 }
 
-int64_t unit_bytes(const Symbols &sym) {
-    int64_t b = 0;
-    for (const bh_view &v : sym.views) b += v.shape.prod() * bh_type_size(v.base->dtype());
-    return b;
+// Algorithmic bytes of a unit: for every non-temporary base, the bytes of its distinct views that
+// are read plus those that are written, each capped at the base's size (overlapping views such as
+// the shifted views of a stencil count once).
+int64_t unit_bytes(const Symbols &sym, const vector<InstrPtr> &instrs) {
+    map<const bh_base *, set<bh_view>> reads, writes;
+    for (const InstrPtr &instr : instrs) {
+        if (bh_opcode_is_system(instr->opcode)) continue;
+        for (size_t o = 0; o < instr->operand.size(); ++o) {
+            const bh_view &v = instr->operand[o];
+            if (v.isConstant() || sym.temps.count(v.base)) continue;
+            const bool write = o == 0 && instr->opcode != BH_GATHER;
+            (write ? writes : reads)[v.base].insert(v);
+            if (instr->opcode == BH_SCATTER || instr->opcode == BH_COND_SCATTER || bh_opcode_is_accumulate(instr->opcode))
+                if (o == 0) reads[v.base].insert(v);
+        }
+    }
+    int64_t total = 0;
+    for (auto *m : {&reads, &writes}) {
+        for (const auto &kv : *m) {
+            int64_t b = 0;
+            for (const bh_view &v : kv.second) b += v.shape.prod() * bh_type_size(v.base->dtype());
+            total += min<int64_t>(b, kv.first->nbytes());
+        }
+    }
+    return total;
+}
+
+int64_t unit_bytes(const Symbols &sym, const vector<const Block *> &items) {
+    vector<InstrPtr> instrs;
+    for (const Block *b : items) {
+        if (b->isInstr()) {
+            instrs.push_back(b->getInstr());
+        } else {
+            jitk::all_instr(b->getLoop(), instrs);
+        }
+    }
+    return unit_bytes(sym, instrs);
 }
 
 // ------------------------------------------------------------------------------------ schedules
@@ -691,7 +724,7 @@ LaunchUnit lower_serial(const vector<const Block *> &items, const CodegenOptions
     em.write_body(pseudo, scope, 4);
     body << "}\n";
     u.fields = pl2.fields;
-    u.algorithmic_bytes = unit_bytes(sym);
+    u.algorithmic_bytes = unit_bytes(sym, pitems);
     finish_source(u, pl2.decl.str(), body.str(), opt);
     return u;
 }
@@ -760,7 +793,7 @@ LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) 
     em.write_body(inner, scope, 12);
     body << "        }\n    }\n}\n";
     u.fields = pl.fields;
-    u.algorithmic_bytes = unit_bytes(sym);
+    u.algorithmic_bytes = unit_bytes(sym, items);
     u.elements = rows * u.cols;
     finish_source(u, pl.decl.str(), body.str(), opt);
     return u;
@@ -879,7 +912,7 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
     body << "    if (threadIdx.x == 0) *p.counter = 0u;\n";
     body << "}\n";
     u.fields = pl.fields;
-    u.algorithmic_bytes = unit_bytes(sym);
+    u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
     u.elements = L.size;
     finish_source(u, pl.decl.str(), body.str(), opt);
     return u;
@@ -979,7 +1012,7 @@ LaunchUnit lower_outer_reduce(const LoopB &loop, const vector<const Block *> &id
     }
     body << "    }\n}\n";
     u.fields = pl.fields;
-    u.algorithmic_bytes = unit_bytes(sym);
+    u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
     u.elements = rows * inner.size * L.size;
     finish_source(u, pl.decl.str(), body.str(), opt);
     return u;

@@ -1,0 +1,110 @@
+"""Device-free checks of the engine's lowering: fusion plan, schedules, NVRTC compilation."""
+import numpy as np
+import pytest
+
+import bohrium_b200 as bh
+from bohrium_b200 import workloads as W
+from tests import programs as P
+
+
+def plan(prog, compile=True, fuser_list=None):
+    ex = bh.DryRunExecutor()
+    rt = bh.Runtime(ex)
+    outs = prog(rt)
+    flush = rt.take()
+    flush.syncs = [o.base for o in outs]
+    res = bh.dry_run(flush, compile=compile, fuser_list=fuser_list)
+    units = [u for k in res["kernels"] for u in k["units"]]
+    for u in units:
+        assert u["compile_error"] == "", u["compile_error"][:3000]
+    return res, units
+
+
+def test_plain_chain_is_one_grid_reduction():
+    def prog(rt):
+        a, b, c = (bh.empty(rt, (1 << 20,), np.float64) for _ in range(3))
+        return [W.plain_chain(rt, a, b, c)]
+    res, units = plan(prog)
+    assert [u["sched"] for u in units] == ["grid_reduce"]
+    # the whole chain is contracted: only the three inputs and the scalar are read/written
+    assert units[0]["bytes"] == 3 * 8 * (1 << 20) + 8
+
+
+def test_black_scholes_iteration_is_one_kernel():
+    def prog(rt):
+        S, K, T = (bh.empty(rt, (10000,), np.float64) for _ in range(3))
+        return [W.black_scholes_iteration(rt, S, K, T, 0)]
+    res, units = plan(prog)
+    scheds = [u["sched"] for u in units]
+    assert scheds.count("grid_reduce") == 1 and len(units) <= 2, scheds
+
+
+def test_heat_step_fuses_stencil_write_and_partial_max():
+    def prog(rt):
+        a = bh.empty(rt, (64, 64), np.float32)
+        b = bh.empty(rt, (64, 64), np.float32)
+        return [W.heat_step(a, b), b]
+    res, units = plan(prog)
+    scheds = [u["sched"] for u in units]
+    assert scheds == ["flat", "grid_reduce"], scheds
+
+
+def test_batching_systems_lower_to_one_unit_each():
+    def prog(rt):
+        outs = []
+        for n in [300, 1000, 4097]:
+            x = bh.empty(rt, (n,), np.float32)
+            y = W.batching_chain(x)
+            outs += [y, y.sum(), y.max()]
+        return outs
+    res, units = plan(prog)
+    assert [u["sched"] for u in units] == ["grid_reduce"] * 3
+    # one compiled kernel serves every length
+    assert len({u["name"] for u in units}) == 1
+
+
+@pytest.mark.parametrize("name", ["ADD", "DIVIDE", "REMAINDER", "POWER", "RIGHT_SHIFT", "MAXIMUM"])
+@pytest.mark.parametrize("dtype", [np.int8, np.int64, np.uint32, np.float32])
+def test_binary_opcodes_compile(name, dtype):
+    if np.dtype(dtype) not in [np.dtype(t) for t in P.BINARY[name]]:
+        pytest.skip("signature not defined")
+    plan(P.binary_program(name, dtype, n=64))
+
+
+@pytest.mark.parametrize("name", P.UNARY_FLOAT + ["ABSOLUTE", "SIGN", "ISNAN"])
+def test_unary_opcodes_compile(name):
+    plan(P.unary_program(name, np.float64, n=64))
+
+
+@pytest.mark.parametrize("name", P.REDUCE_OPS)
+def test_reductions_compile(name):
+    dt = np.bool_ if name.startswith("LOGICAL") else (np.int32 if "BITWISE" in name else np.float32)
+    plan(P.reduce_program(name, dt, (33, 65), None))
+
+
+def test_views_random_gather_scatter_compile():
+    for prog in [P.views_program(), P.random_program((100,), 1, 2), P.gather_scatter_program(100),
+                 P.range_program(100), P.fused_chain_program(1024),
+                 P.accumulate_program("ADD_ACCUMULATE", np.float64, (8, 9), 1),
+                 P.accumulate_program("MULTIPLY_ACCUMULATE", np.int64, (40,), 0)]:
+        plan(prog)
+
+
+def test_outer_axis_reduction_runs_on_gpu_without_swap():
+    """Without push_reductions_inwards an axis-0 reduction sweeps rank 0; it must still lower to a
+    GPU schedule (the reference offloads such blocks to the CPU)."""
+    prog = P.reduce_program("ADD_REDUCE", np.float64, (100, 7, 5), 0)
+    res, units = plan(prog, fuser_list="greedy,collapse_redundant_axes")
+    assert "outer_reduce" in [u["sched"] for u in units]
+
+
+def test_bounds_are_parameters_not_constants():
+    """Loop sizes, offsets and strides are kernel parameters: shapes share compiled kernels."""
+    names = set()
+    for n in [1000, 2000, 12345]:
+        def prog(rt, n=n):
+            a = bh.empty(rt, (n,), np.float32)
+            return [bh.sqrt(a) + 1]
+        _, units = plan(prog, compile=False)
+        names.add(units[0]["name"])
+    assert len(names) == 1

@@ -1,0 +1,171 @@
+"""Parity of the CUDA engine with the CPU oracle (the restated ve/openmp) on the same bytecode.
+
+Integer, boolean and random outputs must be bit-exact. Elementwise floating-point results may
+differ by a few ulps (CUDA's vs glibc's math functions, FMA contraction on the CPU), reductions by
+the change of summation order: 1e-5 relative for float32 and 1e-12 for float64.
+"""
+import numpy as np
+import pytest
+
+import bohrium_b200 as bh
+from tests import programs as P
+from tests.harness import assert_close, float_tol, reduce_tol, run
+
+pytestmark = pytest.mark.gpu
+
+
+def both(gpu_rt, oracle_rt, prog):
+    return run(gpu_rt, prog), run(oracle_rt, prog)
+
+
+@pytest.mark.parametrize("name", sorted(P.BINARY))
+def test_binary_opcodes(gpu_rt, oracle_rt, name):
+    for dt in P.BINARY[name]:
+        g, o = both(gpu_rt, oracle_rt, P.binary_program(name, dt, n=777))
+        rtol, atol = float_tol(dt, name in P.TRANSCENDENTAL)
+        for k in range(2):
+            assert_close(g[k], o[k], rtol, atol, f"{name} {np.dtype(dt)}")
+
+
+@pytest.mark.parametrize("name", P.COMPARE)
+def test_comparisons(gpu_rt, oracle_rt, name):
+    for dt in P.INT_TYPES + P.FLOAT_TYPES:
+        g, o = both(gpu_rt, oracle_rt, P.compare_program(name, dt, n=500))
+        assert_close(g[0], o[0], 0, 0, f"{name} {np.dtype(dt)}")
+
+
+@pytest.mark.parametrize("name", P.LOGICAL)
+def test_logical(gpu_rt, oracle_rt, name):
+    g, o = both(gpu_rt, oracle_rt, P.logical_program(name, n=500))
+    assert_close(g[0], o[0], 0, 0, name)
+
+
+@pytest.mark.parametrize("name", P.UNARY_FLOAT)
+def test_unary_float(gpu_rt, oracle_rt, name):
+    for dt in P.FLOAT_TYPES:
+        g, o = both(gpu_rt, oracle_rt, P.unary_program(name, dt, n=1000))
+        rtol, atol = float_tol(dt, name in P.TRANSCENDENTAL)
+        assert_close(g[0], o[0], rtol, atol, f"{name} {np.dtype(dt)}")
+
+
+@pytest.mark.parametrize("name", P.UNARY_ANY)
+def test_unary_any(gpu_rt, oracle_rt, name):
+    types = {"INVERT": P.INT_TYPES + [np.bool_], "LOGICAL_NOT": [np.bool_]}.get(
+        name, P.INT_TYPES + P.FLOAT_TYPES)
+    for dt in types:
+        g, o = both(gpu_rt, oracle_rt, P.unary_program(name, dt, n=500))
+        assert_close(g[0], o[0], 0, 0, f"{name} {np.dtype(dt)}")
+
+
+def test_type_conversions(gpu_rt, oracle_rt):
+    types = [np.bool_, np.int8, np.int32, np.int64, np.uint8, np.uint64, np.float32, np.float64]
+    for s in types:
+        for d in types:
+            if s == d:
+                continue
+            g, o = both(gpu_rt, oracle_rt, P.identity_program(s, d))
+            assert_close(g[0], o[0], 0, 0, f"{np.dtype(s)}->{np.dtype(d)}")
+
+
+@pytest.mark.parametrize("name", P.REDUCE_OPS)
+@pytest.mark.parametrize("shape,axis", [((1000,), 0), ((37, 53), 0), ((37, 53), 1), ((37, 53), None),
+                                        ((5, 6, 7), 1), ((5, 6, 7), 2), ((3, 4, 5, 6), 0)])
+def test_reductions(gpu_rt, oracle_rt, name, shape, axis):
+    if name.startswith("LOGICAL"):
+        types = [np.bool_]
+    elif name.startswith("BITWISE"):
+        types = [np.int32, np.uint64, np.bool_]
+    else:
+        types = [np.int64, np.float32, np.float64]
+    for dt in types:
+        g, o = both(gpu_rt, oracle_rt, P.reduce_program(name, dt, shape, axis))
+        assert_close(g[0], o[0], reduce_tol(dt), 0, f"{name} {np.dtype(dt)} {shape} axis={axis}")
+
+
+@pytest.mark.parametrize("view", ["transposed", "sliced", "reversed"])
+@pytest.mark.parametrize("axis", [0, 1, None])
+def test_reductions_of_views(gpu_rt, oracle_rt, view, axis):
+    g, o = both(gpu_rt, oracle_rt, P.reduce_program("ADD_REDUCE", np.float64, (40, 30), axis, view))
+    assert_close(g[0], o[0], 1e-12, 0, f"{view} axis={axis}")
+
+
+def test_large_and_ragged_reductions(gpu_rt, oracle_rt):
+    # lengths around the tile size (2048) and the grid size, and a long one
+    for n in [1, 2, 255, 2047, 2048, 2049, 300001, 3_000_017]:
+        g, o = both(gpu_rt, oracle_rt, P.reduce_program("ADD_REDUCE", np.float64, (n,), None))
+        assert_close(g[0], o[0], 1e-12, 0, f"sum n={n}")
+        g, o = both(gpu_rt, oracle_rt, P.reduce_program("MAXIMUM_REDUCE", np.int32, (n,), None))
+        assert_close(g[0], o[0], 0, 0, f"max n={n}")
+
+
+@pytest.mark.parametrize("name", ["ADD_ACCUMULATE", "MULTIPLY_ACCUMULATE"])
+@pytest.mark.parametrize("shape,axis", [((1000,), 0), ((20, 30), 0), ((20, 30), 1), ((4, 5, 6), 2)])
+def test_accumulate(gpu_rt, oracle_rt, name, shape, axis):
+    for dt in [np.int64, np.float64]:
+        g, o = both(gpu_rt, oracle_rt, P.accumulate_program(name, dt, shape, axis))
+        assert_close(g[0], o[0], 1e-12, 0, f"{name} {np.dtype(dt)} {shape} {axis}")
+
+
+def test_views_and_broadcast(gpu_rt, oracle_rt):
+    g, o = both(gpu_rt, oracle_rt, P.views_program())
+    for k in range(3):
+        assert_close(g[k], o[k], 1e-14, 1e-15, f"views[{k}]")
+
+
+@pytest.mark.parametrize("shape,start,key", [((1000,), 0, 42), ((33, 17), 12345, 7), ((5000,), 2**32 - 100, 2**40)])
+def test_random_is_bit_exact(gpu_rt, oracle_rt, shape, start, key):
+    g, o = both(gpu_rt, oracle_rt, P.random_program(shape, start, key))
+    assert_close(g[0], o[0], 0, 0, "random123")
+    assert_close(g[1], o[1], 0, 0, "random_sample float32")
+
+
+def test_random_matches_reference_golden(gpu_rt):
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "random123.json")) as f:
+        cases = json.load(f)["cases"]
+    for case in cases:
+        r = bh.random123(gpu_rt, (len(case["values"]),), case["start"], case["key"]).numpy()
+        assert r.tolist() == case["values"]
+
+
+def test_gather_scatter_range(gpu_rt, oracle_rt):
+    g, o = both(gpu_rt, oracle_rt, P.gather_scatter_program(2000))
+    assert_close(g[0], o[0], 0, 0, "gather")
+    assert_close(g[1], o[1], 0, 0, "scatter")
+    g, o = both(gpu_rt, oracle_rt, P.range_program(3000))
+    assert_close(g[0], o[0], 0, 0, "range")
+    assert_close(g[1], o[1], 0, 0, "range view")
+
+
+@pytest.mark.parametrize("n", [4, 1024, 4096 * 3 + 4, 1 << 20])
+def test_fused_chain(gpu_rt, oracle_rt, n):
+    g, o = both(gpu_rt, oracle_rt, P.fused_chain_program(n))
+    rtol = float_tol(np.float64, True)
+    assert_close(g[0], o[0], *rtol, "map")
+    for k in range(1, 5):
+        assert_close(g[k], o[k], 1e-12, 1e-12, f"reduction[{k}]")
+
+
+def test_empty_arrays(gpu_rt, oracle_rt):
+    g, o = both(gpu_rt, oracle_rt, P.empty_program())
+    assert g[0].shape == o[0].shape == (0,)
+
+
+def test_repeat_with_condition_and_slides(gpu_rt, oracle_rt):
+    """flush-and-repeat with a sliding view and a repeat condition (test/python/tests/test_loop.py)."""
+    from bohrium_b200 import ir
+    results = []
+    for rt in (gpu_rt, oracle_rt):
+        A = np.arange(20, dtype=np.float64)
+        a = bh.array(rt, A)
+        acc = bh.zeros(rt, (1,), np.float64)
+        cond = bh.ones(rt, (1,), np.bool_)
+        rt.flush()
+        add = ir.Instr(ir.OPCODES["ADD"], [acc.view(), acc.view(), ir.View(a.base, 0, (1,), (1,))])
+        add.slides[2] = ([ir.Slide(0, 1, 0, 1, 20)], {})
+        # keep going while acc < 50
+        less = ir.Instr(ir.OPCODES["LESS"], [cond.view(), acc.view(), None], ir.Constant(50.0, ir.FLOAT64))
+        rt.ex.execute(ir.Flush([add, less], nrepeats=20, condition=cond.base))
+        results.append(acc.numpy()[0])
+    assert results[0] == results[1] == float(sum(range(11)))
