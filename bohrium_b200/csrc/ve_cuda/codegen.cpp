@@ -107,7 +107,23 @@ template <typename T> __device__ __forceinline__ T bh_shfl_xor(T v, int m) {
     }
 }
 
-__device__ __forceinline__ bh_i64 bh_floordiv_i64(bh_i64 a, bh_i64 b) { return a / b; }
+// Integer power by repeated squaring: exact wherever the result fits the type (CUDA's double pow
+// can be an ulp below an exact integer, which truncation would turn into the wrong integer).
+// Negative exponents give what pow() truncates to: 1 for a base of 1, +-1 for -1, else 0.
+template <typename T> __device__ __forceinline__ T bh_ipow(T b, T e) {
+    if (e < (T)0) {
+        if (b == (T)1) return (T)1;
+        if (b == (T)-1) return (e & (T)1) ? (T)-1 : (T)1;
+        return (T)0;
+    }
+    T r = (T)1;
+    while (e) {
+        if (e & (T)1) r = (T)(r * b);
+        e = (T)(e >> 1);
+        b = (T)(b * b);
+    }
+    return r;
+}
 )CUDA";
 
 // ---------------------------------------------------------------------------- operation emitting
@@ -161,8 +177,9 @@ string op_statement(const bh_instruction &instr, const vector<string> &ops) {
             }
             return bin("/");
         case BH_POWER:
-            if (bh_type_is_integer(t0) || t0 == bh_type::BOOL)
-                return o + " = pow((double)" + ops[1] + ", (double)" + ops[2] + ");";
+            if (t0 == bh_type::BOOL) return o + " = !" + ops[2] + " || " + ops[1] + ";";
+            if (bh_type_is_integer(t0))
+                return o + " = bh_ipow<" + cuda_type(t0) + ">(" + ops[1] + ", " + ops[2] + ");";
             return o + " = " + fn("pow", t0) + "(" + ops[1] + ", " + ops[2] + ");";
         case BH_ABSOLUTE:
             if (t1 == bh_type::BOOL || bh_type_is_unsigned_integer(t1)) return o + " = " + ops[1] + ";";

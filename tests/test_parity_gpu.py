@@ -22,7 +22,9 @@ def both(gpu_rt, oracle_rt, prog):
 def test_binary_opcodes(gpu_rt, oracle_rt, name):
     for dt in P.BINARY[name]:
         g, o = both(gpu_rt, oracle_rt, P.binary_program(name, dt, n=777))
-        rtol, atol = float_tol(dt, name in P.TRANSCENDENTAL)
+        # a - floor(a/b)*b cancels: the CPU's FMA contraction of the product moves the result by
+        # an ulp of `a`, so remainders get an absolute tolerance at that scale.
+        rtol, atol = float_tol(dt, name in P.TRANSCENDENTAL or name in ("REMAINDER", "MOD"))
         for k in range(2):
             assert_close(g[k], o[k], rtol, atol, f"{name} {np.dtype(dt)}")
 
