@@ -1,0 +1,423 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Bohrium vector engine.
+
+Headline (one JSON line on rank 0): the Black-Scholes workload -- 10M float64 options,
+S~U(5,30), K~U(1,100), T~U(0.25,10), r=0.02, vol=0.3, erf-based normal CDF -- run as 10 flushes
+per step, each flush one iteration ending in a mean-price reduction. `value` is the algorithmic HBM
+throughput of the flushes with the inputs resident in device memory (bytes of S, K and T read per
+flush plus the result written, over the device time of the timed steps). `e2e` is the same metric
+through the C ABI with the inputs handed over from page-locked host buffers every step and the 10
+mean prices read back. `cpu_baseline` is the oracle (the restated ve/openmp engine) on the host
+cores. `extra` adds the other workloads: the plain chain, the 2-D heat stencil and the batching
+workload in its plain and grouped forms.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--no-extra]
+
+With N > 1 (torchrun) every rank runs the same workload on its own GPU ("replicas only": the path
+has no data exchange between GPUs) and `value` is the sum over ranks divided by the slowest rank.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "flush wall-time & HBM GB/s (%peak): batched+learned vs plain ve/cuda; vs ve/openmp"
+BS_OPTIONS = 10_000_000
+BS_ITERS = 10
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------------------------ clocks
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv",
+                                          "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.15)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        try:
+            lines = open(self.path).read().strip().splitlines()[1:]
+        except OSError:
+            lines = []
+        for ln in lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1].split()[0]))
+                mx = float(f[2].split()[0])
+            except ValueError:
+                continue
+            for name, v in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if self.path:
+            os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------- distributed
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allreduce_max(world, x: float) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------------------ workloads
+def build_black_scholes(bh, W, rt, ex, n, pinned=False):
+    S, K, T = W.black_scholes_inputs(n, 0)
+    arrays, hosts = [], []
+    for x in (S, K, T):
+        a = bh.empty(rt, (n,), np.float64)
+        if pinned:
+            hosts.append(ex.set_pinned(a.base, x))
+        else:
+            ex.set_data(a.base, x)
+        arrays.append(a)
+    s, k, t = arrays
+    rt.flush()
+    irs, outs = [], []
+    for it in range(BS_ITERS):
+        m = W.black_scholes_iteration(rt, s, k, t, it)
+        flush = rt.take()
+        irs.append(ex.compile(flush))
+        outs.append(m)
+    return (s, k, t), hosts, irs, outs, (S, K, T)
+
+
+def bs_bytes(n):
+    return 3 * 8 * n + 8
+
+
+def sync_read(bh, ex, outs):
+    """One flush that syncs every result base, then read the host copies."""
+    ex.execute(bh.ir.Flush([], syncs=[o.base for o in outs]))
+    return [ex.lib.bhb_base_data(o.base.handle) for o in outs]
+
+
+def run_ours(args, world, rank, local):
+    os.environ["BH_CUDA_DEVICE_NUMBER"] = str(local)
+    import bohrium_b200 as bh
+    from bohrium_b200 import workloads as W
+    ex = bh.NativeExecutor()
+    rt = bh.Runtime(ex)
+    peak, peak_kind = peaks()
+
+    # ---- device-resident throughput -----------------------------------------------------
+    n = BS_OPTIONS
+    inputs, _, irs, outs, host_inputs = build_black_scholes(bh, W, rt, ex, n)
+    step = lambda: [ir.execute() for ir in irs]
+    for _ in range(max(args.warmup, 3)):
+        step()
+    ex.message("CUDA: sync")
+    barrier(world)
+    launches0 = int(ex.message("CUDA: launches"))
+    with Clocks(local) as clk:
+        ex.message("CUDA: timer start")
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step()
+        dev_ms = float(ex.message("CUDA: timer stop"))
+        wall = time.perf_counter() - t0
+    launches = int(ex.message("CUDA: launches")) - launches0
+    clocks = clk.summary()
+    # Per-launch kernel durations with CUDA events (one profiled step after the timed region).
+    ex.message("CUDA: prof on")
+    ex.message("statistic_enable_and_reset")
+    step()
+    ex.message("CUDA: sync")
+    stat = ex.message("statistic")
+    ex.message("CUDA: prof off")
+    kernel_ms = []
+    for line in stat.splitlines():
+        if line.strip().startswith("- {name"):
+            kernel_ms.append(float(line.split("ms:")[1].strip(" }")))
+    dev_ms_max = allreduce_max(world, dev_ms)
+    bytes_step = BS_ITERS * bs_bytes(n)
+    value = world * bytes_step * args.steps / (dev_ms_max / 1e3) / 1e9
+    got = [float(v) for v in (ex.peek(o.base)[0] for o in outs[:2])]
+    want = [W.black_scholes_numpy(*host_inputs, it) for it in range(2)] if rank == 0 else got
+    check_ok = all(abs(g - w) <= 1e-10 * abs(w) for g, w in zip(got, want))
+    avg_kernel_ms = statistics.mean(kernel_ms) if kernel_ms else dev_ms / args.steps / BS_ITERS
+    achieved = bs_bytes(n) / (avg_kernel_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                "kernel": "bh_grid_reduce (Black-Scholes flush)", "kernel_ms": round(avg_kernel_ms, 5),
+                "algorithmic_bytes_per_launch": bs_bytes(n)}
+    del irs, outs, inputs
+
+    # ---- end to end through the C ABI with page-locked host buffers ---------------------
+    (s, k, t), hosts, irs, outs, _ = build_black_scholes(bh, W, rt, ex, n, pinned=True)
+
+    def e2e_step():
+        for arr, h in zip((s, k, t), hosts):
+            ex.lib.bhb_data_set(ex.rt, arr.base.handle, 1, h.ctypes.data)  # hand over host data (re-upload)
+        for ir in irs:
+            ir.execute()
+        return sync_read(bh, ex, outs)
+
+    for _ in range(2):
+        e2e_step()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = allreduce_max(world, time.perf_counter() - t0)
+    e2e = {"value": round(world * bytes_step * args.steps / e2e_s / 1e9, 2), "unit": "GB/s",
+           "h2d_bytes_per_step": 3 * 8 * n, "d2h_bytes_per_step": 8 * BS_ITERS,
+           "ms_per_step": round(e2e_s * 1e3 / args.steps, 3)}
+    del irs, outs, s, k, t
+
+    extra = {}
+    if args.extra and rank == 0:
+        extra = run_extra(bh, W, ex, rt, peak)
+
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_baseline:
+        cpu = cpu_baseline(n=args.cpu_options)
+
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(dev_ms_max / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded uniform inputs)",
+        "config": {"workload": "black_scholes_f64_10M_options_x10_flushes", "options": n, "flushes_per_step": BS_ITERS,
+                   "bytecodes_per_flush": 44, "l2": "inputs (240 MB) larger than L2",
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "flush_ms_device": round(dev_ms_max / args.steps / BS_ITERS, 4),
+                   "flush_ms_wall": round(wall * 1e3 / args.steps / BS_ITERS, 4),
+                   "frac_of_peak": round(value / world / peak, 4), "result_check": check_ok},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+    }
+    if extra:
+        line["extra"] = extra
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_extra(bh, W, ex, rt, peak):
+    out = {}
+    # Config 1: the plain chain over three float64 arrays of 2^20 elements.
+    n = 1 << 20
+    A, B, C = W.plain_chain_inputs(n, 0)
+    a, b, c = (bh.array(rt, x) for x in (A, B, C))
+    rt.flush()
+    r = W.plain_chain(rt, a, b, c)
+    ir = ex.compile(rt.take())
+    for _ in range(5):
+        ir.execute()
+    ex.message("CUDA: sync")
+    reps = 200
+    ex.message("CUDA: timer start")
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ir.execute()
+    ms = float(ex.message("CUDA: timer stop")) / reps
+    wall = (time.perf_counter() - t0) * 1e3 / reps
+    out["plain_chain_f64_2^20"] = {"flush_ms_device": round(ms, 4), "flush_ms_wall": round(wall, 4),
+                                   "GB/s": round((3 * 8 * n + 8) / (ms / 1e3) / 1e9, 1),
+                                   "note": "25 MB working set: L2-resident across repeated flushes"}
+    del ir, r, a, b, c
+
+    # Config 3: 2-D heat stencil, float32 4096^2, 100 iterations as one flush repeated 50 times
+    # over a two-step (a->b, b->a) bytecode.
+    g = W.heat_grid(4096, 0)
+    ga, gb = bh.array(rt, g), bh.array(rt, g)
+    d1 = W.heat_step(ga, gb)
+    d2 = W.heat_step(gb, ga)
+    rt.flush()
+    # rebuild the same two steps as a repeatable flush
+    d1 = W.heat_step(ga, gb)
+    d2 = W.heat_step(gb, ga)
+    flush = rt.take()
+    flush.nrepeats = 50
+    ir = ex.compile(flush)
+    ir.execute()
+    ex.message("CUDA: sync")
+    ex.message("CUDA: timer start")
+    t0 = time.perf_counter()
+    ir.execute()
+    ms = float(ex.message("CUDA: timer stop"))
+    wall = (time.perf_counter() - t0) * 1e3
+    per_iter = (4096 * 4096 * 4 + 4094 * 4094 * 4)
+    out["heat_f32_4096^2_x100"] = {"flush_ms_device": round(ms, 3), "flush_ms_wall": round(wall, 3),
+                                   "GB/s": round(100 * per_iter / (ms / 1e3) / 1e9, 1),
+                                   "iterations": 100}
+    del ir, d1, d2, ga, gb
+
+    # Config 4: 4096 float32 systems of uneven length in one flush, plain vs grouped launches.
+    lengths = W.batching_lengths(4096, 256, 65536, 0)
+    xs = []
+    for i, L in enumerate(lengths):
+        f = bh.random_sample(rt, (int(L),), start=int(i) << 32, key=7, dtype=np.float32)
+        xs.append(f)
+    rt.flush()
+    outs = []
+    for x in xs:
+        y = W.batching_chain(x)
+        outs += [y, y.sum(), y.max()]
+    ir = ex.compile(rt.take())
+    total = int(lengths.sum())
+    res = {}
+    for mode in ["off", "grouped"]:
+        ex.message(f"CUDA: batch {mode}")
+        for _ in range(3):
+            ir.execute()
+        ex.message("CUDA: sync")
+        l0 = int(ex.message("CUDA: launches"))
+        reps = 5
+        ex.message("CUDA: timer start")
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            ir.execute()
+        ms = float(ex.message("CUDA: timer stop")) / reps
+        wall = (time.perf_counter() - t0) * 1e3 / reps
+        res[mode] = {"flush_ms_device": round(ms, 3), "flush_ms_wall": round(wall, 3),
+                     "launches_per_flush": (int(ex.message("CUDA: launches")) - l0) // reps,
+                     "GB/s": round((8 * total + 8 * 4096) / (max(ms, wall) / 1e3) / 1e9, 1)}
+    ex.message("CUDA: batch off")
+    # bit-identical results between the two forms
+    ex.message("CUDA: batch grouped")
+    ir.execute()
+    grouped = [ex.peek(o.base) for o in outs[1::3][:64]]
+    ex.message("CUDA: batch off")
+    ir.execute()
+    plain = [ex.peek(o.base) for o in outs[1::3][:64]]
+    res["bit_identical"] = all(np.array_equal(p, q) for p, q in zip(plain, grouped))
+    res["speedup_wall"] = round(res["off"]["flush_ms_wall"] / res["grouped"]["flush_ms_wall"], 2)
+    res["systems"] = 4096
+    res["elements"] = total
+    out["batching_4096_systems_f32"] = res
+    return out
+
+
+def cpu_baseline(n=BS_OPTIONS, iters=BS_ITERS):
+    """The oracle (restated ve/openmp) on the host cores: kernel time of the compiled OpenMP code."""
+    import bohrium_b200 as bh
+    from bohrium_b200 import workloads as W
+    from oracle.ve_openmp import OracleExecutor
+    threads = os.cpu_count() or 1
+    ex = OracleExecutor(threads=threads)
+    rt = bh.Runtime(ex)
+    S, K, T = W.black_scholes_inputs(n, 0)
+    s, k, t = (bh.array(rt, x) for x in (S, K, T))
+    W.black_scholes_iteration(rt, s, k, t, 0).numpy()  # compile
+    ex.exec_seconds = 0.0
+    for it in range(iters):
+        W.black_scholes_iteration(rt, s, k, t, it).numpy()
+    secs = ex.exec_seconds
+    return {"value": round(iters * bs_bytes(n) / secs / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": f"Black-Scholes {n} float64 options x {iters} flushes (the full workload); time of the "
+                      f"compiled OpenMP kernels, fusion and compilation excluded as the reference's caches hit",
+            "flush_ms": round(secs * 1e3 / iters, 3)}
+
+
+def run_reference(args, world, rank):
+    """The reference arm: the reference's CPU engine for this path (oracle port of ve/openmp)."""
+    if rank != 0:
+        return
+    n = args.cpu_options
+    cpu = cpu_baseline(n=n, iters=BS_ITERS)
+    steps = []
+    for _ in range(args.steps):
+        steps.append(cpu_baseline(n=n, iters=BS_ITERS)["value"])
+    value = statistics.median(steps)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded uniform inputs)",
+            "config": {"workload": "black_scholes_f64_10M_options_x10_flushes", "options": n,
+                       "flushes_per_step": BS_ITERS},
+            "cpu_baseline": {"value": value, "unit": "GB/s", "cores": cpu["cores"], "kind": "port",
+                             "sample": cpu["sample"]},
+            "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extra", dest="extra", action="store_false")
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--cpu-options", type=int, default=BS_OPTIONS)
+    args = ap.parse_args()
+    world, rank, local = dist_init()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

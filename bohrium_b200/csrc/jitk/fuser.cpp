@@ -376,28 +376,41 @@ void greedy(DAG &g, bool avoid_rank0_sweep) {
 
 // Topological traversal that greedily fuses root vertices (core/jitk/graph.hpp:63-139).
 // `pick` chooses the next root from the candidate set.
-vector<Block> topological(DAG &g, bool avoid_rank0_sweep, bool fifo_queue) {
-    vector<Block> ret;
-    deque<size_t> roots;
-    auto push = [&](size_t x) { roots.push_back(x); };
-    auto pop = [&]() {
+// The queue either is FIFO (breadth first) or prefers reshapable roots: the last reshapable root in
+// vertex order, else the smallest root (core/jitk/fuser.cpp:309-345).
+struct RootQueue {
+    const DAG &g;
+    bool fifo;
+    deque<size_t> q;
+    set<size_t> all, reshapable;
+    RootQueue(const DAG &dag, bool f) : g(dag), fifo(f) {}
+    void push(size_t x) {
+        if (fifo) {
+            q.push_back(x);
+        } else if (all.insert(x).second && g.v[x].block.isReshapable()) {
+            reshapable.insert(x);
+        }
+    }
+    bool empty() const { return fifo ? q.empty() : all.empty(); }
+    size_t pop() {
         size_t r;
-        if (fifo_queue) {
-            r = roots.front();
-            roots.pop_front();
+        if (fifo) {
+            r = q.front();
+            q.pop_front();
         } else {
-            // Prefer the last reshapable root in vertex order, else the smallest vertex.
-            sort(roots.begin(), roots.end());
-            roots.erase(unique(roots.begin(), roots.end()), roots.end());
-            size_t pick = roots.size();
-            for (size_t i = 0; i < roots.size(); ++i)
-                if (g.v[roots[i]].block.isReshapable()) pick = i;
-            if (pick == roots.size()) pick = 0;
-            r = roots[pick];
-            roots.erase(roots.begin() + static_cast<long>(pick));
+            r = reshapable.empty() ? *all.begin() : *reshapable.rbegin();
+            all.erase(r);
+            reshapable.erase(r);
         }
         return r;
-    };
+    }
+};
+
+vector<Block> topological(DAG &g, bool avoid_rank0_sweep, bool fifo_queue) {
+    vector<Block> ret;
+    RootQueue roots(g, fifo_queue);
+    auto push = [&](size_t x) { roots.push(x); };
+    auto pop = [&]() { return roots.pop(); };
     for (size_t x = 0; x < g.v.size(); ++x)
         if (g.v[x].alive && g.v[x].in.empty()) push(x);
     while (!roots.empty()) {
@@ -408,7 +421,7 @@ vector<Block> topological(DAG &g, bool avoid_rank0_sweep, bool fifo_queue) {
             if (g.v[w].in.size() <= 1) push(w);
         g.clear_vertex(vertex);
         if (block.isInstr()) continue;
-        deque<size_t> nonfusible;
+        vector<size_t> nonfusible;
         while (!roots.empty()) {
             const size_t x = pop();
             if (!g.v[x].block.isInstr() && mergeable(block, g.v[x].block, avoid_rank0_sweep)) {
@@ -420,7 +433,7 @@ vector<Block> topological(DAG &g, bool avoid_rank0_sweep, bool fifo_queue) {
                 nonfusible.push_back(x);
             }
         }
-        roots = std::move(nonfusible);
+        for (size_t x : nonfusible) push(x);
     }
     return ret;
 }

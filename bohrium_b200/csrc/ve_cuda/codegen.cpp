@@ -613,6 +613,7 @@ void add_common_fields(Symbols &sym, ParamLayout &pl, const CodegenOptions &opt)
         if (instr->constant.type == bh_type::R123) {
             ParamField f{ParamField::R123_START};
             f.c = instr->constant;
+            f.origin = instr->origin_id;
             pl.add(f, "bh_u64", "c" + to_string(i) + "_start");
             f.kind = ParamField::R123_KEY;
             pl.add(f, "bh_u64", "c" + to_string(i) + "_key");
@@ -621,6 +622,7 @@ void add_common_fields(Symbols &sym, ParamLayout &pl, const CodegenOptions &opt)
                 throw runtime_error("complex constants are not supported by the CUDA engine");
             ParamField f{ParamField::CONST};
             f.c = instr->constant;
+            f.origin = instr->origin_id;
             pl.add(f, cuda_type(instr->constant.type), "c" + to_string(i));
         }
     }
@@ -719,6 +721,34 @@ int64_t unit_bytes(const Symbols &sym, const vector<const Block *> &items) {
 }
 
 // ------------------------------------------------------------------------------------ schedules
+// Every schedule is written as `bh_work(p, w)` for work items w in [0, p.work), plus two kernels:
+// the plain launch (grid-stride over the unit's own work items) and the batched launch, which runs
+// the work items of many units of the same kernel in one persistent grid (item lookup by binary
+// search over the prefix sums of their work counts). Both call the same device code on the same
+// work items, so batched results equal plain results bit for bit.
+const char *kWrappers = R"CUDA(
+extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME__(const __grid_constant__ P p) {
+    for (bh_i64 w = blockIdx.x; w < p.work; w += gridDim.x) bh_work(p, w);
+}
+extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME___batch(const P* __restrict__ items,
+        const bh_i64* __restrict__ prefix, int nitems, bh_i64 total) {
+    for (bh_i64 g = blockIdx.x; g < total; g += gridDim.x) {
+        int lo = 0, hi = nitems - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (prefix[mid] <= g) lo = mid; else hi = mid - 1;
+        }
+        bh_work(items[lo], g - prefix[lo]);
+    }
+}
+)CUDA";
+
+ParamField work_field(int64_t work) {
+    ParamField f{ParamField::I64};
+    f.i64 = work;
+    return f;
+}
+
 LaunchUnit lower_serial(const vector<const Block *> &items, const CodegenOptions &opt) {
     LaunchUnit u;
     u.sched = Sched::SERIAL;
@@ -730,20 +760,35 @@ LaunchUnit lower_serial(const vector<const Block *> &items, const CodegenOptions
     vector<const Block *> pitems;
     for (const Block &b : pseudo._block_list) pitems.push_back(&b);
     Symbols sym = build_symbols(pitems, {});
-    ParamLayout pl2;
-    add_common_fields(sym, pl2, opt);
+    ParamLayout pl;
+    add_common_fields(sym, pl, opt);
+    pl.add(work_field(1), "bh_i64", "work");
     stringstream body;
     Emitter em(sym, body, opt);
-    body << "extern \"C\" __global__ void __launch_bounds__(32) __KERNEL_NAME__(const __grid_constant__ P p) {\n";
-    body << "    if (blockIdx.x != 0 || threadIdx.x != 0) return;\n";
+    body << "__device__ __forceinline__ void bh_work(const P &p, bh_i64 w) {\n";
+    body << "    if (threadIdx.x != 0) return;\n";
     body << pointer_locals(sym);
     Scope scope;
     em.write_body(pseudo, scope, 4);
-    body << "}\n";
-    u.fields = pl2.fields;
+    body << "}\n" << kWrappers;
+    u.fields = pl.fields;
     u.algorithmic_bytes = unit_bytes(sym, pitems);
-    finish_source(u, pl2.decl.str(), body.str(), opt);
+    finish_source(u, pl.decl.str(), body.str(), opt);
     return u;
+}
+
+// Temporaries declared on the threaded chain above the innermost threaded loop.
+void declare_chain_temps(Emitter &em, Symbols &sym, Scope &scope, const vector<const LoopB *> &chain, unsigned upto,
+                         ostream &body, int ind) {
+    for (unsigned r = 0; r < upto; ++r) {
+        for (const bh_base *b : em.sorted_temps(*chain[r])) {
+            if (sym.temps.count(b) && !scope.is_tmp(b)) {
+                scope.tmps.insert(b);
+                body << string(static_cast<size_t>(ind), ' ') << cuda_type(b->dtype()) << " t" << sym.base_index(b)
+                     << ";\n";
+            }
+        }
+    }
 }
 
 // FLAT: `loop` has P >= 1 leading parallel ranks.
@@ -751,72 +796,56 @@ LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) 
     LaunchUnit u;
     u.sched = Sched::FLAT;
     const Block holder(loop);
-    const vector<const Block *> items = {&holder};
-    Symbols sym = build_symbols(items, {});
+    Symbols sym = build_symbols({&holder}, {});
     const LoopB &L = holder.getLoop();
     const vector<const LoopB *> chain = jitk::get_first_loop_blocks(L);
     const LoopB &inner = *chain[P - 1];
-    const bool innermost = inner.isInnermost();
-    u.V = innermost ? opt.flat_v : 1;
-    ParamLayout pl;
-    add_common_fields(sym, pl, opt);
-    ParamField f{ParamField::I64};
-    pl.add(f, "bh_i64", "rows");
-    pl.add(f, "bh_i64", "chunks");
-    pl.add(f, "bh_i64", "work");
+    u.V = inner.isInnermost() ? opt.flat_v : 1;
     int64_t rows = 1;
     for (unsigned r = 0; r + 1 < P; ++r) rows *= chain[r]->size;
     u.rows = rows;
     u.cols = inner.size;
     const int64_t per = static_cast<int64_t>(kThreads) * u.V;
     const int64_t chunks = (u.cols + per - 1) / per;
-    pl.fields[pl.fields.size() - 3].i64 = rows;
-    pl.fields[pl.fields.size() - 2].i64 = chunks;
-    pl.fields[pl.fields.size() - 1].i64 = rows * chunks;
+    ParamLayout pl;
+    add_common_fields(sym, pl, opt);
+    pl.add(work_field(chunks), "bh_i64", "chunks");
+    pl.add(work_field(rows * chunks), "bh_i64", "work");
 
     stringstream body;
     Emitter em(sym, body, opt);
-    body << "extern \"C\" __global__ void __launch_bounds__(" << kThreads
-         << ") __KERNEL_NAME__(const __grid_constant__ P p) {\n";
+    body << "__device__ __forceinline__ void bh_work(const P &p, bh_i64 w) {\n";
     body << pointer_locals(sym);
-    body << "    for (bh_i64 w = blockIdx.x; w < p.work; w += gridDim.x) {\n";
-    body << "        const bh_i64 row = w / p.chunks;\n";
-    body << "        const bh_i64 chunk = w - row * p.chunks;\n";
-    body << "        bh_i64 rem = row;\n";
+    body << "    const bh_i64 row = w / p.chunks;\n";
+    body << "    const bh_i64 chunk = w - row * p.chunks;\n";
+    body << "    bh_i64 rem = row;\n";
     for (int r = static_cast<int>(P) - 2; r >= 0; --r) {
         const int lid = sym.loop_id.at(chain[r]);
         if (r == 0) {
-            body << "        const bh_i64 i0 = rem;\n";
+            body << "    const bh_i64 i0 = rem;\n";
         } else {
-            body << "        const bh_i64 i" << r << " = rem % p.n" << lid << "; rem /= p.n" << lid << ";\n";
+            body << "    const bh_i64 i" << r << " = rem % p.n" << lid << "; rem /= p.n" << lid << ";\n";
         }
     }
-    body << "        (void)rem;\n";
-    body << "        const bh_i64 cbase = chunk * " << per << " + threadIdx.x;\n";
+    body << "    (void)rem;\n";
+    body << "    const bh_i64 cbase = chunk * " << per << " + threadIdx.x;\n";
     body << "#pragma unroll\n";
-    body << "        for (int j = 0; j < " << u.V << "; ++j) {\n";
-    body << "            const bh_i64 i" << (P - 1) << " = cbase + j * " << kThreads << ";\n";
-    body << "            if (i" << (P - 1) << " >= p.n" << sym.loop_id.at(&inner) << ") break;\n";
+    body << "    for (int j = 0; j < " << u.V << "; ++j) {\n";
+    body << "        const bh_i64 i" << (P - 1) << " = cbase + j * " << kThreads << ";\n";
+    body << "        if (i" << (P - 1) << " >= p.n" << sym.loop_id.at(&inner) << ") break;\n";
     Scope scope;
-    // Temporaries declared on the threaded chain above the innermost threaded loop.
-    for (unsigned r = 0; r + 1 < P; ++r) {
-        for (const bh_base *b : em.sorted_temps(*chain[r])) {
-            if (sym.temps.count(b) && !scope.is_tmp(b)) {
-                scope.tmps.insert(b);
-                body << "            " << cuda_type(b->dtype()) << " t" << sym.base_index(b) << ";\n";
-            }
-        }
-    }
-    em.write_body(inner, scope, 12);
-    body << "        }\n    }\n}\n";
+    declare_chain_temps(em, sym, scope, chain, P - 1, body, 8);
+    em.write_body(inner, scope, 8);
+    body << "    }\n}\n" << kWrappers;
     u.fields = pl.fields;
-    u.algorithmic_bytes = unit_bytes(sym, items);
+    u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
     u.elements = rows * u.cols;
     finish_source(u, pl.decl.str(), body.str(), opt);
     return u;
 }
 
-// CTA-wide deterministic tree reduction of `v` (fixed xor-shuffle butterfly, then warp 0).
+// CTA-wide deterministic tree reduction of `v` (fixed xor-shuffle butterfly, then warp 0); the
+// result is valid in thread 0.
 string block_reduce_fn(const string &ctype, const string &fname, bh_opcode op, const string &identity) {
     stringstream ss;
     ss << "__device__ __forceinline__ " << ctype << " " << fname << "(" << ctype << " v, " << ctype << " *sm) {\n";
@@ -824,6 +853,7 @@ string block_reduce_fn(const string &ctype, const string &fname, bh_opcode op, c
     ss << "    for (int m = 16; m >= 1; m >>= 1) { const " << ctype << " o = bh_shfl_xor(v, m); v = "
        << reduce_expr(op, "v", "o") << "; }\n";
     ss << "    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n";
+    ss << "    __syncthreads();\n";
     ss << "    if (lane == 0) sm[warp] = v;\n";
     ss << "    __syncthreads();\n";
     ss << "    if (warp == 0) {\n";
@@ -832,13 +862,14 @@ string block_reduce_fn(const string &ctype, const string &fname, bh_opcode op, c
     ss << "        for (int m = 16; m >= 1; m >>= 1) { const " << ctype << " o = bh_shfl_xor(v, m); v = "
        << reduce_expr(op, "v", "o") << "; }\n";
     ss << "    }\n";
-    ss << "    __syncthreads();\n";
     ss << "    return v;\n}\n";
     return ss.str();
 }
 
 // GRID_REDUCE: `loop` is a 1-D innermost loop whose rank-0 sweeps are reductions to scalars.
-// `identities` are the kernel-level identity instructions of those reductions (folded).
+// `identities` are the kernel-level identity instructions of those reductions (folded). Work item
+// = one tile of kReduceTile elements; the CTA that completes the last tile of a unit folds the
+// unit's tile partials in tile order and writes the results.
 LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identities, const CodegenOptions &opt) {
     LaunchUnit u;
     u.sched = Sched::GRID_REDUCE;
@@ -848,17 +879,14 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
     for (const InstrPtr &i : identities) folded.insert(i.get());
     Symbols sym = build_symbols({&holder}, folded);
     const LoopB &L = holder.getLoop();
-    // Reductions of this loop, ordered by origin id.
     vector<InstrPtr> reds(L._sweeps.begin(), L._sweeps.end());
     sort(reds.begin(), reds.end(), [](const InstrPtr &a, const InstrPtr &b) { return a->origin_id < b->origin_id; });
     u.nred = static_cast<int>(reds.size());
-    ParamLayout pl;
-    add_common_fields(sym, pl, opt);
-    ParamField f{ParamField::I64};
     u.cols = L.size;
     const int64_t ntiles = (L.size + kReduceTile - 1) / kReduceTile;
-    f.i64 = ntiles;
-    pl.add(f, "bh_i64", "ntiles");
+    ParamLayout pl;
+    add_common_fields(sym, pl, opt);
+    pl.add(work_field(ntiles), "bh_i64", "work");
     ParamField fs{ParamField::SCRATCH};
     pl.add(fs, "unsigned char*", "scratch");
     ParamField fc{ParamField::COUNTER};
@@ -866,49 +894,41 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
 
     stringstream helpers, body;
     Emitter em(sym, body, opt);
-    // Each reduction gets an accumulator per thread and a slot per tile in the scratch buffer.
     vector<string> ctypes, idents, accs;
-    int64_t scratch_off = 0;
-    vector<int64_t> offs;
     for (size_t k = 0; k < reds.size(); ++k) {
         const InstrPtr &r = reds[k];
         const bh_type t = r->operand[0].base->dtype();
         ctypes.push_back(cuda_type(t));
         idents.push_back(constant_literal(jitk::sweep_identity(r->opcode, t)));
         accs.push_back("tacc" + to_string(k));
-        offs.push_back(scratch_off);
-        scratch_off += 8; // per tile
         helpers << block_reduce_fn(ctypes[k], "bh_block_reduce" + to_string(k), r->opcode, idents[k]);
         em.external_acc[ViewKey(r->operand[0])] = accs[k];
     }
-    u.scratch_bytes_per_tile = scratch_off;
+    u.scratch_bytes_per_tile = 8 * static_cast<int64_t>(reds.size());
     body << helpers.str();
-    body << "extern \"C\" __global__ void __launch_bounds__(" << kThreads
-         << ") __KERNEL_NAME__(const __grid_constant__ P p) {\n";
+    body << "__device__ void bh_work(const P &p, bh_i64 tile) {\n";
     body << pointer_locals(sym);
     body << "    __shared__ unsigned long long sm_raw[" << (kThreads / 32) << "];\n";
     body << "    __shared__ bool am_last;\n";
     for (size_t k = 0; k < reds.size(); ++k)
-        body << "    " << ctypes[k] << "* part" << k << " = (" << ctypes[k] << "*)(p.scratch + p.ntiles * " << offs[k]
+        body << "    " << ctypes[k] << "* part" << k << " = (" << ctypes[k] << "*)(p.scratch + p.work * " << 8 * k
              << ");\n";
-    body << "    for (bh_i64 tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {\n";
-    for (size_t k = 0; k < reds.size(); ++k) body << "        " << ctypes[k] << " " << accs[k] << " = " << idents[k] << ";\n";
+    for (size_t k = 0; k < reds.size(); ++k) body << "    " << ctypes[k] << " " << accs[k] << " = " << idents[k] << ";\n";
     body << "#pragma unroll\n";
-    body << "        for (int j = 0; j < " << kReduceV << "; ++j) {\n";
-    body << "            const bh_i64 i0 = tile * " << kReduceTile << " + j * " << kThreads << " + threadIdx.x;\n";
-    body << "            if (i0 >= p.n" << sym.loop_id.at(&L) << ") break;\n";
+    body << "    for (int j = 0; j < " << kReduceV << "; ++j) {\n";
+    body << "        const bh_i64 i0 = tile * " << kReduceTile << " + j * " << kThreads << " + threadIdx.x;\n";
+    body << "        if (i0 >= p.n" << sym.loop_id.at(&L) << ") break;\n";
     Scope scope;
-    em.write_body(L, scope, 12);
-    body << "        }\n";
-    for (size_t k = 0; k < reds.size(); ++k) {
-        body << "        " << accs[k] << " = bh_block_reduce" << k << "(" << accs[k] << ", (" << ctypes[k]
-             << "*)sm_raw);\n";
-        body << "        if (threadIdx.x == 0) part" << k << "[tile] = " << accs[k] << ";\n";
-    }
+    em.write_body(L, scope, 8);
     body << "    }\n";
-    body << "    __threadfence();\n";
-    body << "    __syncthreads();\n";
-    body << "    if (threadIdx.x == 0) am_last = atomicAdd(p.counter, 1u) == gridDim.x - 1;\n";
+    for (size_t k = 0; k < reds.size(); ++k) {
+        body << "    " << accs[k] << " = bh_block_reduce" << k << "(" << accs[k] << ", (" << ctypes[k] << "*)sm_raw);\n";
+        body << "    if (threadIdx.x == 0) part" << k << "[tile] = " << accs[k] << ";\n";
+    }
+    body << "    if (threadIdx.x == 0) {\n";
+    body << "        __threadfence();\n";
+    body << "        am_last = atomicAdd(p.counter, 1u) == (unsigned)(p.work - 1);\n";
+    body << "    }\n";
     body << "    __syncthreads();\n";
     body << "    if (!am_last) return;\n";
     body << "    __threadfence();\n";
@@ -916,7 +936,7 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
         const InstrPtr &r = reds[k];
         body << "    {\n";
         body << "        " << ctypes[k] << " acc = " << idents[k] << ";\n";
-        body << "        for (bh_i64 t = threadIdx.x; t < p.ntiles; t += " << kThreads << ") {\n";
+        body << "        for (bh_i64 t = threadIdx.x; t < p.work; t += " << kThreads << ") {\n";
         body << "            const " << ctypes[k] << " x = ((volatile " << ctypes[k] << "*)part" << k << ")[t];\n";
         body << "            acc = " << reduce_expr(r->opcode, "acc", "x") << ";\n";
         body << "        }\n";
@@ -927,7 +947,7 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
         body << "    }\n";
     }
     body << "    if (threadIdx.x == 0) *p.counter = 0u;\n";
-    body << "}\n";
+    body << "}\n" << kWrappers;
     u.fields = pl.fields;
     u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
     u.elements = L.size;
@@ -944,11 +964,7 @@ bool outer_reduce_applicable(const LoopB &L) {
     if (!jitk::all_local_instr(L).empty()) return false;
     if (L._block_list.size() != 1 || L._block_list[0].isInstr()) return false;
     const LoopB &sub = L._block_list[0].getLoop();
-    const unsigned P = static_cast<unsigned>(jitk::parallel_ranks(sub, 64).first);
-    if (P == 0) return false;
-    // Every sweep must be inside the threaded chain's innermost loop or below it, and the whole
-    // sub-nest must be free of deeper sweeps over the threaded ranks (guaranteed by P).
-    return true;
+    return jitk::parallel_ranks(sub, 64).first > 0;
 }
 
 LaunchUnit lower_outer_reduce(const LoopB &loop, const vector<const Block *> &identity_loops,
@@ -965,69 +981,58 @@ LaunchUnit lower_outer_reduce(const LoopB &loop, const vector<const Block *> &id
     const unsigned P = static_cast<unsigned>(jitk::parallel_ranks(sub, 64).first);
     const vector<const LoopB *> chain = jitk::get_first_loop_blocks(sub);
     const LoopB &inner = *chain[P - 1];
-    ParamLayout pl;
-    add_common_fields(sym, pl, opt);
     int64_t rows = 1;
     for (unsigned r = 0; r + 1 < P; ++r) rows *= chain[r]->size;
     u.rows = rows;
     u.cols = inner.size;
-    ParamField f{ParamField::I64};
-    f.i64 = rows * inner.size;
-    pl.add(f, "bh_i64", "points");
+    ParamLayout pl;
+    add_common_fields(sym, pl, opt);
+    pl.add(work_field(rows * inner.size), "bh_i64", "points");
+    pl.add(work_field((rows * inner.size + kThreads - 1) / kThreads), "bh_i64", "work");
     vector<InstrPtr> reds(L._sweeps.begin(), L._sweeps.end());
     sort(reds.begin(), reds.end(), [](const InstrPtr &a, const InstrPtr &b) { return a->origin_id < b->origin_id; });
 
     stringstream body;
     Emitter em(sym, body, opt);
-    body << "extern \"C\" __global__ void __launch_bounds__(" << kThreads
-         << ") __KERNEL_NAME__(const __grid_constant__ P p) {\n";
+    body << "__device__ __forceinline__ void bh_work(const P &p, bh_i64 w) {\n";
     body << pointer_locals(sym);
-    body << "    for (bh_i64 pt = (bh_i64)blockIdx.x * " << kThreads << " + threadIdx.x; pt < p.points; pt += (bh_i64)gridDim.x * "
-         << kThreads << ") {\n";
-    // Decompose the point into the sub-nest's threaded indices (ranks 1..P).
-    body << "        bh_i64 rem = pt;\n";
+    body << "    const bh_i64 pt = w * " << kThreads << " + threadIdx.x;\n";
+    body << "    if (pt >= p.points) return;\n";
+    body << "    bh_i64 rem = pt;\n";
     for (int r = static_cast<int>(P) - 1; r >= 0; --r) {
         const int rank = r + 1;
         const int lid = sym.loop_id.at(chain[r]);
         if (r == 0) {
-            body << "        const bh_i64 i" << rank << " = rem;\n";
+            body << "    const bh_i64 i" << rank << " = rem;\n";
         } else {
-            body << "        const bh_i64 i" << rank << " = rem % p.n" << lid << "; rem /= p.n" << lid << ";\n";
+            body << "    const bh_i64 i" << rank << " = rem % p.n" << lid << "; rem /= p.n" << lid << ";\n";
         }
     }
-    // Accumulators of the rank-0 reductions, initialised with the identity.
     Scope scope;
     for (size_t k = 0; k < reds.size(); ++k) {
         const bh_type t = reds[k]->operand[0].base->dtype();
         const string nm = "oacc" + to_string(k);
-        body << "        " << cuda_type(t) << " " << nm << " = "
-             << constant_literal(jitk::sweep_identity(reds[k]->opcode, t)) << ";\n";
+        body << "    " << cuda_type(t) << " " << nm << " = " << constant_literal(jitk::sweep_identity(reds[k]->opcode, t))
+             << ";\n";
         em.external_acc[ViewKey(reds[k]->operand[0])] = nm;
     }
-    for (unsigned r = 0; r + 1 < P; ++r) {
-        for (const bh_base *b : em.sorted_temps(*chain[r])) {
-            if (sym.temps.count(b) && !scope.is_tmp(b)) {
-                scope.tmps.insert(b);
-                body << "        " << cuda_type(b->dtype()) << " t" << sym.base_index(b) << ";\n";
-            }
-        }
-    }
-    body << "        for (bh_i64 i0 = 0; i0 < p.n" << sym.loop_id.at(&L) << "; ++i0) {\n";
+    declare_chain_temps(em, sym, scope, chain, P - 1, body, 4);
+    body << "    for (bh_i64 i0 = 0; i0 < p.n" << sym.loop_id.at(&L) << "; ++i0) {\n";
     Scope s0;
     s0.parent = &scope;
     for (const bh_base *b : em.sorted_temps(L)) {
         if (sym.temps.count(b) && !s0.is_tmp(b)) {
             s0.tmps.insert(b);
-            body << "            " << cuda_type(b->dtype()) << " t" << sym.base_index(b) << ";\n";
+            body << "        " << cuda_type(b->dtype()) << " t" << sym.base_index(b) << ";\n";
         }
     }
-    em.write_body(inner, s0, 12);
-    body << "        }\n";
+    em.write_body(inner, s0, 8);
+    body << "    }\n";
     for (size_t k = 0; k < reds.size(); ++k) {
         if (sym.temps.count(reds[k]->operand[0].base)) continue;
-        body << "        " << em.array_ref(reds[k]->operand[0], 0) << " = oacc" << k << ";\n";
+        body << "    " << em.array_ref(reds[k]->operand[0], 0) << " = oacc" << k << ";\n";
     }
-    body << "    }\n}\n";
+    body << "}\n" << kWrappers;
     u.fields = pl.fields;
     u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
     u.elements = rows * inner.size * L.size;

@@ -47,6 +47,7 @@ struct ParamField {
     bh_base *base = nullptr; // PTR
     int64_t i64 = 0;         // I64
     bh_constant c{};         // CONST / R123_*
+    int64_t origin = -1;     // CONST / R123_*: origin id of the instruction holding the constant
 };
 
 struct LaunchUnit {

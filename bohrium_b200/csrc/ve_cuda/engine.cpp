@@ -122,8 +122,7 @@ EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
     if (limit_pct < 0 || limit_pct > 100) throw runtime_error("config: `malloc_cache_limit` must be between 0 and 100");
     threshold = static_cast<uint64_t>(static_cast<double>(prop.totalGlobalMem) * (limit_pct / 100.0));
     check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold), "cudaMemPoolSetAttribute");
-    check(cudaMalloc(&counters, 4096 * sizeof(unsigned int)), "cudaMalloc(counters)");
-    check(cudaMemset(counters, 0, 4096 * sizeof(unsigned int)), "cudaMemset(counters)");
+    ensure_counters(4096);
     check(cudaMalloc(&err_record, sizeof(unsigned long long)), "cudaMalloc(err)");
     check(cudaMemset(err_record, 0, sizeof(unsigned long long)), "cudaMemset(err)");
     if (!cache_dir.empty()) mkdir(cache_dir.c_str(), 0755);
@@ -136,6 +135,10 @@ EngineCUDA::~EngineCUDA() {
             if (kv.second.ptr) cudaFree(kv.second.ptr);
         if (scratch) cudaFree(scratch);
         if (counters) cudaFree(counters);
+        if (staging_dev) cudaFree(staging_dev);
+        if (staging_host) cudaFreeHost(staging_host);
+        for (void *p : staging_retired) cudaFreeHost(p);
+        if (staging_event) cudaEventDestroy(static_cast<cudaEvent_t>(staging_event));
         if (err_record) cudaFree(err_record);
         cudaStreamDestroy(static_cast<cudaStream_t>(_stream));
     } catch (...) {
@@ -230,6 +233,27 @@ double EngineCUDA::last_execute_ms() {
     return ms;
 }
 
+void EngineCUDA::timer_start() {
+    if (!tm_begin) {
+        cudaEvent_t a, b;
+        check(cudaEventCreate(&a), "cudaEventCreate");
+        check(cudaEventCreate(&b), "cudaEventCreate");
+        tm_begin = a;
+        tm_end = b;
+    }
+    check(cudaEventRecord(static_cast<cudaEvent_t>(tm_begin), static_cast<cudaStream_t>(_stream)), "cudaEventRecord");
+}
+
+double EngineCUDA::timer_stop_ms() {
+    if (!tm_begin) return 0.0;
+    check(cudaEventRecord(static_cast<cudaEvent_t>(tm_end), static_cast<cudaStream_t>(_stream)), "cudaEventRecord");
+    check(cudaEventSynchronize(static_cast<cudaEvent_t>(tm_end)), "cudaEventSynchronize");
+    float ms = 0;
+    check(cudaEventElapsedTime(&ms, static_cast<cudaEvent_t>(tm_begin), static_cast<cudaEvent_t>(tm_end)),
+          "cudaEventElapsedTime");
+    return ms;
+}
+
 void EngineCUDA::copyToHost(const set<bh_base *> &bases, bool evict) {
     bool any = false;
     for (bh_base *base : bases) {
@@ -295,13 +319,24 @@ void *EngineCUDA::ensure_scratch(int64_t bytes) {
     return scratch;
 }
 
+unsigned int *EngineCUDA::ensure_counters(int64_t n) {
+    if (n <= counter_capacity) return counters;
+    const int64_t nc = max<int64_t>(n, counter_capacity * 2);
+    cudaStream_t s = static_cast<cudaStream_t>(_stream);
+    if (counters) check(cudaFreeAsync(counters, s), "cudaFreeAsync(counters)");
+    check(cudaMallocAsync(&counters, static_cast<size_t>(nc) * sizeof(unsigned int), s), "cudaMallocAsync(counters)");
+    check(cudaMemsetAsync(counters, 0, static_cast<size_t>(nc) * sizeof(unsigned int), s), "cudaMemsetAsync(counters)");
+    counter_capacity = nc;
+    return counters;
+}
+
 // ------------------------------------------------------------------------------- compilation
-void *EngineCUDA::function_for(const LaunchUnit &u) {
+EngineCUDA::Compiled *EngineCUDA::compiled_for(const LaunchUnit &u) {
     const uint64_t h = fnv1a(u.source.data(), u.source.size());
     auto it = functions.find(h);
     if (it != functions.end()) {
         ++_stats.kernel_cache_hits;
-        return it->second;
+        return &it->second;
     }
     ++_stats.kernel_cache_misses;
     const auto t0 = chrono::steady_clock::now();
@@ -354,114 +389,209 @@ void *EngineCUDA::function_for(const LaunchUnit &u) {
     }
     CUmodule mod;
     api->ck(api->cuModuleLoadData(&mod, cubin.data()), "cuModuleLoadData");
-    CUfunction f;
+    Compiled c;
+    CUfunction f, fb;
     api->ck(api->cuModuleGetFunction(&f, mod, u.name.c_str()), "cuModuleGetFunction");
-    functions[h] = reinterpret_cast<void *>(f);
-    int occ = 0;
-    const int threads = u.sched == Sched::SERIAL ? 32 : kThreads;
-    api->ck(api->cuOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, threads, 0), "cuOccupancy");
-    occupancy[reinterpret_cast<void *>(f)] = max(occ, 1);
+    api->ck(api->cuModuleGetFunction(&fb, mod, (u.name + "_batch").c_str()), "cuModuleGetFunction(batch)");
+    c.fn = reinterpret_cast<void *>(f);
+    c.fn_batch = reinterpret_cast<void *>(fb);
+    api->ck(api->cuOccupancyMaxActiveBlocksPerMultiprocessor(&c.occ, f, kThreads, 0), "cuOccupancy");
+    api->ck(api->cuOccupancyMaxActiveBlocksPerMultiprocessor(&c.occ_batch, fb, kThreads, 0), "cuOccupancy");
+    c.occ = max(c.occ, 1);
+    c.occ_batch = max(c.occ_batch, 1);
     _stats.time_compile += seconds_since(t0);
     if (verbose) cerr << "[ve_cuda] compiled " << u.name << "\n" << u.source << endl;
-    return reinterpret_cast<void *>(f);
+    return &functions.emplace(h, c).first->second;
 }
 
 // ------------------------------------------------------------------------------------ launch
-vector<uint8_t> EngineCUDA::pack_params(const LaunchUnit &u) {
-    vector<uint8_t> buf(u.fields.size() * 8, 0);
-    int64_t scratch_need = 0;
-    if (u.sched == Sched::GRID_REDUCE) scratch_need = u.work_items() * u.scratch_bytes_per_tile;
-    if (u.sched == Sched::SCAN1D) scratch_need = u.work_items() * 16;
-    void *scr = scratch_need > 0 ? ensure_scratch(scratch_need) : scratch;
+// Scratch bytes a unit needs for its tile partials.
+static int64_t unit_scratch(const LaunchUnit &u) {
+    return u.sched == Sched::GRID_REDUCE ? u.work_items() * u.scratch_bytes_per_tile : 0;
+}
+
+void EngineCUDA::pack_params(const PlanUnit &pu, const vector<bh_base *> &bases,
+                             const vector<bh_instruction *> &instrs, int64_t scratch_off, int64_t counter_idx,
+                             uint8_t *out) {
+    const LaunchUnit &u = pu.unit;
+    memset(out, 0, u.fields.size() * 8);
     for (size_t i = 0; i < u.fields.size(); ++i) {
         const ParamField &f = u.fields[i];
-        uint8_t *slot = &buf[i * 8];
+        uint8_t *slot = out + i * 8;
         switch (f.kind) {
             case ParamField::PTR: {
-                void *p = getBuffer(f.base);
+                bh_base *b = pu.ptr_base[i] >= 0 ? bases[static_cast<size_t>(pu.ptr_base[i])] : f.base;
+                void *p = getBuffer(b);
                 memcpy(slot, &p, 8);
                 break;
             }
             case ParamField::I64: memcpy(slot, &f.i64, 8); break;
-            case ParamField::CONST: memcpy(slot, &f.c.value, static_cast<size_t>(bh_type_size(f.c.type))); break;
-            case ParamField::R123_START: memcpy(slot, &f.c.value.r123.start, 8); break;
-            case ParamField::R123_KEY: memcpy(slot, &f.c.value.r123.key, 8); break;
+            case ParamField::CONST: {
+                const bh_constant &c =
+                    f.origin >= 0 && f.origin < static_cast<int64_t>(instrs.size()) ? instrs[f.origin]->constant : f.c;
+                memcpy(slot, &c.value, static_cast<size_t>(bh_type_size(f.c.type)));
+                break;
+            }
+            case ParamField::R123_START:
+            case ParamField::R123_KEY: {
+                const bh_constant &c =
+                    f.origin >= 0 && f.origin < static_cast<int64_t>(instrs.size()) ? instrs[f.origin]->constant : f.c;
+                const uint64_t v = f.kind == ParamField::R123_START ? c.value.r123.start : c.value.r123.key;
+                memcpy(slot, &v, 8);
+                break;
+            }
             case ParamField::SCRATCH: {
-                void *p = f.i64 == -1 ? static_cast<void *>(err_record) : scr;
+                void *p = f.i64 == -1 ? static_cast<void *>(err_record)
+                                      : static_cast<void *>(static_cast<uint8_t *>(scratch) + scratch_off);
                 memcpy(slot, &p, 8);
                 break;
             }
             case ParamField::COUNTER: {
-                void *p = counters;
+                void *p = counters + counter_idx;
                 memcpy(slot, &p, 8);
                 break;
             }
         }
     }
-    return buf;
 }
 
-void EngineCUDA::launch(const LaunchUnit &u, const vector<uint8_t> &params, const string *) {
-    void *fv = function_for(u);
-    CUfunction f = reinterpret_cast<CUfunction>(fv);
+void EngineCUDA::record_begin(UnitRecord &r, void *&e0) {
+    if (!prof) return;
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, static_cast<cudaStream_t>(_stream));
+    e0 = e;
+    (void)r;
+}
+
+void EngineCUDA::record_end(UnitRecord &r, void *e0) {
+    if (!prof) return;
+    cudaEvent_t e1;
+    cudaEventCreate(&e1);
+    cudaEventRecord(e1, static_cast<cudaStream_t>(_stream));
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&r.ms, static_cast<cudaEvent_t>(e0), e1);
+    cudaEventDestroy(static_cast<cudaEvent_t>(e0));
+    cudaEventDestroy(e1);
+    _stats.records.push_back(r);
+}
+
+void EngineCUDA::launch_plain(const PlanUnit &pu, const vector<bh_base *> &bases,
+                              const vector<bh_instruction *> &instrs) {
+    const LaunchUnit &u = pu.unit;
     const int64_t work = u.work_items();
-    int64_t grid = 1;
-    unsigned threads = kThreads;
-    if (u.sched == Sched::SERIAL) {
-        threads = 32;
-    } else {
-        const int64_t resident = static_cast<int64_t>(_sm_count) * occupancy[fv];
-        grid = max<int64_t>(1, min<int64_t>(work, resident));
-    }
     if (work == 0) return;
-    void *args[] = {const_cast<uint8_t *>(params.data())};
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (prof) {
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
-        cudaEventRecord(e0, static_cast<cudaStream_t>(_stream));
-    }
-    api->ck(api->cuLaunchKernel(f, static_cast<unsigned>(grid), 1, 1, threads, 1, 1, 0,
-                                static_cast<CUstream>(_stream), args, nullptr),
+    ensure_scratch(unit_scratch(u));
+    ensure_counters(1);
+    vector<uint8_t> params(u.fields.size() * 8);
+    pack_params(pu, bases, instrs, 0, 0, params.data());
+    const int64_t resident = static_cast<int64_t>(_sm_count) * pu.compiled->occ;
+    const int64_t grid = max<int64_t>(1, min<int64_t>(work, resident));
+    void *args[] = {params.data()};
+    UnitRecord rec{u.name, u.sched, u.elements, u.algorithmic_bytes, 1, 0.f};
+    void *e0 = nullptr;
+    record_begin(rec, e0);
+    api->ck(api->cuLaunchKernel(reinterpret_cast<CUfunction>(pu.compiled->fn), static_cast<unsigned>(grid), 1, 1,
+                                kThreads, 1, 1, 0, static_cast<CUstream>(_stream), args, nullptr),
             "cuLaunchKernel");
+    record_end(rec, e0);
     ++_stats.launches;
     if (u.sched == Sched::SERIAL) ++_stats.serial_units;
-    if (prof) {
-        cudaEventRecord(e1, static_cast<cudaStream_t>(_stream));
-        cudaEventSynchronize(e1);
-        UnitRecord r;
-        r.name = u.name;
-        r.sched = u.sched;
-        r.elements = u.elements;
-        r.bytes = u.algorithmic_bytes;
-        cudaEventElapsedTime(&r.ms, e0, e1);
-        _stats.records.push_back(r);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-    }
 }
 
-void EngineCUDA::check_error_record() {
-    if (!cg_opt.bounds_check) return;
-    unsigned long long v = 0;
-    check(cudaMemcpyAsync(&v, err_record, sizeof(v), cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(_stream)),
-          "cudaMemcpyAsync(err)");
-    synchronize();
-    if (v != 0) {
-        check(cudaMemset(err_record, 0, sizeof(v)), "cudaMemset(err)");
-        last_error_index = v & 0x7fffffffffffffffULL;
-        throw runtime_error("bounds check: a generated kernel indexed element " + to_string(last_error_index) +
-                            " outside its array");
+void EngineCUDA::launch_batched(const vector<const PlanUnit *> &group, const vector<bh_base *> &bases,
+                                const vector<bh_instruction *> &instrs) {
+    const PlanUnit &proto = *group[0];
+    const size_t psize = proto.unit.fields.size() * 8;
+    const size_t n = group.size();
+    // Per-item scratch and counters.
+    int64_t scratch_total = 0;
+    vector<int64_t> scratch_off(n);
+    for (size_t k = 0; k < n; ++k) {
+        scratch_off[k] = scratch_total;
+        scratch_total += (unit_scratch(group[k]->unit) + 255) / 256 * 256;
     }
+    ensure_scratch(scratch_total);
+    ensure_counters(static_cast<int64_t>(n));
+    // Items (parameter structs) followed by the prefix sums of their work counts.
+    const size_t items_bytes = (psize * n + 15) / 16 * 16;
+    const size_t bytes = items_bytes + (n + 1) * sizeof(int64_t);
+    uint8_t *host = staging_alloc(bytes);
+    int64_t *prefix = reinterpret_cast<int64_t *>(host + items_bytes);
+    int64_t total = 0;
+    for (size_t k = 0; k < n; ++k) {
+        pack_params(*group[k], bases, instrs, scratch_off[k], static_cast<int64_t>(k), host + k * psize);
+        prefix[k] = total;
+        total += group[k]->unit.work_items();
+    }
+    prefix[n] = total;
+    if (total == 0) return;
+    uint8_t *dev = device_staging(bytes);
+    check(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, static_cast<cudaStream_t>(_stream)),
+          "cudaMemcpyAsync(batch items)");
+    if (!staging_event) {
+        cudaEvent_t e;
+        check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        staging_event = e;
+    }
+    check(cudaEventRecord(static_cast<cudaEvent_t>(staging_event), static_cast<cudaStream_t>(_stream)),
+          "cudaEventRecord(staging)");
+    void *items_ptr = dev;
+    void *prefix_ptr = dev + items_bytes;
+    int nitems = static_cast<int>(n);
+    void *args[] = {&items_ptr, &prefix_ptr, &nitems, &total};
+    const int64_t resident = static_cast<int64_t>(_sm_count) * proto.compiled->occ_batch;
+    const int64_t grid = max<int64_t>(1, min<int64_t>(total, resident));
+    UnitRecord rec{proto.unit.name + "_batch", proto.unit.sched, 0, 0, static_cast<int>(n), 0.f};
+    for (const PlanUnit *pu : group) {
+        rec.elements += pu->unit.elements;
+        rec.bytes += pu->unit.algorithmic_bytes;
+    }
+    void *e0 = nullptr;
+    record_begin(rec, e0);
+    api->ck(api->cuLaunchKernel(reinterpret_cast<CUfunction>(proto.compiled->fn_batch), static_cast<unsigned>(grid),
+                                1, 1, kThreads, 1, 1, 0, static_cast<CUstream>(_stream), args, nullptr),
+            "cuLaunchKernel(batch)");
+    record_end(rec, e0);
+    ++_stats.launches;
+    ++_stats.grouped_launches;
 }
+
+uint8_t *EngineCUDA::staging_alloc(size_t bytes) {
+    // Host staging lives for the whole flush; it is recycled once the previous flush's copies ended.
+    if (staging_used + bytes > staging_capacity) {
+        // Keep old blocks alive until the stream has consumed them.
+        synchronize();
+        for (void *p : staging_retired) cudaFreeHost(p);
+        staging_retired.clear();
+        if (staging_host) staging_retired.push_back(staging_host);
+        staging_capacity = max<size_t>(bytes * 2, max<size_t>(staging_capacity * 2, 1 << 20));
+        void *p = nullptr;
+        check(cudaMallocHost(&p, staging_capacity), "cudaMallocHost(staging)");
+        staging_host = static_cast<uint8_t *>(p);
+        staging_used = 0;
+        if (staging_dev) check(cudaFreeAsync(staging_dev, static_cast<cudaStream_t>(_stream)), "cudaFreeAsync");
+        check(cudaMallocAsync(reinterpret_cast<void **>(&staging_dev), staging_capacity,
+                              static_cast<cudaStream_t>(_stream)),
+              "cudaMallocAsync(staging)");
+    }
+    uint8_t *p = staging_host + staging_used;
+    last_staging_offset = staging_used;
+    staging_used += (bytes + 255) / 256 * 256;
+    return p;
+}
+
+uint8_t *EngineCUDA::device_staging(size_t) { return staging_dev + last_staging_offset; }
 
 // ------------------------------------------------------------------------------- fuse cache
 namespace {
-// Structural hash of an instruction list: opcodes, sweep axes, the constant slot, and for every
-// view its base (numbered by first appearance), dtype, start (unless sliding), shape and stride.
-uint64_t hash_instr_list(const vector<bh_instruction *> &instr_list, vector<bh_base *> &base_ids) {
+// Structural hash of an instruction list: opcodes, sweep axes, the constant slot, constructor
+// flags, and for every view its base (numbered by first appearance), dtype, size, start (unless
+// sliding), shape and stride. `base_ids` receives the bases in first-appearance order.
+uint64_t hash_instr_list(const vector<bh_instruction *> &instr_list, vector<bh_base *> &base_ids, bool &sliding) {
     Hasher h;
     unordered_map<const bh_base *, uint64_t> ids;
+    sliding = false;
     for (const bh_instruction *instr : instr_list) {
         h.add(static_cast<uint64_t>(instr->opcode));
         h.add(static_cast<uint64_t>(instr->sweep_axis()));
@@ -483,7 +613,11 @@ uint64_t hash_instr_list(const vector<bh_instruction *> &instr_list, vector<bh_b
             h.add(id);
             h.add(static_cast<uint64_t>(v.base->dtype()));
             h.add(static_cast<uint64_t>(v.base->nelem()));
-            if (!v.hasSlide()) h.add(static_cast<uint64_t>(v.start));
+            if (v.hasSlide()) {
+                sliding = true;
+            } else {
+                h.add(static_cast<uint64_t>(v.start));
+            }
             h.add(static_cast<uint64_t>(v.ndim));
             for (int64_t d = 0; d < v.ndim; ++d) {
                 h.add(static_cast<uint64_t>(v.shape[d]));
@@ -524,13 +658,9 @@ void rebase(Block &block, const map<bh_base *, bh_base *> &cached2new,
 }
 } // namespace
 
-vector<LoopB> EngineCUDA::kernels_for(vector<bh_instruction *> &instr_list) {
+vector<LoopB> EngineCUDA::kernels_for(vector<bh_instruction *> &instr_list, uint64_t key,
+                                      const vector<bh_base *> &base_ids) {
     const auto t0 = chrono::steady_clock::now();
-    int64_t oc = 0;
-    for (bh_instruction *i : instr_list) i->origin_id = oc++;
-    vector<bh_base *> base_ids;
-    // Frees are part of the structure too (they decide contraction).
-    const uint64_t key = hash_instr_list(instr_list, base_ids);
     vector<LoopB> kernels;
     auto it = fuse_cache.find(key);
     if (it != fuse_cache.end() && it->second.base_ids.size() == base_ids.size()) {
@@ -545,7 +675,7 @@ vector<LoopB> EngineCUDA::kernels_for(vector<bh_instruction *> &instr_list) {
     } else {
         ++_stats.fuse_cache_misses;
         vector<Block> blocks;
-        kernels = get_kernel_list(instr_list, fusion_config, nullptr, &blocks);
+        kernels = get_kernel_list(instr_list, fusion_config, nullptr, &blocks, chooser ? &chooser : nullptr);
         fuse_cache[key] = FusePayload{std::move(blocks), base_ids};
     }
     _stats.time_fusion += seconds_since(t0);
@@ -567,23 +697,105 @@ void EngineCUDA::setConstructorFlag(vector<bh_instruction *> &instr_list) {
     }
 }
 
-void EngineCUDA::run_kernels(const vector<LoopB> &kernels) {
+// -------------------------------------------------------------------------------- flush plans
+EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const vector<bh_base *> &base_ids) {
+    FlushPlan plan;
+    unordered_map<const bh_base *, int> index;
+    for (size_t i = 0; i < base_ids.size(); ++i) index[base_ids[i]] = static_cast<int>(i);
+    auto idx = [&](const bh_base *b) -> int {
+        auto it = index.find(b);
+        return it == index.end() ? -1 : it->second;
+    };
+    // Dependency levels: a kernel runs after every earlier kernel it shares a written base with.
+    vector<int> last_write_level(base_ids.size(), -1), last_read_level(base_ids.size(), -1);
     for (const LoopB &kernel : kernels) {
-        ++_stats.kernels;
+        PlanKernel pk;
         if (!kernel.isSystemOnly()) {
             const auto tc = chrono::steady_clock::now();
-            const vector<LaunchUnit> units = lower_kernel(kernel, cg_opt);
+            vector<LaunchUnit> units = lower_kernel(kernel, cg_opt);
             _stats.time_codegen += seconds_since(tc);
-            for (const LaunchUnit &u : units) {
-                const vector<uint8_t> params = pack_params(u);
-                launch(u, params);
-            }
-            // Everything written by the kernel is newer on the device.
-            for (const InstrPtr &instr : all_instr(kernel)) {
-                if (!instr->operand.empty() && !instr->operand[0].isConstant()) host_stale.insert(instr->operand[0].base);
+            for (LaunchUnit &u : units) {
+                PlanUnit pu;
+                pu.compiled = compiled_for(u);
+                pu.ptr_base.assign(u.fields.size(), -1);
+                for (size_t f = 0; f < u.fields.size(); ++f)
+                    if (u.fields[f].kind == ParamField::PTR) pu.ptr_base[f] = idx(u.fields[f].base);
+                pu.unit = std::move(u);
+                pk.units.push_back(std::move(pu));
             }
         }
-        for (bh_base *base : kernel.getAllFrees()) free_base(base);
+        set<int> reads, writes;
+        for (const InstrPtr &instr : all_instr(kernel)) {
+            for (size_t o = 0; o < instr->operand.size(); ++o) {
+                const bh_view &v = instr->operand[o];
+                if (v.isConstant()) continue;
+                const int b = idx(v.base);
+                if (b < 0) continue;
+                if (o == 0) {
+                    writes.insert(b);
+                } else {
+                    reads.insert(b);
+                }
+            }
+        }
+        for (bh_base *f : kernel.getAllFrees()) {
+            const int b = idx(f);
+            if (b >= 0) {
+                pk.frees.push_back(b);
+                writes.insert(b);
+            }
+        }
+        pk.writes.assign(writes.begin(), writes.end());
+        int level = 0;
+        for (int b : reads) level = max(level, last_write_level[b] + 1);
+        for (int b : writes) level = max(level, max(last_write_level[b], last_read_level[b]) + 1);
+        pk.level = level;
+        const int end_level = level + max<int>(static_cast<int>(pk.units.size()), 1) - 1;
+        for (int b : reads) last_read_level[b] = max(last_read_level[b], end_level);
+        for (int b : writes) last_write_level[b] = max(last_write_level[b], end_level);
+        plan.nlevels = max(plan.nlevels, end_level + 1);
+        plan.kernels.push_back(std::move(pk));
+    }
+    return plan;
+}
+
+void EngineCUDA::run_plan(const FlushPlan &plan, const vector<bh_base *> &bases, const vector<bh_instruction *> &instrs) {
+    if (batch_mode == "off" || plan.kernels.size() < 2) {
+        for (const PlanKernel &pk : plan.kernels) {
+            ++_stats.kernels;
+            for (const PlanUnit &pu : pk.units) launch_plain(pu, bases, instrs);
+            for (int w : pk.writes) host_stale.insert(bases[static_cast<size_t>(w)]);
+            for (int f : pk.frees) free_base(bases[static_cast<size_t>(f)]);
+        }
+        return;
+    }
+    // Grouped execution: level by level, units of the same compiled kernel run as one launch.
+    vector<vector<const PlanUnit *>> by_level(static_cast<size_t>(plan.nlevels));
+    vector<vector<const PlanKernel *>> kernels_by_end(static_cast<size_t>(plan.nlevels));
+    for (const PlanKernel &pk : plan.kernels) {
+        ++_stats.kernels;
+        for (size_t j = 0; j < pk.units.size(); ++j) by_level[pk.level + j].push_back(&pk.units[j]);
+        kernels_by_end[pk.level + max<size_t>(pk.units.size(), 1) - 1].push_back(&pk);
+    }
+    for (size_t lv = 0; lv < by_level.size(); ++lv) {
+        map<const Compiled *, vector<const PlanUnit *>> groups;
+        vector<const Compiled *> order;
+        for (const PlanUnit *pu : by_level[lv]) {
+            if (!groups.count(pu->compiled)) order.push_back(pu->compiled);
+            groups[pu->compiled].push_back(pu);
+        }
+        for (const Compiled *c : order) {
+            const auto &g = groups[c];
+            if (g.size() == 1) {
+                launch_plain(*g[0], bases, instrs);
+            } else {
+                launch_batched(g, bases, instrs);
+            }
+        }
+        for (const PlanKernel *pk : kernels_by_end[lv]) {
+            for (int w : pk->writes) host_stale.insert(bases[static_cast<size_t>(w)]);
+            for (int f : pk->frees) free_base(bases[static_cast<size_t>(f)]);
+        }
     }
 }
 
@@ -593,8 +805,28 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
     vector<bh_instruction *> instr_list = remove_non_computed_system_instr(bhir->instr_list, frees);
     for (bh_base *base : frees) free_base(base);
     setConstructorFlag(instr_list);
-    const vector<LoopB> kernels = kernels_for(instr_list);
-    run_kernels(kernels);
+    int64_t oc = 0;
+    for (bh_instruction *i : instr_list) i->origin_id = oc++;
+    vector<bh_base *> base_ids;
+    bool sliding = false;
+    const uint64_t key = hash_instr_list(instr_list, base_ids, sliding);
+    if (staging_used > 0 && staging_event) {
+        // The previous flush's parameter copies must have left the staging area before reuse.
+        check(cudaEventSynchronize(static_cast<cudaEvent_t>(staging_event)), "cudaEventSynchronize(staging)");
+    }
+    staging_used = 0;
+    auto it = sliding ? plans.end() : plans.find(key);
+    if (it != plans.end() && it->second.nbases == base_ids.size()) {
+        ++_stats.plan_cache_hits;
+        run_plan(it->second, base_ids, instr_list);
+    } else {
+        ++_stats.plan_cache_misses;
+        const vector<LoopB> kernels = kernels_for(instr_list, key, base_ids);
+        FlushPlan plan = build_plan(kernels, base_ids);
+        plan.nbases = base_ids.size();
+        run_plan(plan, base_ids, instr_list);
+        if (!sliding) plans[key] = std::move(plan);
+    }
     copyToHost(bhir->getSyncs(), false);
     check_error_record();
     _stats.time_exec_host += seconds_since(t0);

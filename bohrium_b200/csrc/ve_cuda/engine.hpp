@@ -73,6 +73,10 @@ public:
     void record_execute_begin();
     void record_execute_end();
     double last_execute_ms();
+    // Events on the engine's stream around an arbitrary region (device time of everything launched
+    // between the two calls).
+    void timer_start();
+    double timer_stop_ms();
 
     std::string info() const;
     std::string statistics() const;
@@ -81,12 +85,16 @@ public:
     void *stream() const { return _stream; }
     int smCount() const { return _sm_count; }
 
-    // Launch a compiled unit with the given host-side parameter bytes.
-    void launch(const LaunchUnit &u, const std::vector<uint8_t> &params, const std::string *tag = nullptr);
-    // Build the parameter bytes of a unit for the current buffers.
-    std::vector<uint8_t> pack_params(const LaunchUnit &u);
-    // Compiled function for a unit (compiles on first use).
-    void *function_for(const LaunchUnit &u);
+    // A compiled unit: the plain kernel, its batched twin and their resident CTAs per SM.
+    struct Compiled {
+        void *fn = nullptr, *fn_batch = nullptr;
+        int occ = 1, occ_batch = 1;
+    };
+    // Compiled kernels of a unit (NVRTC on first use, then the in-memory or disk cache).
+    Compiled *compiled_for(const LaunchUnit &u);
+
+    // Merge chooser used when the fuser list contains "learned" (set by the cost model).
+    jitk::MergeChooser chooser;
 
     // Configuration
     bool prof = false;
@@ -114,18 +122,56 @@ private:
     std::unordered_map<bh_base *, DevBuf> buffers;
     std::set<bh_base *> host_stale; // device copy newer than the host copy
     std::set<void *> pinned;        // host blocks from host_alloc()
-    void *ev_begin = nullptr, *ev_end = nullptr;
+    void *ev_begin = nullptr, *ev_end = nullptr, *tm_begin = nullptr, *tm_end = nullptr;
 
-    // Kernel cache: source hash -> function
-    std::unordered_map<uint64_t, void *> functions;
-    std::unordered_map<void *, int> occupancy; // function -> resident CTAs per SM
+    // Kernel cache: source hash -> compiled kernels
+    std::unordered_map<uint64_t, Compiled> functions;
 
-    // Scratch arena for grid reductions and the error record.
+    // Scratch arena for grid reductions (tile partials), their completion counters and the error
+    // record of bounds-checked kernels.
     void *scratch = nullptr;
     int64_t scratch_bytes = 0;
     unsigned int *counters = nullptr;
+    int64_t counter_capacity = 0;
     unsigned long long *err_record = nullptr;
     void *ensure_scratch(int64_t bytes);
+    unsigned int *ensure_counters(int64_t n);
+
+    // Page-locked staging of batched-launch parameter blocks (recycled per flush).
+    uint8_t *staging_host = nullptr, *staging_dev = nullptr;
+    size_t staging_capacity = 0, staging_used = 0, last_staging_offset = 0;
+    std::vector<void *> staging_retired;
+    void *staging_event = nullptr;
+    uint8_t *staging_alloc(size_t bytes);
+    uint8_t *device_staging(size_t bytes);
+
+    // Flush plans: for a repeated instruction list (same structure, new bases/constants) the
+    // compiled launch units are reused and only their parameters are packed again.
+    struct PlanUnit {
+        LaunchUnit unit;
+        Compiled *compiled = nullptr;
+        std::vector<int> ptr_base; // per field: index of the base in flush order (PTR fields)
+    };
+    struct PlanKernel {
+        std::vector<PlanUnit> units;
+        std::vector<int> frees, writes;
+        int level = 0; // dependency level of the first unit
+    };
+    struct FlushPlan {
+        std::vector<PlanKernel> kernels;
+        int nlevels = 0;
+        size_t nbases = 0;
+    };
+    std::unordered_map<uint64_t, FlushPlan> plans;
+    FlushPlan build_plan(const std::vector<jitk::LoopB> &kernels, const std::vector<bh_base *> &base_ids);
+    void run_plan(const FlushPlan &plan, const std::vector<bh_base *> &bases, const std::vector<bh_instruction *> &instrs);
+    void pack_params(const PlanUnit &pu, const std::vector<bh_base *> &bases, const std::vector<bh_instruction *> &instrs,
+                     int64_t scratch_off, int64_t counter_idx, uint8_t *out);
+    void launch_plain(const PlanUnit &pu, const std::vector<bh_base *> &bases, const std::vector<bh_instruction *> &instrs);
+    void launch_batched(const std::vector<const PlanUnit *> &group, const std::vector<bh_base *> &bases,
+                        const std::vector<bh_instruction *> &instrs);
+    void record_begin(UnitRecord &r, void *&e0);
+    void record_end(UnitRecord &r, void *e0);
 
     // Fuse cache: instruction-list hash -> block list and base order
     struct FusePayload {
@@ -136,8 +182,8 @@ private:
 
     void copyToDevice(bh_base *base);
     void setConstructorFlag(std::vector<bh_instruction *> &instr_list);
-    std::vector<jitk::LoopB> kernels_for(std::vector<bh_instruction *> &instr_list);
-    void run_kernels(const std::vector<jitk::LoopB> &kernels);
+    std::vector<jitk::LoopB> kernels_for(std::vector<bh_instruction *> &instr_list, uint64_t key,
+                                         const std::vector<bh_base *> &base_ids);
     void free_base(bh_base *base);
     void check_error_record();
 };

@@ -66,6 +66,15 @@ public:
             return ss.str();
         } else if (msg == "CUDA: sync") {
             engine.synchronize();
+        } else if (msg == "CUDA: timer start") {
+            engine.timer_start();
+        } else if (msg == "CUDA: timer stop") {
+            ss.precision(9);
+            ss << engine.timer_stop_ms();
+            return ss.str();
+        } else if (msg == "CUDA: launches") {
+            ss << engine.stats().launches;
+            return ss.str();
         } else if (msg.rfind("host_alloc ", 0) == 0) {
             ss << reinterpret_cast<uintptr_t>(engine.host_alloc(stoll(msg.substr(11))));
             return ss.str();
