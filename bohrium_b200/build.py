@@ -79,7 +79,7 @@ def _link(target: str, objs: list[str], libs: list[str], verbose: bool, use_nvcc
     if use_nvcc:
         cmd = [NVCC, "-shared", "-o", target] + objs + ARCH + ["-Xlinker", "-rpath,$ORIGIN", "-L" + LIB] + libs
     else:
-        cmd = [CXX, "-shared", "-o", target] + objs + ["-Wl,-rpath,$ORIGIN", "-L" + LIB] + libs
+        cmd = [CXX, "-shared", "-o", target] + objs + ["-Wl,-rpath,$ORIGIN", "-Wl,--no-undefined", "-L" + LIB] + libs
     if verbose:
         print(" ".join(cmd))
     _run(cmd)

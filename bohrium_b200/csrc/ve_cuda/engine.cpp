@@ -583,6 +583,20 @@ uint8_t *EngineCUDA::staging_alloc(size_t bytes) {
 
 uint8_t *EngineCUDA::device_staging(size_t) { return staging_dev + last_staging_offset; }
 
+void EngineCUDA::check_error_record() {
+    if (!cg_opt.bounds_check) return;
+    unsigned long long v = 0;
+    check(cudaMemcpyAsync(&v, err_record, sizeof(v), cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(_stream)),
+          "cudaMemcpyAsync(err)");
+    synchronize();
+    if (v != 0) {
+        check(cudaMemset(err_record, 0, sizeof(v)), "cudaMemset(err)");
+        last_error_index = v & 0x7fffffffffffffffULL;
+        throw runtime_error("bounds check: a generated kernel indexed element " + to_string(last_error_index) +
+                            " outside its array");
+    }
+}
+
 // ------------------------------------------------------------------------------- fuse cache
 namespace {
 // Structural hash of an instruction list: opcodes, sweep axes, the constant slot, constructor
