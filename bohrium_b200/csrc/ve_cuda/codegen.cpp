@@ -26,6 +26,7 @@ const char *sched_name(Sched s) {
     switch (s) {
         case Sched::FLAT: return "flat";
         case Sched::GRID_REDUCE: return "grid_reduce";
+        case Sched::SPLIT_REDUCE: return "split_reduce";
         case Sched::OUTER_REDUCE: return "outer_reduce";
         case Sched::SCAN1D: return "scan1d";
         case Sched::SERIAL: return "serial";
@@ -40,11 +41,24 @@ int64_t LaunchUnit::work_items() const {
             return rows * ((cols + per - 1) / per);
         }
         case Sched::GRID_REDUCE: return (cols + kReduceTile - 1) / kReduceTile;
+        case Sched::SPLIT_REDUCE: return (rows * cols + kThreads - 1) / kThreads * chunks;
         case Sched::OUTER_REDUCE: return (rows * cols + kThreads - 1) / kThreads;
         case Sched::SCAN1D: return (cols + kScanChunk - 1) / kScanChunk;
         case Sched::SERIAL: return 1;
     }
     return 1;
+}
+
+int64_t LaunchUnit::scratch_bytes() const {
+    if (sched == Sched::GRID_REDUCE) return work_items() * scratch_bytes_per_tile;
+    if (sched == Sched::SPLIT_REDUCE) return 8 * static_cast<int64_t>(nred) * chunks * rows * cols;
+    return 0;
+}
+
+int64_t LaunchUnit::counters_needed() const {
+    if (sched == Sched::GRID_REDUCE) return 1;
+    if (sched == Sched::SPLIT_REDUCE) return (rows * cols + kThreads - 1) / kThreads;
+    return 0;
 }
 
 string cuda_type(bh_type t) {
@@ -844,6 +858,183 @@ LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) 
     return u;
 }
 
+// Parallel points below which an inner reduction is split along its swept axis, and the number of
+// (point, chunk) threads the split aims at. Both are fixed constants so that the summation order
+// depends on the array shapes only.
+constexpr int64_t kSplitTargetThreads = 600000;
+constexpr int64_t kSplitMinChunk = 16;
+
+// The swept sub-loop of `inner` when `inner` is [identity instructions] [swept innermost sub-loop]
+// [instructions], and the sub-loop's sweeps are reductions; nullptr otherwise.
+const LoopB *split_candidate(const LoopB &inner) {
+    const LoopB *sub = nullptr;
+    bool after = false;
+    for (const Block &b : inner._block_list) {
+        if (b.isInstr()) {
+            if (!after) {
+                const bh_instruction &i = *b.getInstr();
+                if (!(i.opcode == BH_IDENTITY && i.operand.size() == 2 && i.operand[1].isConstant())) return nullptr;
+            }
+            continue;
+        }
+        if (sub != nullptr) return nullptr;
+        sub = &b.getLoop();
+        after = true;
+    }
+    if (sub == nullptr || sub->_sweeps.empty() || !sub->isInnermost()) return nullptr;
+    for (const InstrPtr &s : sub->_sweeps)
+        if (!bh_opcode_is_reduction(s->opcode) || !jitk::sweeping_innermost_axis(s)) return nullptr;
+    // The identities must initialise outputs of these sweeps.
+    set<ViewKey> outs;
+    for (const InstrPtr &s : sub->_sweeps) outs.insert(ViewKey(s->operand[0]));
+    for (const Block &b : inner._block_list) {
+        if (!b.isInstr()) break;
+        if (!outs.count(ViewKey(b.getInstr()->operand[0]))) return nullptr;
+    }
+    return sub;
+}
+
+int64_t split_chunks(int64_t points, int64_t len) {
+    if (points <= 0 || len <= 0) return 1;
+    const int64_t want = (kSplitTargetThreads + points - 1) / points;
+    const int64_t most = max<int64_t>(1, len / kSplitMinChunk);
+    return max<int64_t>(1, min(want, most));
+}
+
+LaunchUnit lower_split_reduce(const LoopB &loop, unsigned P, const CodegenOptions &opt) {
+    LaunchUnit u;
+    u.sched = Sched::SPLIT_REDUCE;
+    const Block holder(loop);
+    const LoopB &L = holder.getLoop();
+    const vector<const LoopB *> chain = jitk::get_first_loop_blocks(L);
+    const LoopB &inner = *chain[P - 1];
+    const LoopB &sub = *split_candidate(inner);
+    set<const bh_instruction *> folded;
+    for (const Block &b : inner._block_list) {
+        if (!b.isInstr()) break;
+        folded.insert(b.getInstr().get());
+    }
+    Symbols sym = build_symbols({&holder}, folded);
+    vector<InstrPtr> reds(sub._sweeps.begin(), sub._sweeps.end());
+    sort(reds.begin(), reds.end(), [](const InstrPtr &a, const InstrPtr &b) { return a->origin_id < b->origin_id; });
+    u.nred = static_cast<int>(reds.size());
+    int64_t rows = 1;
+    for (unsigned r = 0; r + 1 < P; ++r) rows *= chain[r]->size;
+    u.rows = rows;
+    u.cols = inner.size;
+    const int64_t points = rows * inner.size;
+    u.chunks = split_chunks(points, sub.size);
+    const int64_t chunk_len = (sub.size + u.chunks - 1) / u.chunks;
+    ParamLayout pl;
+    add_common_fields(sym, pl, opt);
+    pl.add(work_field(points), "bh_i64", "points");
+    pl.add(work_field(u.chunks), "bh_i64", "chunks");
+    pl.add(work_field(chunk_len), "bh_i64", "chunk_len");
+    pl.add(work_field(u.work_items()), "bh_i64", "work");
+    ParamField fs{ParamField::SCRATCH};
+    pl.add(fs, "unsigned char*", "scratch");
+    ParamField fc{ParamField::COUNTER};
+    pl.add(fc, "unsigned int*", "counter");
+
+    stringstream body;
+    Emitter em(sym, body, opt);
+    vector<string> ctypes, idents;
+    for (size_t k = 0; k < reds.size(); ++k) {
+        const bh_type t = reds[k]->operand[0].base->dtype();
+        ctypes.push_back(cuda_type(t));
+        idents.push_back(constant_literal(jitk::sweep_identity(reds[k]->opcode, t)));
+        em.external_acc[ViewKey(reds[k]->operand[0])] = "pacc" + to_string(k);
+    }
+    const int sub_lid = sym.loop_id.at(&sub);
+    body << "__device__ void bh_work(const P &p, bh_i64 w) {\n";
+    body << pointer_locals(sym);
+    body << "    __shared__ bool am_last;\n";
+    body << "    const bh_i64 pb = w / p.chunks, chunk = w - pb * p.chunks;\n";
+    body << "    const bh_i64 pt = pb * " << kThreads << " + threadIdx.x;\n";
+    for (size_t k = 0; k < reds.size(); ++k)
+        body << "    " << ctypes[k] << "* part" << k << " = (" << ctypes[k] << "*)(p.scratch + " << 8 * k
+             << " * p.chunks * p.points);\n";
+    // Decompose the point into the threaded indices i0..i{P-1}.
+    auto decompose = [&](int ind) {
+        const string sp(static_cast<size_t>(ind), ' ');
+        body << sp << "bh_i64 rem = pt;\n";
+        for (int r = static_cast<int>(P) - 1; r >= 0; --r) {
+            const int lid = sym.loop_id.at(chain[r]);
+            if (r == 0) {
+                body << sp << "const bh_i64 i0 = rem;\n";
+            } else {
+                body << sp << "const bh_i64 i" << r << " = rem % p.n" << lid << "; rem /= p.n" << lid << ";\n";
+            }
+        }
+        body << sp << "(void)rem;\n";
+    };
+    body << "    if (pt < p.points) {\n";
+    decompose(8);
+    {
+        Scope scope;
+        declare_chain_temps(em, sym, scope, chain, P, body, 8);
+        for (size_t k = 0; k < reds.size(); ++k) body << "        " << ctypes[k] << " pacc" << k << " = " << idents[k] << ";\n";
+        body << "        const bh_i64 lo = chunk * p.chunk_len;\n";
+        body << "        const bh_i64 hi = min(lo + p.chunk_len, (bh_i64)p.n" << sub_lid << ");\n";
+        body << "        for (bh_i64 i" << P << " = lo; i" << P << " < hi; ++i" << P << ") {\n";
+        Scope s1;
+        s1.parent = &scope;
+        em.write_body(sub, s1, 12);
+        body << "        }\n";
+        for (size_t k = 0; k < reds.size(); ++k)
+            body << "        part" << k << "[chunk * p.points + pt] = pacc" << k << ";\n";
+    }
+    body << "    }\n";
+    body << "    __syncthreads();\n";
+    body << "    if (threadIdx.x == 0) {\n";
+    body << "        __threadfence();\n";
+    body << "        am_last = atomicAdd(p.counter + pb, 1u) == (unsigned)(p.chunks - 1);\n";
+    body << "    }\n";
+    body << "    __syncthreads();\n";
+    body << "    if (!am_last) return;\n";
+    body << "    __threadfence();\n";
+    body << "    if (threadIdx.x == 0) p.counter[pb] = 0u;\n";
+    body << "    if (pt >= p.points) return;\n";
+    {
+        decompose(4);
+        Scope scope;
+        declare_chain_temps(em, sym, scope, chain, P - 1, body, 4);
+        for (size_t k = 0; k < reds.size(); ++k) {
+            body << "    " << ctypes[k] << " pacc" << k << " = " << idents[k] << ";\n";
+            body << "    for (bh_i64 c = 0; c < p.chunks; ++c) {\n";
+            body << "        const " << ctypes[k] << " x = ((volatile " << ctypes[k] << "*)part" << k
+                 << ")[c * p.points + pt];\n";
+            body << "        pacc" << k << " = " << reduce_expr(reds[k]->opcode, "pacc" + to_string(k), "x") << ";\n";
+            body << "    }\n";
+        }
+        // Instructions after the swept sub-loop, then the reduction outputs.
+        for (const bh_base *b : em.sorted_temps(inner)) {
+            if (sym.temps.count(b) && !scope.is_tmp(b)) {
+                scope.tmps.insert(b);
+                body << "    " << cuda_type(b->dtype()) << " t" << sym.base_index(b) << ";\n";
+            }
+        }
+        bool after = false;
+        for (const Block &b : inner._block_list) {
+            if (!b.isInstr()) {
+                after = true;
+                continue;
+            }
+            if (after) em.write_instr(*b.getInstr(), scope, 4);
+        }
+        for (size_t k = 0; k < reds.size(); ++k) {
+            if (sym.temps.count(reds[k]->operand[0].base)) continue;
+            body << "    " << em.array_ref(reds[k]->operand[0], reds[k]->sweep_axis()) << " = pacc" << k << ";\n";
+        }
+    }
+    body << "}\n" << kWrappers;
+    u.fields = pl.fields;
+    u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
+    u.elements = points * sub.size;
+    finish_source(u, pl.decl.str(), body.str(), opt);
+    return u;
+}
+
 // CTA-wide deterministic tree reduction of `v` (fixed xor-shuffle butterfly, then warp 0); the
 // result is valid in thread 0.
 string block_reduce_fn(const string &ctype, const string &fname, bh_opcode op, const string &identity) {
@@ -1090,7 +1281,15 @@ vector<LaunchUnit> lower_kernel(const LoopB &kernel, const CodegenOptions &opt) 
                 units.push_back(lower_flat(il->getLoop(), Pi, opt));
             }
             pending_id_loops.clear();
-            units.push_back(lower_flat(L, P, opt));
+            const vector<const LoopB *> chain = jitk::get_first_loop_blocks(L);
+            const LoopB *sub = split_candidate(*chain[P - 1]);
+            int64_t points = 1;
+            for (unsigned r = 0; r < P; ++r) points *= chain[r]->size;
+            if (sub != nullptr && split_chunks(points, sub->size) > 1) {
+                units.push_back(lower_split_reduce(L, P, opt));
+            } else {
+                units.push_back(lower_flat(L, P, opt));
+            }
             continue;
         }
         bool all_reduce = !L._sweeps.empty();

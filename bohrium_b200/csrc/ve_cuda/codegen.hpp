@@ -13,6 +13,11 @@
 //                 folds the tile partials in tile order. The summation order depends only on the
 //                 element count, never on the grid size, so batched and plain launches agree bit
 //                 for bit.
+//   SPLIT_REDUCE  a FLAT nest with few parallel points whose innermost threaded loop holds one
+//                 swept sub-loop (axis reductions such as max over the rows of a 2-D array): the
+//                 swept axis is cut into chunks so that ~600K threads work at once; each thread folds
+//                 its chunk in order, and the last CTA of each 256-point block folds the chunk
+//                 partials in chunk order (deterministic) and runs the instructions that follow.
 //   OUTER_REDUCE  a nest that reduces its outermost axis into an array: threads own the output
 //                 elements (the inner parallel ranks) and loop over the reduced axis.
 //   SCAN1D        a 1-D nest whose outermost axis is an accumulate (cumulative sum/product):
@@ -33,7 +38,7 @@
 namespace bohrium {
 namespace cuda {
 
-enum class Sched { FLAT, GRID_REDUCE, OUTER_REDUCE, SCAN1D, SERIAL };
+enum class Sched { FLAT, GRID_REDUCE, SPLIT_REDUCE, OUTER_REDUCE, SCAN1D, SERIAL };
 const char *sched_name(Sched s);
 
 constexpr int kThreads = 256;      // threads per CTA for every schedule
@@ -57,9 +62,13 @@ struct LaunchUnit {
     int V = 1;          // elements per thread along the innermost parallel rank (FLAT)
     std::vector<ParamField> fields;
     int64_t rows = 1, cols = 1; // FLAT / OUTER_REDUCE index space; GRID_REDUCE/SCAN1D: cols = length
-    int nred = 0;               // GRID_REDUCE: number of reductions
+    int nred = 0;               // GRID_REDUCE / SPLIT_REDUCE: number of reductions
     int64_t scratch_bytes_per_tile = 0; // GRID_REDUCE: bytes of partials per tile (all reductions)
+    int64_t chunks = 1;         // SPLIT_REDUCE: chunks of the swept axis
     int64_t work_items() const;
+    int64_t scratch_bytes() const;   // partials in the scratch arena
+    int64_t counters_needed() const; // completion counters
+
     // Bytes of arrays read/written by this unit (algorithmic, temporaries excluded).
     int64_t algorithmic_bytes = 0;
     int64_t elements = 0;

@@ -405,10 +405,8 @@ EngineCUDA::Compiled *EngineCUDA::compiled_for(const LaunchUnit &u) {
 }
 
 // ------------------------------------------------------------------------------------ launch
-// Scratch bytes a unit needs for its tile partials.
-static int64_t unit_scratch(const LaunchUnit &u) {
-    return u.sched == Sched::GRID_REDUCE ? u.work_items() * u.scratch_bytes_per_tile : 0;
-}
+// Scratch bytes a unit needs for its partials.
+static int64_t unit_scratch(const LaunchUnit &u) { return u.scratch_bytes(); }
 
 void EngineCUDA::pack_params(const PlanUnit &pu, const vector<bh_base *> &bases,
                              const vector<bh_instruction *> &instrs, int64_t scratch_off, int64_t counter_idx,
@@ -482,7 +480,7 @@ void EngineCUDA::launch_plain(const PlanUnit &pu, const vector<bh_base *> &bases
     const int64_t work = u.work_items();
     if (work == 0) return;
     ensure_scratch(unit_scratch(u));
-    ensure_counters(1);
+    ensure_counters(max<int64_t>(u.counters_needed(), 1));
     vector<uint8_t> params(u.fields.size() * 8);
     pack_params(pu, bases, instrs, 0, 0, params.data());
     const int64_t resident = static_cast<int64_t>(_sm_count) * pu.compiled->occ;
@@ -505,14 +503,16 @@ void EngineCUDA::launch_batched(const vector<const PlanUnit *> &group, const vec
     const size_t psize = proto.unit.fields.size() * 8;
     const size_t n = group.size();
     // Per-item scratch and counters.
-    int64_t scratch_total = 0;
-    vector<int64_t> scratch_off(n);
+    int64_t scratch_total = 0, counter_total = 0;
+    vector<int64_t> scratch_off(n), counter_off(n);
     for (size_t k = 0; k < n; ++k) {
         scratch_off[k] = scratch_total;
         scratch_total += (unit_scratch(group[k]->unit) + 255) / 256 * 256;
+        counter_off[k] = counter_total;
+        counter_total += group[k]->unit.counters_needed();
     }
     ensure_scratch(scratch_total);
-    ensure_counters(static_cast<int64_t>(n));
+    ensure_counters(max<int64_t>(counter_total, 1));
     // Items (parameter structs) followed by the prefix sums of their work counts.
     const size_t items_bytes = (psize * n + 15) / 16 * 16;
     const size_t bytes = items_bytes + (n + 1) * sizeof(int64_t);
@@ -520,7 +520,7 @@ void EngineCUDA::launch_batched(const vector<const PlanUnit *> &group, const vec
     int64_t *prefix = reinterpret_cast<int64_t *>(host + items_bytes);
     int64_t total = 0;
     for (size_t k = 0; k < n; ++k) {
-        pack_params(*group[k], bases, instrs, scratch_off[k], static_cast<int64_t>(k), host + k * psize);
+        pack_params(*group[k], bases, instrs, scratch_off[k], counter_off[k], host + k * psize);
         prefix[k] = total;
         total += group[k]->unit.work_items();
     }
@@ -696,6 +696,67 @@ vector<LoopB> EngineCUDA::kernels_for(vector<bh_instruction *> &instr_list, uint
     return kernels;
 }
 
+// One pass over the flushed list (core/jitk/instruction.cpp:580-593 and engine.cpp:338-351 of the
+// reference, fused): drop BH_NONE/BH_TALLY, free bases that are freed without being computed, set
+// the constructor flags (first use is as an output and the base has neither device nor host data),
+// number instructions (origin ids) and bases (first appearance), and hash the structure.
+uint64_t EngineCUDA::prepare(vector<bh_instruction> &list, vector<bh_instruction *> &out, vector<bh_base *> &base_ids,
+                             bool &sliding) {
+    Hasher h;
+    unordered_map<const bh_base *, uint32_t> ids;
+    ids.reserve(list.size() * 2 + 16);
+    out.reserve(list.size());
+    sliding = false;
+    vector<bh_base *> dead;
+    for (bh_instruction &instr : list) {
+        if (instr.opcode == BH_NONE || instr.opcode == BH_TALLY) continue;
+        if (instr.opcode == BH_FREE && !ids.count(instr.operand[0].base)) {
+            dead.push_back(instr.operand[0].base);
+            continue;
+        }
+        instr.origin_id = static_cast<int64_t>(out.size());
+        instr.constructor = false;
+        h.add(static_cast<uint64_t>(instr.opcode));
+        h.add(static_cast<uint64_t>(instr.sweep_axis()));
+        for (size_t o = 0; o < instr.operand.size(); ++o) {
+            const bh_view &v = instr.operand[o];
+            if (v.isConstant()) {
+                h.add(0xC0115747ULL);
+                continue;
+            }
+            auto it = ids.find(v.base);
+            uint64_t id;
+            if (it == ids.end()) {
+                id = ids.size();
+                ids.emplace(v.base, static_cast<uint32_t>(id));
+                base_ids.push_back(v.base);
+                if (o == 0 && instr.opcode != BH_FREE && !buffers.count(v.base) && v.base->getDataPtr() == nullptr)
+                    instr.constructor = true;
+            } else {
+                id = it->second;
+            }
+            h.add(id);
+            h.add(static_cast<uint64_t>(v.base->dtype()));
+            h.add(static_cast<uint64_t>(v.base->nelem()));
+            if (v.hasSlide()) {
+                sliding = true;
+            } else {
+                h.add(static_cast<uint64_t>(v.start));
+            }
+            h.add(static_cast<uint64_t>(v.ndim));
+            for (int64_t d = 0; d < v.ndim; ++d) {
+                h.add(static_cast<uint64_t>(v.shape[d]));
+                h.add(static_cast<uint64_t>(v.stride[d]));
+            }
+        }
+        h.add(instr.constructor ? 1 : 0);
+        out.push_back(&instr);
+    }
+    h.add(out.size());
+    for (bh_base *b : dead) free_base(b);
+    return h.h;
+}
+
 void EngineCUDA::setConstructorFlag(vector<bh_instruction *> &instr_list) {
     // Arrays already on the device or with host data are not constructed by this flush.
     set<const bh_base *> constructed;
@@ -815,15 +876,12 @@ void EngineCUDA::run_plan(const FlushPlan &plan, const vector<bh_base *> &bases,
 
 void EngineCUDA::handleExecution(BhIR *bhir) {
     const auto t0 = chrono::steady_clock::now();
-    set<bh_base *> frees;
-    vector<bh_instruction *> instr_list = remove_non_computed_system_instr(bhir->instr_list, frees);
-    for (bh_base *base : frees) free_base(base);
-    setConstructorFlag(instr_list);
-    int64_t oc = 0;
-    for (bh_instruction *i : instr_list) i->origin_id = oc++;
+    vector<bh_instruction *> instr_list;
     vector<bh_base *> base_ids;
     bool sliding = false;
-    const uint64_t key = hash_instr_list(instr_list, base_ids, sliding);
+    const uint64_t key = prepare(bhir->instr_list, instr_list, base_ids, sliding);
+    const auto t1 = chrono::steady_clock::now();
+    _stats.time_prepare += chrono::duration<double>(t1 - t0).count();
     if (staging_used > 0 && staging_event) {
         // The previous flush's parameter copies must have left the staging area before reuse.
         check(cudaEventSynchronize(static_cast<cudaEvent_t>(staging_event)), "cudaEventSynchronize(staging)");
@@ -841,12 +899,25 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
         run_plan(plan, base_ids, instr_list);
         if (!sliding) plans[key] = std::move(plan);
     }
-    copyToHost(bhir->getSyncs(), false);
+    const auto t2 = chrono::steady_clock::now();
+    _stats.time_launch += chrono::duration<double>(t2 - t1).count();
+    copyToHost(bhir->_syncs, false);
     check_error_record();
     _stats.time_exec_host += seconds_since(t0);
 }
 
 void EngineCUDA::handleExtmethod(BhIR *bhir) {
+    // Only a list that contains extension methods needs splitting (and copying).
+    bool any = false;
+    if (!comp.extmethods.empty() || !comp.child_extmethods.empty()) {
+        for (const bh_instruction &instr : bhir->instr_list) {
+            if (comp.extmethods.count(instr.opcode) || comp.child_extmethods.count(instr.opcode)) {
+                any = true;
+                break;
+            }
+        }
+    }
+    if (!any) return;
     vector<bh_instruction> instr_list;
     for (bh_instruction &instr : bhir->instr_list) {
         auto ext = comp.extmethods.find(instr.opcode);
@@ -870,7 +941,7 @@ void EngineCUDA::handleExtmethod(BhIR *bhir) {
             instr_list.push_back(instr);
         }
     }
-    bhir->instr_list = instr_list;
+    bhir->instr_list = std::move(instr_list);
 }
 
 namespace {
@@ -955,7 +1026,9 @@ string EngineCUDA::statistics() const {
        << "\nkernel_cache_misses: " << _stats.kernel_cache_misses << "\ndisk_cache_hits: " << _stats.disk_cache_hits
        << "\nbytes_h2d: " << _stats.bytes_h2d << "\nbytes_d2h: " << _stats.bytes_d2h
        << "\ntime_fusion: " << _stats.time_fusion << "\ntime_codegen: " << _stats.time_codegen
-       << "\ntime_compile: " << _stats.time_compile << "\ntime_exec_host: " << _stats.time_exec_host << "\n";
+       << "\ntime_compile: " << _stats.time_compile << "\ntime_exec_host: " << _stats.time_exec_host
+       << "\ntime_prepare: " << _stats.time_prepare << "\ntime_launch: " << _stats.time_launch
+       << "\nplan_cache_hits: " << _stats.plan_cache_hits << "\nplan_cache_misses: " << _stats.plan_cache_misses << "\n";
     if (!_stats.records.empty()) {
         ss << "units:\n";
         for (const UnitRecord &r : _stats.records)

@@ -46,6 +46,7 @@ struct Stats {
     uint64_t bytes_h2d = 0, bytes_d2h = 0;
     uint64_t serial_units = 0;
     double time_fusion = 0, time_codegen = 0, time_compile = 0, time_exec_host = 0;
+    double time_prepare = 0, time_launch = 0; // host time: list clean-up + hashing, plan execution
     std::vector<UnitRecord> records; // filled when profiling
 };
 
@@ -182,6 +183,8 @@ private:
 
     void copyToDevice(bh_base *base);
     void setConstructorFlag(std::vector<bh_instruction *> &instr_list);
+    uint64_t prepare(std::vector<bh_instruction> &list, std::vector<bh_instruction *> &out,
+                     std::vector<bh_base *> &base_ids, bool &sliding);
     std::vector<jitk::LoopB> kernels_for(std::vector<bh_instruction *> &instr_list, uint64_t key,
                                          const std::vector<bh_base *> &base_ids);
     void free_base(bh_base *base);

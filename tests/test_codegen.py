@@ -39,14 +39,14 @@ def test_black_scholes_iteration_is_one_kernel():
     assert scheds.count("grid_reduce") == 1 and len(units) <= 2, scheds
 
 
-def test_heat_step_fuses_stencil_write_and_partial_max():
+def test_heat_step_fuses_stencil_write_and_split_partial_max():
     def prog(rt):
         a = bh.empty(rt, (64, 64), np.float32)
         b = bh.empty(rt, (64, 64), np.float32)
         return [W.heat_step(a, b), b]
     res, units = plan(prog)
     scheds = [u["sched"] for u in units]
-    assert scheds == ["flat", "grid_reduce"], scheds
+    assert scheds == ["split_reduce", "grid_reduce"], scheds
 
 
 def test_batching_systems_lower_to_one_unit_each():

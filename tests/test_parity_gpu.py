@@ -171,3 +171,53 @@ def test_repeat_with_condition_and_slides(gpu_rt, oracle_rt):
         rt.ex.execute(ir.Flush([add, less], nrepeats=20, condition=cond.base))
         results.append(acc.numpy()[0])
     assert results[0] == results[1] == float(sum(range(11)))
+
+
+@pytest.mark.parametrize("shape,axis", [((100_000, 3), 0), ((4096, 50), 0), ((3, 70_000), 1), ((2000, 2000), 0),
+                                        ((16, 9000, 4), 1)])
+def test_split_reductions(gpu_rt, oracle_rt, shape, axis):
+    """Axis reductions with few outputs and a long swept axis (the split-reduction schedule),
+    including a fused consumer of the reduction (mean = sum / n)."""
+    def prog(rt):
+        A = P.data(shape, np.float64, 11)
+        a = bh.array(rt, A)
+        m = a.max(axis)
+        s = a.sum(axis)
+        mean = s / float(shape[axis])
+        return [m, s, mean]
+    g, o = both(gpu_rt, oracle_rt, prog)
+    assert_close(g[0], o[0], 0, 0, "max")
+    assert_close(g[1], o[1], 1e-12, 1e-12, "sum")
+    assert_close(g[2], o[2], 1e-12, 1e-12, "mean")
+
+
+def test_grouped_launches_are_bit_identical(gpu_executor):
+    """Independent kernels of one flush run as one grouped launch; the results equal the plain
+    one-launch-per-kernel results bit for bit."""
+    from bohrium_b200 import workloads as W
+    rt = bh.Runtime(gpu_executor)
+    lengths = W.batching_lengths(64, 256, 20000, 9)
+    xs = [bh.array(rt, np.random.default_rng(i).random(int(n), dtype=np.float32)) for i, n in enumerate(lengths)]
+    rt.flush()
+    outs = []
+    for x in xs:
+        y = W.batching_chain(x)
+        outs += [y, y.sum(), y.max()]
+    ir = gpu_executor.compile(rt.take())
+    results = {}
+    try:
+        for mode in ["off", "grouped"]:
+            gpu_executor.message(f"CUDA: batch {mode}")
+            l0 = int(gpu_executor.message("CUDA: launches"))
+            ir.execute()
+            ir.execute()
+            launches = int(gpu_executor.message("CUDA: launches")) - l0
+            results[mode] = [gpu_executor.peek(o.base) for o in outs]
+            if mode == "grouped":
+                assert launches <= 4, launches
+            else:
+                assert launches == 2 * 64, launches
+    finally:
+        gpu_executor.message("CUDA: batch off")
+    for p, q in zip(results["off"], results["grouped"]):
+        assert np.array_equal(p, q)
