@@ -155,6 +155,18 @@ def bs_bytes(n):
     return 3 * 8 * n + 8
 
 
+def stats(ex) -> dict:
+    out = {}
+    for line in ex.message("statistic").splitlines():
+        if ":" in line and not line.startswith(" "):
+            k, v = line.split(":", 1)
+            try:
+                out[k.strip()] = float(v)
+            except ValueError:
+                pass
+    return out
+
+
 def sync_read(bh, ex, outs):
     """One flush that syncs every result base, then read the host copies."""
     ex.execute(bh.ir.Flush([], syncs=[o.base for o in outs]))
@@ -170,7 +182,7 @@ def run_ours(args, world, rank, local):
     peak, peak_kind = peaks()
 
     # ---- device-resident throughput -----------------------------------------------------
-    n = BS_OPTIONS
+    n = args.bs_options
     inputs, _, irs, outs, host_inputs = build_black_scholes(bh, W, rt, ex, n)
     step = lambda: [ir.execute() for ir in irs]
     for _ in range(max(args.warmup, 3)):
@@ -178,6 +190,7 @@ def run_ours(args, world, rank, local):
     ex.message("CUDA: sync")
     barrier(world)
     launches0 = int(ex.message("CUDA: launches"))
+    host0 = stats(ex)
     with Clocks(local) as clk:
         ex.message("CUDA: timer start")
         t0 = time.perf_counter()
@@ -186,7 +199,11 @@ def run_ours(args, world, rank, local):
         dev_ms = float(ex.message("CUDA: timer stop"))
         wall = time.perf_counter() - t0
     launches = int(ex.message("CUDA: launches")) - launches0
+    host1 = stats(ex)
     clocks = clk.summary()
+    nflush = args.steps * BS_ITERS
+    host_us = {k: round((host1.get(k, 0) - host0.get(k, 0)) * 1e6 / nflush, 2)
+               for k in ("time_exec_host", "time_prepare", "time_launch")}
     # Per-launch kernel durations with CUDA events (one profiled step after the timed region).
     ex.message("CUDA: prof on")
     ex.message("statistic_enable_and_reset")
@@ -251,7 +268,8 @@ def run_ours(args, world, rank, local):
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "flush_ms_device": round(dev_ms_max / args.steps / BS_ITERS, 4),
                    "flush_ms_wall": round(wall * 1e3 / args.steps / BS_ITERS, 4),
-                   "frac_of_peak": round(value / world / peak, 4), "result_check": check_ok},
+                   "frac_of_peak": round(value / world / peak, 4), "result_check": check_ok,
+                   "host_us_per_flush": host_us},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
     }
     if extra:
@@ -330,6 +348,7 @@ def run_extra(bh, W, ex, rt, peak):
             ir.execute()
         ex.message("CUDA: sync")
         l0 = int(ex.message("CUDA: launches"))
+        h0 = stats(ex)
         reps = 5
         ex.message("CUDA: timer start")
         t0 = time.perf_counter()
@@ -339,7 +358,11 @@ def run_extra(bh, W, ex, rt, peak):
         wall = (time.perf_counter() - t0) * 1e3 / reps
         res[mode] = {"flush_ms_device": round(ms, 3), "flush_ms_wall": round(wall, 3),
                      "launches_per_flush": (int(ex.message("CUDA: launches")) - l0) // reps,
+                     "host_ms_per_flush": None,
                      "GB/s": round((8 * total + 8 * 4096) / (max(ms, wall) / 1e3) / 1e9, 1)}
+        h1 = stats(ex)
+        res[mode]["host_ms_per_flush"] = {k: round((h1.get(k, 0) - h0.get(k, 0)) * 1e3 / reps, 3)
+                                          for k in ("time_exec_host", "time_prepare", "time_launch")}
     ex.message("CUDA: batch off")
     # bit-identical results between the two forms
     ex.message("CUDA: batch grouped")
@@ -407,6 +430,7 @@ def main():
     ap.add_argument("--no-extra", dest="extra", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-options", type=int, default=BS_OPTIONS)
+    ap.add_argument("--bs-options", type=int, default=BS_OPTIONS, help="options of the headline workload")
     args = ap.parse_args()
     world, rank, local = dist_init()
     if args.impl == "reference":
