@@ -113,7 +113,29 @@ BhIR *decode(const int64_t *w, int64_t n, bh_base *const *syncs, int64_t nsyncs,
         }
     }
     set<bh_base *> s(syncs, syncs + nsyncs);
-    return new BhIR(std::move(list), std::move(s), nrepeats, cond);
+    BhIR *ir = new BhIR(std::move(list), std::move(s), nrepeats, cond);
+    if (nslide == 0) {
+        // The handle is immutable: fingerprint its encoding once so that an engine can recognise
+        // the repeated flush (sliding views change between executions, so they get none).
+        uint64_t h = 0xcbf29ce484222325ULL ^ static_cast<uint64_t>(n);
+        auto mix = [&h](uint64_t v) {
+            v *= 0x9E3779B97F4A7C15ULL;
+            h = (h ^ (v ^ (v >> 29))) * 0x100000001B3ULL;
+        };
+        for (int64_t k = 0; k < n; ++k) mix(static_cast<uint64_t>(w[k]));
+        // Base identity includes element type and size (a base address can be reused).
+        for (const bh_instruction &instr : ir->instr_list)
+            for (const bh_view &v : instr.operand)
+                if (!v.isConstant()) {
+                    mix(static_cast<uint64_t>(v.base->dtype()));
+                    mix(static_cast<uint64_t>(v.base->nelem()));
+                }
+        for (int64_t k = 0; k < nsyncs; ++k) mix(reinterpret_cast<uint64_t>(syncs[k]));
+        mix(nrepeats);
+        mix(reinterpret_cast<uint64_t>(cond));
+        ir->_fingerprint = h | 1ULL;
+    }
+    return ir;
 }
 } // namespace
 

@@ -843,14 +843,27 @@ LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) 
     }
     body << "    (void)rem;\n";
     body << "    const bh_i64 cbase = chunk * " << per << " + threadIdx.x;\n";
+    // The element body is written once and used twice: full chunks run without bounds checks (so
+    // the compiler can issue every load of the unrolled loop early), the last chunk with them.
+    stringstream elem;
+    {
+        Emitter eb(sym, elem, opt);
+        Scope scope;
+        declare_chain_temps(eb, sym, scope, chain, P - 1, elem, 12);
+        eb.write_body(inner, scope, 12);
+    }
+    const string n_inner = "p.n" + to_string(sym.loop_id.at(&inner));
+    body << "    if ((chunk + 1) * " << per << " <= " << n_inner << ") {\n";
     body << "#pragma unroll\n";
-    body << "    for (int j = 0; j < " << u.V << "; ++j) {\n";
-    body << "        const bh_i64 i" << (P - 1) << " = cbase + j * " << kThreads << ";\n";
-    body << "        if (i" << (P - 1) << " >= p.n" << sym.loop_id.at(&inner) << ") break;\n";
-    Scope scope;
-    declare_chain_temps(em, sym, scope, chain, P - 1, body, 8);
-    em.write_body(inner, scope, 8);
-    body << "    }\n}\n" << kWrappers;
+    body << "        for (int j = 0; j < " << u.V << "; ++j) {\n";
+    body << "            const bh_i64 i" << (P - 1) << " = cbase + j * " << kThreads << ";\n";
+    body << elem.str();
+    body << "        }\n    } else {\n";
+    body << "        for (int j = 0; j < " << u.V << "; ++j) {\n";
+    body << "            const bh_i64 i" << (P - 1) << " = cbase + j * " << kThreads << ";\n";
+    body << "            if (i" << (P - 1) << " >= " << n_inner << ") break;\n";
+    body << elem.str();
+    body << "        }\n    }\n}\n" << kWrappers;
     u.fields = pl.fields;
     u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
     u.elements = rows * u.cols;
@@ -1105,13 +1118,26 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
         body << "    " << ctypes[k] << "* part" << k << " = (" << ctypes[k] << "*)(p.scratch + p.work * " << 8 * k
              << ");\n";
     for (size_t k = 0; k < reds.size(); ++k) body << "    " << ctypes[k] << " " << accs[k] << " = " << idents[k] << ";\n";
+    // Full tiles run without bounds checks; the accumulation order (j = 0..7) is the same in both.
+    stringstream elem;
+    {
+        Emitter eb(sym, elem, opt);
+        eb.external_acc = em.external_acc;
+        Scope scope;
+        eb.write_body(L, scope, 12);
+    }
+    const string n0 = "p.n" + to_string(sym.loop_id.at(&L));
+    body << "    if ((tile + 1) * " << kReduceTile << " <= " << n0 << ") {\n";
     body << "#pragma unroll\n";
-    body << "    for (int j = 0; j < " << kReduceV << "; ++j) {\n";
-    body << "        const bh_i64 i0 = tile * " << kReduceTile << " + j * " << kThreads << " + threadIdx.x;\n";
-    body << "        if (i0 >= p.n" << sym.loop_id.at(&L) << ") break;\n";
-    Scope scope;
-    em.write_body(L, scope, 8);
-    body << "    }\n";
+    body << "        for (int j = 0; j < " << kReduceV << "; ++j) {\n";
+    body << "            const bh_i64 i0 = tile * " << kReduceTile << " + j * " << kThreads << " + threadIdx.x;\n";
+    body << elem.str();
+    body << "        }\n    } else {\n";
+    body << "        for (int j = 0; j < " << kReduceV << "; ++j) {\n";
+    body << "            const bh_i64 i0 = tile * " << kReduceTile << " + j * " << kThreads << " + threadIdx.x;\n";
+    body << "            if (i0 >= " << n0 << ") break;\n";
+    body << elem.str();
+    body << "        }\n    }\n";
     for (size_t k = 0; k < reds.size(); ++k) {
         body << "    " << accs[k] << " = bh_block_reduce" << k << "(" << accs[k] << ", (" << ctypes[k] << "*)sm_raw);\n";
         body << "    if (threadIdx.x == 0) part" << k << "[tile] = " << accs[k] << ";\n";

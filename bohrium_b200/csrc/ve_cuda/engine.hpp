@@ -41,7 +41,7 @@ struct UnitRecord {
 struct Stats {
     uint64_t flushes = 0, kernels = 0, launches = 0, grouped_launches = 0, graph_replays = 0;
     uint64_t fuse_cache_hits = 0, fuse_cache_misses = 0;
-    uint64_t plan_cache_hits = 0, plan_cache_misses = 0;
+    uint64_t plan_cache_hits = 0, plan_cache_misses = 0, replays = 0;
     uint64_t kernel_cache_hits = 0, kernel_cache_misses = 0, disk_cache_hits = 0;
     uint64_t bytes_h2d = 0, bytes_d2h = 0;
     uint64_t serial_units = 0;
@@ -164,6 +164,16 @@ private:
         size_t nbases = 0;
     };
     std::unordered_map<uint64_t, FlushPlan> plans;
+    // Replay of a fingerprinted BhIR (BhIR::_fingerprint): the plan, the bases in flush order,
+    // the bases freed without being computed, and the bases whose constructor flag the plan
+    // assumed (first used as an output) with that flag. A replay only has to re-check those flags.
+    struct Replay {
+        const FlushPlan *plan = nullptr;
+        std::vector<bh_base *> base_ids, dead;
+        std::vector<std::pair<bh_base *, bool>> first_outputs;
+    };
+    std::unordered_map<uint64_t, Replay> replays;
+    bool replay_valid(const Replay &r) const;
     FlushPlan build_plan(const std::vector<jitk::LoopB> &kernels, const std::vector<bh_base *> &base_ids);
     void run_plan(const FlushPlan &plan, const std::vector<bh_base *> &bases, const std::vector<bh_instruction *> &instrs);
     void pack_params(const PlanUnit &pu, const std::vector<bh_base *> &bases, const std::vector<bh_instruction *> &instrs,
@@ -184,7 +194,7 @@ private:
     void copyToDevice(bh_base *base);
     void setConstructorFlag(std::vector<bh_instruction *> &instr_list);
     uint64_t prepare(std::vector<bh_instruction> &list, std::vector<bh_instruction *> &out,
-                     std::vector<bh_base *> &base_ids, bool &sliding);
+                     std::vector<bh_base *> &base_ids, bool &sliding, Replay *replay = nullptr);
     std::vector<jitk::LoopB> kernels_for(std::vector<bh_instruction *> &instr_list, uint64_t key,
                                          const std::vector<bh_base *> &base_ids);
     void free_base(bh_base *base);

@@ -15,6 +15,11 @@ public:
     uint64_t _nrepeats;
     // Repeat while this single BH_BOOL element is true (nullptr: no condition).
     bh_base *_repeat_condition;
+    // Optional content fingerprint set by a caller that executes the same, unmodified BhIR more
+    // than once (0: unknown). An engine may use it to recognise a repeated flush without scanning
+    // the instruction list; the caller must reset it to 0 if it changes the BhIR. (Not part of the
+    // reference's BhIR; callers that never set it see no difference.)
+    uint64_t _fingerprint = 0;
 
     BhIR(std::vector<bh_instruction> instr_list, std::set<bh_base *> syncs, uint64_t nrepeats = 1,
          bh_base *repeat_condition = nullptr)
