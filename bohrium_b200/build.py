@@ -73,13 +73,10 @@ def _compile(src: str, verbose: bool) -> str:
     return obj
 
 
-def _link(target: str, objs: list[str], libs: list[str], verbose: bool, use_nvcc: bool = False) -> None:
+def _link(target: str, objs: list[str], libs: list[str], verbose: bool) -> None:
     if not _stale(target, objs):
         return
-    if use_nvcc:
-        cmd = [NVCC, "-shared", "-o", target] + objs + ARCH + ["-Xlinker", "-rpath,$ORIGIN", "-L" + LIB] + libs
-    else:
-        cmd = [CXX, "-shared", "-o", target] + objs + ["-Wl,-rpath,$ORIGIN", "-Wl,--no-undefined", "-L" + LIB] + libs
+    cmd = [CXX, "-shared", "-o", target] + objs + ["-Wl,-rpath,$ORIGIN", "-Wl,--no-undefined", "-L" + LIB] + libs
     if verbose:
         print(" ".join(cmd))
     _run(cmd)
@@ -100,8 +97,10 @@ def build(verbose: bool = False) -> dict:
     cuda_objs = [_compile(s, verbose) for s in sources("ve_cuda")]
     ve = os.path.join(LIB, "libbh_ve_cuda.so")
     cuda_lib = os.path.join(CUDA_HOME, "lib64")
+    # .cu objects are compiled without relocatable device code, so g++ links them (against
+    # cudart_static, which registers their fat binaries) with --no-undefined like the rest.
     _link(ve, cuda_objs, ["-lbh_core", "-L" + cuda_lib, "-lcudart_static", "-lnvrtc", "-ldl", "-lpthread", "-lrt"],
-          verbose, use_nvcc=any(o.endswith(".cu.o") for o in cuda_objs))
+          verbose)
 
     node_objs = [_compile(s, verbose) for s in sources("vem_node")]
     node = os.path.join(LIB, "libbh_vem_node.so")

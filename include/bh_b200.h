@@ -110,6 +110,18 @@ void bhb_set_last_error(const char *msg);
  * or NULL on error. `fuser_list` overrides the transformer list (NULL: the engine default). */
 const char *bh_ve_cuda_dry_run(bhb_ir *ir, int compile, const char *fuser_list);
 
+/* libbh_ve_cuda.so: allocation-free sum of `n` contiguous float64 values at device address `in`,
+ * written to the device address `out`, enqueued on `stream` (a cudaStream_t; NULL: the legacy
+ * default stream). No counterpart in the reference: it is the engine's ADD_REDUCE grid reduction
+ * with its tile partials in a fixed static device array (65,792 bytes per device) instead of
+ * allocated scratch, for callers that cannot let a library allocate device memory. It calls no
+ * cudaMalloc, cudaFree or other allocating routine. n is at most 16,777,216 (8,192 tiles of 2,048);
+ * larger n is rejected with an error. The first call on each device, made with that device
+ * current, does a one-time set-up (cudaGetSymbolAddress of the array); make it before any stream
+ * capture. All calls share the array: calls whose kernels overlap on the GPU race. Returns 0, or
+ * -1 with bhb_last_error() set. */
+int bh_ve_cuda_sum_f64_noalloc(const double *in, int64_t n, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
