@@ -221,8 +221,8 @@ def run_ours(args, world, rank, local):
     dev_ms_max = allreduce_max(world, dev_ms)
     bytes_step = BS_ITERS * bs_bytes(n)
     value = world * bytes_step * args.steps / (dev_ms_max / 1e3) / 1e9
-    got = [float(v) for v in (ex.peek(o.base)[0] for o in outs[:2])]
-    want = [W.black_scholes_numpy(*host_inputs, it) for it in range(2)] if rank == 0 else got
+    got = [float(v) for v in (ex.peek(o.base)[0] for o in outs[:3])]
+    want = [W.black_scholes_numpy(*host_inputs, it) for it in range(3)] if rank == 0 else got
     check_ok = all(abs(g - w) <= 1e-10 * abs(w) for g, w in zip(got, want))
     avg_kernel_ms = statistics.mean(kernel_ms) if kernel_ms else dev_ms / args.steps / BS_ITERS
     achieved = bs_bytes(n) / (avg_kernel_ms / 1e3) / 1e9
@@ -281,9 +281,8 @@ def run_ours(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
-def run_extra(bh, W, ex, rt, peak):
-    out = {}
-    # Config 1: the plain chain over three float64 arrays of 2^20 elements.
+def extra_plain_chain(bh, W, ex, rt, out):
+    """The plain chain over three float64 arrays of 2^20 elements."""
     n = 1 << 20
     A, B, C = W.plain_chain_inputs(n, 0)
     a, b, c = (bh.array(rt, x) for x in (A, B, C))
@@ -305,9 +304,11 @@ def run_extra(bh, W, ex, rt, peak):
                                    "note": "25 MB working set: L2-resident across repeated flushes"}
     del ir, r, a, b, c
 
-    # Config 3: 2-D heat stencil, float32 4096^2, 100 iterations as one flush repeated 50 times
-    # over a two-step (a->b, b->a) bytecode.
-    g = W.heat_grid(4096, 0)
+
+def extra_heat(bh, W, ex, rt, out, n=4096):
+    """2-D heat stencil, float32 n^2, 100 iterations as one flush repeated 50 times over a
+    two-step (a->b, b->a) bytecode."""
+    g = W.heat_grid(n, 0)
     ga, gb = bh.array(rt, g), bh.array(rt, g)
     d1 = W.heat_step(ga, gb)
     d2 = W.heat_step(gb, ga)
@@ -325,13 +326,15 @@ def run_extra(bh, W, ex, rt, peak):
     ir.execute()
     ms = float(ex.message("CUDA: timer stop"))
     wall = (time.perf_counter() - t0) * 1e3
-    per_iter = (4096 * 4096 * 4 + 4094 * 4094 * 4)
-    out["heat_f32_4096^2_x100"] = {"flush_ms_device": round(ms, 3), "flush_ms_wall": round(wall, 3),
+    per_iter = (n * n * 4 + (n - 2) * (n - 2) * 4)
+    out[f"heat_f32_{n}^2_x100"] = {"flush_ms_device": round(ms, 3), "flush_ms_wall": round(wall, 3),
                                    "GB/s": round(100 * per_iter / (ms / 1e3) / 1e9, 1),
                                    "iterations": 100}
     del ir, d1, d2, ga, gb
 
-    # Config 4: 4096 float32 systems of uneven length in one flush, plain vs grouped launches.
+
+def extra_batching(bh, W, ex, rt, out):
+    """4096 float32 systems of uneven length in one flush, plain vs grouped launches."""
     lengths = W.batching_lengths(4096, 256, 65536, 0)
     xs = []
     for i, L in enumerate(lengths):
@@ -379,6 +382,19 @@ def run_extra(bh, W, ex, rt, peak):
     res["systems"] = 4096
     res["elements"] = total
     out["batching_4096_systems_f32"] = res
+
+
+EXTRAS = {"plain_chain": extra_plain_chain, "heat": extra_heat, "batching": extra_batching}
+
+
+def run_extra(bh, W, ex, rt, peak, only=None, heat_n=4096):
+    out = {}
+    for name, fn in EXTRAS.items():
+        if only is None or name == only:
+            if name == "heat":
+                fn(bh, W, ex, rt, out, n=heat_n)
+            else:
+                fn(bh, W, ex, rt, out)
     return out
 
 
@@ -434,9 +450,19 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-options", type=int, default=BS_OPTIONS)
     ap.add_argument("--bs-options", type=int, default=BS_OPTIONS, help="options of the headline workload")
+    ap.add_argument("--only", choices=sorted(EXTRAS), default=None,
+                    help="run one of the other workloads alone (no headline line; for profiling)")
+    ap.add_argument("--heat-n", type=int, default=4096, help="grid side of the heat workload")
     args = ap.parse_args()
     world, rank, local = dist_init()
-    if args.impl == "reference":
+    if args.only:
+        import bohrium_b200 as bh
+        from bohrium_b200 import workloads as W
+        ex = bh.NativeExecutor()
+        res = run_extra(bh, W, ex, bh.Runtime(ex), peaks()[0], only=args.only, heat_n=args.heat_n)
+        if rank == 0:
+            print(json.dumps({"only": args.only, **res}), flush=True)
+    elif args.impl == "reference":
         run_reference(args, world, rank)
     else:
         run_ours(args, world, rank, local)

@@ -900,7 +900,7 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
             staging_used = 0;
             ++_stats.plan_cache_hits;
             ++_stats.replays;
-            run_plan(*r.plan, r.base_ids, {});
+            run_plan(*r.plan, r.base_ids, r.instrs);
             _stats.time_launch += seconds_since(t1);
             copyToHost(bhir->_syncs, false);
             check_error_record();
@@ -937,6 +937,9 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
         if (pit != plans.end()) {
             replay.plan = &pit->second;
             replay.base_ids = base_ids;
+            replay.instr_copy.reserve(instr_list.size());
+            for (const bh_instruction *i : instr_list) replay.instr_copy.push_back(*i);
+            for (bh_instruction &i : replay.instr_copy) replay.instrs.push_back(&i);
             replays[bhir->_fingerprint] = std::move(replay);
         }
     }

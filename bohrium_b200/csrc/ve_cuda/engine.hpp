@@ -171,6 +171,10 @@ private:
         const FlushPlan *plan = nullptr;
         std::vector<bh_base *> base_ids, dead;
         std::vector<std::pair<bh_base *, bool>> first_outputs;
+        // The flush's own instructions (by origin id): plans are shared between flushes of the
+        // same structure, so constants and Random123 start/key must come from this flush.
+        std::vector<bh_instruction> instr_copy;
+        std::vector<bh_instruction *> instrs;
     };
     std::unordered_map<uint64_t, Replay> replays;
     bool replay_valid(const Replay &r) const;

@@ -189,8 +189,8 @@ def random_dag(rt: Runtime, seed: int, nops: int, nelem: int, dtype=np.float32, 
             elif form == 2:
                 z = z[:, ::-1] if cols > 1 else z
             elif form == 3:
-                z = z[rng.integers(rows):rng.integers(rows) + 1, :] if rows > 1 else z
-                z = z if z.shape[0] == 1 else z[:1, :]
+                r0, _ = rng.integers(rows), rng.integers(rows)
+                z = z[r0:r0 + 1, :] if rows > 1 else z
             from .array import binary
             y = binary(name, x, z)
         nodes.append(y)

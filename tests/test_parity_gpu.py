@@ -221,3 +221,27 @@ def test_grouped_launches_are_bit_identical(gpu_executor):
         gpu_executor.message("CUDA: batch off")
     for p, q in zip(results["off"], results["grouped"]):
         assert np.array_equal(p, q)
+
+
+def test_replayed_flushes_keep_their_own_constants(gpu_executor, oracle_rt):
+    """Compiled flushes of the same structure but different constants (and Random123 keys) share
+    one plan; replaying each one must still use its own constants."""
+    rt = bh.Runtime(gpu_executor)
+    host = np.random.default_rng(3).random(10000)
+    x = bh.array(rt, host)
+    rt.flush()
+    irs, outs = [], []
+    for k in range(3):
+        r = bh.random123(rt, (10000,), 5, 100 + k)
+        y = (x * float(k + 2) + float(k)).sum()
+        outs.append((y, r))
+        irs.append(gpu_executor.compile(rt.take()))
+    for _ in range(3):  # first run builds the plan, later runs replay it
+        for ir in irs:
+            ir.execute()
+    for k, (y, r) in enumerate(outs):
+        want_r = bh.random123(oracle_rt, (10000,), 5, 100 + k).numpy()
+        assert np.array_equal(gpu_executor.peek(r.base), want_r), k
+        want = float(np.sum(host * float(k + 2) + float(k)))
+        got = float(gpu_executor.peek(y.base)[0])
+        assert abs(got - want) <= 1e-12 * abs(want), (k, got, want)
