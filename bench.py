@@ -348,7 +348,7 @@ def extra_batching(bh, W, ex, rt, out):
     ir = ex.compile(rt.take())
     total = int(lengths.sum())
     res = {}
-    for mode in ["off", "grouped"]:
+    for mode in ["off", "grouped", "graph"]:
         ex.message(f"CUDA: batch {mode}")
         for _ in range(3):
             ir.execute()
@@ -370,15 +370,17 @@ def extra_batching(bh, W, ex, rt, out):
         res[mode]["host_ms_per_flush"] = {k: round((h1.get(k, 0) - h0.get(k, 0)) * 1e3 / reps, 3)
                                           for k in ("time_exec_host", "time_prepare", "time_launch")}
     ex.message("CUDA: batch off")
-    # bit-identical results between the two forms
-    ex.message("CUDA: batch grouped")
-    ir.execute()
-    grouped = [ex.peek(o.base) for o in outs[1::3][:64]]
+    # bit-identical results between the forms (every output of every system)
+    got = {}
+    for mode in ["graph", "grouped", "off"]:
+        ex.message(f"CUDA: batch {mode}")
+        ir.execute()
+        ir.execute()
+        got[mode] = [ex.peek(o.base).tobytes() for o in outs]
     ex.message("CUDA: batch off")
-    ir.execute()
-    plain = [ex.peek(o.base) for o in outs[1::3][:64]]
-    res["bit_identical"] = all(np.array_equal(p, q) for p, q in zip(plain, grouped))
+    res["bit_identical"] = got["graph"] == got["off"] and got["grouped"] == got["off"]
     res["speedup_wall"] = round(res["off"]["flush_ms_wall"] / res["grouped"]["flush_ms_wall"], 2)
+    res["speedup_wall_graph"] = round(res["off"]["flush_ms_wall"] / res["graph"]["flush_ms_wall"], 2)
     res["systems"] = 4096
     res["elements"] = total
     out["batching_4096_systems_f32"] = res

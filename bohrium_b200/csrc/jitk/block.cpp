@@ -499,6 +499,20 @@ Block reshape_and_merge(const LoopB &l1, const LoopB &l2) {
     throw runtime_error("reshape_and_merge: the blocks are not mergeable!");
 }
 
+namespace {
+thread_local bool t_avoid_mixed_sweeps = false;
+
+void sweep_ranks(const LoopB &l, set<int> &out) {
+    if (!l._sweeps.empty()) out.insert(l.rank);
+    for (const Block &b : l._block_list)
+        if (!b.isInstr()) sweep_ranks(b.getLoop(), out);
+}
+} // namespace
+
+MixedSweepRule::MixedSweepRule(bool on) : previous(t_avoid_mixed_sweeps) { t_avoid_mixed_sweeps = on; }
+bool MixedSweepRule::active() { return t_avoid_mixed_sweeps; }
+MixedSweepRule::~MixedSweepRule() { t_avoid_mixed_sweeps = previous; }
+
 bool mergeable(const Block &b1, const Block &b2, bool avoid_rank0_sweep) {
     if (b1.isInstr() || b2.isInstr()) return false;
     const LoopB &l1 = b1.getLoop();
@@ -506,6 +520,12 @@ bool mergeable(const Block &b1, const Block &b2, bool avoid_rank0_sweep) {
     if (l2.isSystemOnly()) return true;
     if (avoid_rank0_sweep && l1.rank == 0 && l2.rank == 0) {
         if (l1._sweeps.empty() != l2._sweeps.empty()) return false;
+    }
+    if (t_avoid_mixed_sweeps) {
+        set<int> ranks;
+        sweep_ranks(l1, ranks);
+        sweep_ranks(l2, ranks);
+        if (ranks.size() > 1) return false;
     }
     if (sweeps_accessed_by_block(l1._sweeps, l2)) return false;
     if (l1.size == l2.size || (l2._reshapable && l1.size != 0 && l2.size % l1.size == 0) ||

@@ -110,6 +110,15 @@ Block create_nested_block(const std::vector<InstrPtr> &instr_list, int rank, int
 std::pair<uint64_t, uint64_t> parallel_ranks(const LoopB &block, unsigned int max_depth = 3);
 std::vector<const LoopB *> get_first_loop_blocks(const LoopB &block);
 bool mergeable(const Block &b1, const Block &b2, bool avoid_rank0_sweep);
+// While an instance lives (on this thread), mergeable() also refuses merges whose result sweeps
+// axes at more than one loop rank (e.g. a column sum fused with a row sum): such a nest can only
+// run on one thread, so the GPU keeps the two reductions in separate kernels.
+struct MixedSweepRule {
+    explicit MixedSweepRule(bool on);
+    ~MixedSweepRule();
+    static bool active();
+    bool previous;
+};
 Block reshape_and_merge(const LoopB &l1, const LoopB &l2);
 
 // Reshape the dimensions from `rank` inwards of a reshapable instruction to `size_of_rank_dim`

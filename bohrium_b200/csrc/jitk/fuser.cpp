@@ -27,6 +27,7 @@ FusionConfig::FusionConfig(const ConfigParser &config, bool avoid_rank0)
       fuser_list(config.defaultGetList("fuser_list", {"greedy", "collapse_redundant_axes"})),
       greedy_threshold(config.defaultGet<uint64_t>("greedy_threshold", 10000)),
       avoid_rank0_sweep(config.defaultGet<bool>("avoid_rank0_sweep", avoid_rank0)),
+      avoid_mixed_sweeps(config.defaultGet<bool>("avoid_mixed_sweeps", false)),
       monolithic(config.defaultGet<bool>("monolithic", false)) {}
 
 // ------------------------------------------------------------------------------- simplification
@@ -79,9 +80,13 @@ bool fully_dp_compatible(const InstrPtr &a, const InstrPtr &b) {
 bool fully_fusible(const vector<InstrPtr> &instr_list, const InstrPtr &instr) {
     if (instr_list.empty() || bh_opcode_is_system(instr->opcode)) return true;
     const BhIntVec dshape = instr->shape();
+    const bool sweep = bh_opcode_is_sweep(instr->opcode);
     for (const InstrPtr &i : instr_list) {
         if (bh_opcode_is_system(i->opcode)) continue;
         if (i->shape() != dshape || !fully_dp_compatible(i, instr)) return false;
+        // With the mixed-sweep rule, a group sweeps at most one axis (see MixedSweepRule).
+        if (sweep && MixedSweepRule::active() && bh_opcode_is_sweep(i->opcode) && i->sweep_axis() != instr->sweep_axis())
+            return false;
     }
     return true;
 }
@@ -755,6 +760,7 @@ vector<LoopB> add_identity_block(vector<Block> &block_list, int64_t &origin_coun
 
 vector<Block> fuse_block_list(const vector<bh_instruction *> &instr_list, const FusionConfig &config,
                               const MergeChooser *chooser) {
+    const MixedSweepRule rule(config.avoid_mixed_sweeps);
     vector<Block> block_list;
     if (config.pre_fuser == "none" || config.pre_fuser == "singleton") {
         block_list = fuser_singleton(instr_list);

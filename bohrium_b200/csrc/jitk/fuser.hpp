@@ -23,6 +23,7 @@ struct FusionConfig {
     std::vector<std::string> fuser_list = {"greedy", "collapse_redundant_axes"};
     uint64_t greedy_threshold = 10000;
     bool avoid_rank0_sweep = false;
+    bool avoid_mixed_sweeps = false; // see MixedSweepRule (block.hpp)
     bool monolithic = false;
     FusionConfig() = default;
     FusionConfig(const ConfigParser &config, bool avoid_rank0_sweep);

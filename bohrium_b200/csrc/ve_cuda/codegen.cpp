@@ -27,6 +27,7 @@ const char *sched_name(Sched s) {
         case Sched::FLAT: return "flat";
         case Sched::GRID_REDUCE: return "grid_reduce";
         case Sched::SPLIT_REDUCE: return "split_reduce";
+        case Sched::LANE_REDUCE: return "lane_reduce";
         case Sched::OUTER_REDUCE: return "outer_reduce";
         case Sched::SCAN1D: return "scan1d";
         case Sched::SERIAL: return "serial";
@@ -42,6 +43,10 @@ int64_t LaunchUnit::work_items() const {
         }
         case Sched::GRID_REDUCE: return (cols + kReduceTile - 1) / kReduceTile;
         case Sched::SPLIT_REDUCE: return (rows * cols + kThreads - 1) / kThreads * chunks;
+        case Sched::LANE_REDUCE: {
+            const int64_t per = kThreads / chunks;
+            return (rows * cols + per - 1) / per;
+        }
         case Sched::OUTER_REDUCE: return (rows * cols + kThreads - 1) / kThreads;
         case Sched::SCAN1D: return (cols + kScanChunk - 1) / kScanChunk;
         case Sched::SERIAL: return 1;
@@ -119,6 +124,21 @@ template <typename T> __device__ __forceinline__ T bh_shfl_xor(T v, int m) {
         x = __shfl_xor_sync(0xffffffffu, x, m);
         T r; memcpy(&r, &x, sizeof(T)); return r;
     }
+}
+
+// Load through L2 only (ld.global.cg): for values that other CTAs wrote during this launch.
+template <typename T> __device__ __forceinline__ T bh_ldcg(const T *ptr) {
+    T r;
+    if (sizeof(T) == 8) {
+        const long long x = __ldcg((const long long *)ptr); memcpy(&r, &x, 8);
+    } else if (sizeof(T) == 4) {
+        const int x = __ldcg((const int *)ptr); memcpy(&r, &x, 4);
+    } else if (sizeof(T) == 2) {
+        const short x = __ldcg((const short *)ptr); memcpy(&r, &x, 2);
+    } else {
+        const signed char x = __ldcg((const signed char *)ptr); memcpy(&r, &x, 1);
+    }
+    return r;
 }
 
 // Integer power by repeated squaring: exact wherever the result fits the type (CUDA's double pow
@@ -330,8 +350,13 @@ struct Symbols {
     map<const bh_base *, int> base_id; // every base (params and temporaries)
     set<const bh_base *> temps;
     set<const bh_base *> always_array;
-    map<bh_view, int> view_id; // exact view -> offset/stride slot
+    map<bh_view, int> view_id; // exact view -> offset slot
     vector<bh_view> views;
+    // Views with equal strides share one set of stride parameters (a stride group), and their
+    // index expressions share the strided part, so the compiler computes it once.
+    map<vector<int64_t>, int> stride_group_id;
+    vector<vector<int64_t>> stride_groups;
+    vector<int> view_group; // per view
     map<const LoopB *, int> loop_id;
     vector<const LoopB *> loops;
     map<const bh_instruction *, int> const_id;
@@ -395,6 +420,13 @@ Symbols build_symbols(const vector<const Block *> &items, const set<const bh_ins
             if (!s.view_id.count(v)) {
                 s.view_id[v] = static_cast<int>(s.views.size());
                 s.views.push_back(v);
+                vector<int64_t> key(v.stride.begin(), v.stride.begin() + v.ndim);
+                auto g = s.stride_group_id.find(key);
+                if (g == s.stride_group_id.end()) {
+                    g = s.stride_group_id.emplace(key, static_cast<int>(s.stride_groups.size())).first;
+                    s.stride_groups.push_back(key);
+                }
+                s.view_group.push_back(g->second);
             }
         }
         if (instr->has_constant() && !bh_opcode_is_sweep(instr->opcode) && !folded.count(instr.get())) {
@@ -439,23 +471,26 @@ public:
         return ret;
     }
 
+    // Element index of view `v`: (sum of loop index x group stride) + view offset. The strided
+    // part is written identically for all views of a stride group.
     string index_expr(const bh_view &v, int hidden_axis = BH_MAXDIM, pair<int, int> axis_offset = {-1, 0}) {
         const int vid = sym.view_id.at(v);
+        const int gid = sym.view_group.at(static_cast<size_t>(vid));
+        if (v.is_scalar() || v.ndim == 0) return "(p.v" + to_string(vid) + "_o)";
         stringstream ss;
-        ss << "(p.v" << vid << "_o";
-        if (!v.is_scalar()) {
-            for (int64_t i = 0; i < v.ndim; ++i) {
-                int t = static_cast<int>(i);
-                if (t >= hidden_axis) ++t;
-                if (axis_offset.first == t) {
-                    ss << " + (i" << t << " == 0 ? 0 : i" << t << " + (" << axis_offset.second << "))";
-                } else {
-                    ss << " + i" << t;
-                }
-                ss << " * p.v" << vid << "_s" << i;
+        ss << "((";
+        for (int64_t i = 0; i < v.ndim; ++i) {
+            int t = static_cast<int>(i);
+            if (t >= hidden_axis) ++t;
+            if (i > 0) ss << " + ";
+            if (axis_offset.first == t) {
+                ss << "(i" << t << " == 0 ? 0 : i" << t << " + (" << axis_offset.second << "))";
+            } else {
+                ss << "i" << t;
             }
+            ss << " * p.g" << gid << "_s" << i;
         }
-        ss << ")";
+        ss << ") + p.v" << vid << "_o)";
         return ss.str();
     }
 
@@ -608,13 +643,15 @@ void add_common_fields(Symbols &sym, ParamLayout &pl, const CodegenOptions &opt)
         pl.add(f, cuda_type(sym.params[i]->dtype()) + "* __restrict__", "a" + to_string(i));
     }
     for (size_t i = 0; i < sym.views.size(); ++i) {
-        const bh_view &v = sym.views[i];
         ParamField f{ParamField::I64};
-        f.i64 = v.start;
+        f.i64 = sym.views[i].start;
         pl.add(f, "bh_i64", "v" + to_string(i) + "_o");
-        for (int64_t d = 0; d < v.ndim; ++d) {
-            f.i64 = v.stride[d];
-            pl.add(f, "bh_i64", "v" + to_string(i) + "_s" + to_string(d));
+    }
+    for (size_t g = 0; g < sym.stride_groups.size(); ++g) {
+        for (size_t d = 0; d < sym.stride_groups[g].size(); ++d) {
+            ParamField f{ParamField::I64};
+            f.i64 = sym.stride_groups[g][d];
+            pl.add(f, "bh_i64", "g" + to_string(g) + "_s" + to_string(d));
         }
     }
     for (size_t i = 0; i < sym.loops.size(); ++i) {
@@ -876,6 +913,9 @@ LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) 
 // depends on the array shapes only.
 constexpr int64_t kSplitTargetThreads = 600000;
 constexpr int64_t kSplitMinChunk = 16;
+// Points from which LANE_REDUCE (C lanes of one CTA per point) fills the GPU well enough to be
+// preferred over SPLIT_REDUCE when the swept axis is contiguous.
+constexpr int64_t kLaneMinPoints = 148;
 
 // The swept sub-loop of `inner` when `inner` is [identity instructions] [swept innermost sub-loop]
 // [instructions], and the sub-loop's sweeps are reductions; nullptr otherwise.
@@ -914,6 +954,176 @@ int64_t split_chunks(int64_t points, int64_t len) {
     return max<int64_t>(1, min(want, most));
 }
 
+int ilog2(int64_t x) {
+    int r = 0;
+    while ((int64_t(1) << (r + 1)) <= x) ++r;
+    return r;
+}
+
+// Lanes per point of LANE_REDUCE: a power of two up to a CTA (256) chosen from the shapes alone.
+int64_t lane_count(int64_t points, int64_t len) {
+    int64_t c = 1;
+    while (c < kThreads && points * c < kSplitTargetThreads && c * 4 <= len) c *= 2;
+    return c;
+}
+
+// True when every array the swept sub-loop (at `rank`) reads walks that axis with unit stride (or
+// broadcasts along it), and at least one does: C consecutive lanes then read adjacent elements.
+bool swept_axis_contiguous(const LoopB &sub, int rank) {
+    bool unit = false;
+    for (const InstrPtr &ip : jitk::all_instr(sub)) {
+        for (size_t o = 1; o < ip->operand.size(); ++o) {
+            const bh_view &v = ip->operand[o];
+            if (v.isConstant() || v.ndim <= rank) continue;
+            const int64_t st = v.stride[rank];
+            if (st == 1) {
+                unit = true;
+            } else if (st != 0 && v.shape[rank] > 1) {
+                return false;
+            }
+        }
+    }
+    return unit;
+}
+
+// LANE_REDUCE: the SPLIT_REDUCE structure ([identities] [swept innermost sub-loop] [instructions]
+// inside P threaded ranks) when the swept axis is contiguous in memory. C lanes of one CTA share a
+// point: lane c folds elements c, c+C, c+2C, ... in order (adjacent lanes read adjacent elements),
+// then the C lane partials are combined by a fixed shuffle tree (xor C/2 .. 1 within a warp; for
+// C > 32 the warp sums are folded in warp order), and lane 0 runs the instructions that follow.
+// No scratch memory and no counters: one pass.
+LaunchUnit lower_lane_reduce(const LoopB &loop, unsigned P, const CodegenOptions &opt) {
+    LaunchUnit u;
+    u.sched = Sched::LANE_REDUCE;
+    const Block holder(loop);
+    const LoopB &L = holder.getLoop();
+    const vector<const LoopB *> chain = jitk::get_first_loop_blocks(L);
+    const LoopB &inner = *chain[P - 1];
+    const LoopB &sub = *split_candidate(inner);
+    set<const bh_instruction *> folded;
+    for (const Block &b : inner._block_list) {
+        if (!b.isInstr()) break;
+        folded.insert(b.getInstr().get());
+    }
+    Symbols sym = build_symbols({&holder}, folded);
+    vector<InstrPtr> reds(sub._sweeps.begin(), sub._sweeps.end());
+    sort(reds.begin(), reds.end(), [](const InstrPtr &a, const InstrPtr &b) { return a->origin_id < b->origin_id; });
+    u.nred = static_cast<int>(reds.size());
+    int64_t rows = 1;
+    for (unsigned r = 0; r + 1 < P; ++r) rows *= chain[r]->size;
+    u.rows = rows;
+    u.cols = inner.size;
+    const int64_t points = rows * inner.size;
+    const int64_t C = lane_count(points, sub.size);
+    u.chunks = C;
+    for (const InstrPtr &r : reds)
+        u.red_orders.emplace_back(r->origin_id, "lanes:" + to_string(C) + ":" + to_string(sub.size));
+    ParamLayout pl;
+    add_common_fields(sym, pl, opt);
+    pl.add(work_field(points), "bh_i64", "points");
+    pl.add(work_field(u.work_items()), "bh_i64", "work");
+
+    stringstream body;
+    Emitter em(sym, body, opt);
+    vector<string> ctypes, idents;
+    for (size_t k = 0; k < reds.size(); ++k) {
+        const bh_type t = reds[k]->operand[0].base->dtype();
+        ctypes.push_back(cuda_type(t));
+        idents.push_back(constant_literal(jitk::sweep_identity(reds[k]->opcode, t)));
+        em.external_acc[ViewKey(reds[k]->operand[0])] = "pacc" + to_string(k);
+    }
+    const int sub_lid = sym.loop_id.at(&sub);
+    const int64_t per_cta = kThreads / C;
+    body << "__device__ void bh_work(const P &p, bh_i64 w) {\n";
+    body << pointer_locals(sym);
+    if (C > 32) {
+        for (size_t k = 0; k < reds.size(); ++k)
+            body << "    __shared__ " << ctypes[k] << " wsum" << k << "[" << kThreads / 32 << "];\n";
+    }
+    body << "    const int lane = threadIdx.x & " << (C - 1) << ";\n";
+    body << "    const bh_i64 pt = w * " << per_cta << " + (threadIdx.x >> " << ilog2(C) << ");\n";
+    for (size_t k = 0; k < reds.size(); ++k) body << "    " << ctypes[k] << " pacc" << k << " = " << idents[k] << ";\n";
+    auto decompose = [&](int ind) {
+        const string sp(static_cast<size_t>(ind), ' ');
+        body << sp << "bh_i64 rem = pt;\n";
+        for (int r = static_cast<int>(P) - 1; r >= 0; --r) {
+            const int lid = sym.loop_id.at(chain[r]);
+            if (r == 0) {
+                body << sp << "const bh_i64 i0 = rem;\n";
+            } else {
+                body << sp << "const bh_i64 i" << r << " = rem % p.n" << lid << "; rem /= p.n" << lid << ";\n";
+            }
+        }
+        body << sp << "(void)rem;\n";
+    };
+    body << "    if (pt < p.points) {\n";
+    decompose(8);
+    {
+        Scope scope;
+        declare_chain_temps(em, sym, scope, chain, P, body, 8);
+        body << "        for (bh_i64 i" << P << " = lane; i" << P << " < p.n" << sub_lid << "; i" << P << " += " << C
+             << ") {\n";
+        Scope s1;
+        s1.parent = &scope;
+        em.write_body(sub, s1, 12);
+        body << "        }\n";
+    }
+    body << "    }\n";
+    // Combine the C lanes of each point (every lane of the warp takes part; lanes of points past
+    // the end hold the identity).
+    const int64_t in_warp = C < 32 ? C : 32;
+    for (size_t k = 0; k < reds.size(); ++k) {
+        body << "#pragma unroll\n";
+        body << "    for (int m = " << in_warp / 2 << "; m >= 1; m >>= 1) { const " << ctypes[k]
+             << " o = bh_shfl_xor(pacc" << k << ", m); pacc" << k << " = "
+             << reduce_expr(reds[k]->opcode, "pacc" + to_string(k), "o") << "; }\n";
+    }
+    if (C > 32) {
+        const int64_t nw = C / 32;
+        for (size_t k = 0; k < reds.size(); ++k) body << "    if ((threadIdx.x & 31) == 0) wsum" << k << "[threadIdx.x >> 5] = pacc" << k << ";\n";
+        body << "    __syncthreads();\n";
+        body << "    if (lane == 0) {\n";
+        body << "        const int w0 = threadIdx.x >> 5;\n";
+        for (size_t k = 0; k < reds.size(); ++k) {
+            body << "        pacc" << k << " = wsum" << k << "[w0];\n";
+            body << "        for (int j = 1; j < " << nw << "; ++j) pacc" << k << " = "
+                 << reduce_expr(reds[k]->opcode, "pacc" + to_string(k), "wsum" + to_string(k) + "[w0 + j]") << ";\n";
+        }
+        body << "    }\n";
+        body << "    __syncthreads();  // wsum is rewritten by the next work item of this CTA\n";
+    }
+    body << "    if (lane != 0 || pt >= p.points) return;\n";
+    {
+        decompose(4);
+        Scope scope;
+        declare_chain_temps(em, sym, scope, chain, P - 1, body, 4);
+        for (const bh_base *b : em.sorted_temps(inner)) {
+            if (sym.temps.count(b) && !scope.is_tmp(b)) {
+                scope.tmps.insert(b);
+                body << "    " << cuda_type(b->dtype()) << " t" << sym.base_index(b) << ";\n";
+            }
+        }
+        bool after = false;
+        for (const Block &b : inner._block_list) {
+            if (!b.isInstr()) {
+                after = true;
+                continue;
+            }
+            if (after) em.write_instr(*b.getInstr(), scope, 4);
+        }
+        for (size_t k = 0; k < reds.size(); ++k) {
+            if (sym.temps.count(reds[k]->operand[0].base)) continue;
+            body << "    " << em.array_ref(reds[k]->operand[0], reds[k]->sweep_axis()) << " = pacc" << k << ";\n";
+        }
+    }
+    body << "}\n" << kWrappers;
+    u.fields = pl.fields;
+    u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
+    u.elements = points * sub.size;
+    finish_source(u, pl.decl.str(), body.str(), opt);
+    return u;
+}
+
 LaunchUnit lower_split_reduce(const LoopB &loop, unsigned P, const CodegenOptions &opt) {
     LaunchUnit u;
     u.sched = Sched::SPLIT_REDUCE;
@@ -938,6 +1148,9 @@ LaunchUnit lower_split_reduce(const LoopB &loop, unsigned P, const CodegenOption
     const int64_t points = rows * inner.size;
     u.chunks = split_chunks(points, sub.size);
     const int64_t chunk_len = (sub.size + u.chunks - 1) / u.chunks;
+    for (const InstrPtr &r : reds)
+        u.red_orders.emplace_back(r->origin_id, "split:" + to_string(u.chunks) + ":" + to_string(chunk_len) + ":" +
+                                                    to_string(sub.size));
     ParamLayout pl;
     add_common_fields(sym, pl, opt);
     pl.add(work_field(points), "bh_i64", "points");
@@ -1012,12 +1225,26 @@ LaunchUnit lower_split_reduce(const LoopB &loop, unsigned P, const CodegenOption
         decompose(4);
         Scope scope;
         declare_chain_temps(em, sym, scope, chain, P - 1, body, 4);
+        // The chunk partials were written by other CTAs (made visible by the fence and the
+        // counter): read them through L2 (ld.global.cg), eight loads in flight, folded in chunk
+        // order.
         for (size_t k = 0; k < reds.size(); ++k) {
-            body << "    " << ctypes[k] << " pacc" << k << " = " << idents[k] << ";\n";
-            body << "    for (bh_i64 c = 0; c < p.chunks; ++c) {\n";
-            body << "        const " << ctypes[k] << " x = ((volatile " << ctypes[k] << "*)part" << k
-                 << ")[c * p.points + pt];\n";
-            body << "        pacc" << k << " = " << reduce_expr(reds[k]->opcode, "pacc" + to_string(k), "x") << ";\n";
+            const string acc = "pacc" + to_string(k), T = ctypes[k];
+            body << "    " << T << " " << acc << " = " << idents[k] << ";\n";
+            body << "    {\n";
+            body << "        bh_i64 c = 0;\n";
+            body << "        for (; c + 8 <= p.chunks; c += 8) {\n";
+            body << "            " << T << " x[8];\n";
+            body << "#pragma unroll\n";
+            body << "            for (int j = 0; j < 8; ++j) x[j] = bh_ldcg(part" << k << " + (c + j) * p.points + pt);\n";
+            body << "#pragma unroll\n";
+            body << "            for (int j = 0; j < 8; ++j) " << acc << " = " << reduce_expr(reds[k]->opcode, acc, "x[j]")
+                 << ";\n";
+            body << "        }\n";
+            body << "        for (; c < p.chunks; ++c) {\n";
+            body << "            const " << T << " x = bh_ldcg(part" << k << " + c * p.points + pt);\n";
+            body << "            " << acc << " = " << reduce_expr(reds[k]->opcode, acc, "x") << ";\n";
+            body << "        }\n";
             body << "    }\n";
         }
         // Instructions after the swept sub-loop, then the reduction outputs.
@@ -1109,6 +1336,7 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
         em.external_acc[ViewKey(r->operand[0])] = accs[k];
     }
     u.scratch_bytes_per_tile = 8 * static_cast<int64_t>(reds.size());
+    for (const InstrPtr &r : reds) u.red_orders.emplace_back(r->origin_id, "tree:" + to_string(L.size));
     body << helpers.str();
     body << "__device__ void bh_work(const P &p, bh_i64 tile) {\n";
     body << pointer_locals(sym);
@@ -1311,7 +1539,10 @@ vector<LaunchUnit> lower_kernel(const LoopB &kernel, const CodegenOptions &opt) 
             const LoopB *sub = split_candidate(*chain[P - 1]);
             int64_t points = 1;
             for (unsigned r = 0; r < P; ++r) points *= chain[r]->size;
-            if (sub != nullptr && split_chunks(points, sub->size) > 1) {
+            if (sub != nullptr && points >= kLaneMinPoints && lane_count(points, sub->size) > 1 &&
+                swept_axis_contiguous(*sub, static_cast<int>(P))) {
+                units.push_back(lower_lane_reduce(L, P, opt));
+            } else if (sub != nullptr && split_chunks(points, sub->size) > 1) {
                 units.push_back(lower_split_reduce(L, P, opt));
             } else {
                 units.push_back(lower_flat(L, P, opt));

@@ -18,6 +18,10 @@
 //                 swept axis is cut into chunks so that ~600K threads work at once; each thread folds
 //                 its chunk in order, and the last CTA of each 256-point block folds the chunk
 //                 partials in chunk order (deterministic) and runs the instructions that follow.
+//   LANE_REDUCE   the SPLIT_REDUCE structure when the swept axis is contiguous and there are
+//                 enough points: C (power of two <= 256, from the shapes) lanes of one CTA share a
+//                 point, lane c folds elements c, c+C, ... (coalesced), and a fixed shuffle tree
+//                 combines the lanes; one pass, no scratch.
 //   OUTER_REDUCE  a nest that reduces its outermost axis into an array: threads own the output
 //                 elements (the inner parallel ranks) and loop over the reduced axis.
 //   SCAN1D        a 1-D nest whose outermost axis is an accumulate (cumulative sum/product):
@@ -38,7 +42,7 @@
 namespace bohrium {
 namespace cuda {
 
-enum class Sched { FLAT, GRID_REDUCE, SPLIT_REDUCE, OUTER_REDUCE, SCAN1D, SERIAL };
+enum class Sched { FLAT, GRID_REDUCE, SPLIT_REDUCE, LANE_REDUCE, OUTER_REDUCE, SCAN1D, SERIAL };
 const char *sched_name(Sched s);
 
 constexpr int kThreads = 256;      // threads per CTA for every schedule
@@ -64,7 +68,7 @@ struct LaunchUnit {
     int64_t rows = 1, cols = 1; // FLAT / OUTER_REDUCE index space; GRID_REDUCE/SCAN1D: cols = length
     int nred = 0;               // GRID_REDUCE / SPLIT_REDUCE: number of reductions
     int64_t scratch_bytes_per_tile = 0; // GRID_REDUCE: bytes of partials per tile (all reductions)
-    int64_t chunks = 1;         // SPLIT_REDUCE: chunks of the swept axis
+    int64_t chunks = 1;         // SPLIT_REDUCE: chunks of the swept axis; LANE_REDUCE: lanes per point
     int64_t work_items() const;
     int64_t scratch_bytes() const;   // partials in the scratch arena
     int64_t counters_needed() const; // completion counters
@@ -72,6 +76,11 @@ struct LaunchUnit {
     // Bytes of arrays read/written by this unit (algorithmic, temporaries excluded).
     int64_t algorithmic_bytes = 0;
     int64_t elements = 0;
+
+    // Summation order of the sweeps this unit reduces across threads, by origin id: "tree:<n>"
+    // (GRID_REDUCE) or "split:<chunks>:<chunk length>:<n>" (SPLIT_REDUCE). Every other sweep is
+    // folded by one thread in index order ("seq"), whatever the schedule.
+    std::vector<std::pair<int64_t, std::string>> red_orders;
 };
 
 struct CodegenOptions {

@@ -87,7 +87,9 @@ extern "C" const char *bh_ve_cuda_dry_run(bhb_ir *handle, int compile, const cha
                 }
             }
         }
+        // The engine's defaults (bohrium_b200/config.ini).
         cfg.avoid_rank0_sweep = false;
+        cfg.avoid_mixed_sweeps = true;
         const vector<jitk::LoopB> kernels = jitk::get_kernel_list(instr_list, cfg);
         cuda::CodegenOptions opt;
         stringstream ss;

@@ -1,5 +1,7 @@
 // B200 vector engine: memory, compilation, launching and the flush loop.
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -11,6 +13,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <nvrtc.h>
+#include <bh_b200.h>
 #include <bohrium/bh_main_memory.hpp>
 #include "engine.hpp"
 
@@ -60,6 +63,7 @@ struct DeviceApi {
                                CUstream, void **, void **) = nullptr;
     CUresult (*cuOccupancyMaxActiveBlocksPerMultiprocessor)(int *, CUfunction, int, size_t) = nullptr;
     CUresult (*cuGetErrorString)(CUresult, const char **) = nullptr;
+    CUresult (*cuFuncGetAttribute)(int *, CUfunction_attribute, CUfunction) = nullptr;
 
     template <typename F>
     void get(const char *name, F &fp) {
@@ -75,6 +79,7 @@ struct DeviceApi {
         get("cuLaunchKernel", cuLaunchKernel);
         get("cuOccupancyMaxActiveBlocksPerMultiprocessor", cuOccupancyMaxActiveBlocksPerMultiprocessor);
         get("cuGetErrorString", cuGetErrorString);
+        get("cuFuncGetAttribute", cuFuncGetAttribute);
     }
     void ck(CUresult r, const char *what) const {
         if (r != CUDA_SUCCESS) {
@@ -99,6 +104,10 @@ EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
     cache_dir = cfg.defaultGet<string>("cache_dir", "");
     if (cache_dir == "NONE") cache_dir.clear();
     _device = cfg.defaultGet<int>("device_number", 0);
+    learned_on = cfg.defaultGet<bool>("learned", false);
+    learned_runs = cfg.defaultGet<int>("learned_runs", 2);
+    record = cfg.defaultGet<bool>("record", false);
+    chooser = [this](const vector<pair<const Block *, const Block *>> &cands) { return choose_merge(cands); };
 
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
@@ -126,6 +135,11 @@ EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
     check(cudaMalloc(&err_record, sizeof(unsigned long long)), "cudaMalloc(err)");
     check(cudaMemset(err_record, 0, sizeof(unsigned long long)), "cudaMemset(err)");
     if (!cache_dir.empty()) mkdir(cache_dir.c_str(), 0755);
+    autotune = cfg.defaultGet<bool>("autotune", true);
+    tune_min_elements = cfg.defaultGet<int64_t>("autotune_min_elements", 1 << 20);
+    load_tune_choices();
+    const string model = cfg.defaultGet<string>("costmodel", "");
+    if (!model.empty() && model != "NONE") load_costmodel(model);
 }
 
 EngineCUDA::~EngineCUDA() {
@@ -140,6 +154,9 @@ EngineCUDA::~EngineCUDA() {
         for (void *p : staging_retired) cudaFreeHost(p);
         if (staging_event) cudaEventDestroy(static_cast<cudaEvent_t>(staging_event));
         if (err_record) cudaFree(err_record);
+        if (rec_e0) cudaEventDestroy(static_cast<cudaEvent_t>(rec_e0));
+        if (rec_e1) cudaEventDestroy(static_cast<cudaEvent_t>(rec_e1));
+        if (cm) bh_ve_cuda_costmodel_destroy(cm);
         cudaStreamDestroy(static_cast<cudaStream_t>(_stream));
     } catch (...) {
     }
@@ -331,6 +348,133 @@ unsigned int *EngineCUDA::ensure_counters(int64_t n) {
 }
 
 // ------------------------------------------------------------------------------- compilation
+namespace {
+
+vector<string> nvrtc_options(bool fmad, int maxrreg = 0) {
+    vector<string> o = {"-arch=sm_100a", "-std=c++17", fmad ? "--fmad=true" : "--fmad=false", "-lineinfo"};
+    if (maxrreg > 0) o.push_back("--maxrregcount=" + to_string(maxrreg));
+    return o;
+}
+
+// NVRTC compilation of one source to a cubin (thread-safe: one program per call). Returns the
+// compiler log through `error` on failure.
+bool nvrtc_cubin(const string &name, const string &source, const vector<string> &opts, vector<char> &cubin,
+                 string &error) {
+    nvrtcProgram prog;
+    if (nvrtcCreateProgram(&prog, source.c_str(), (name + ".cu").c_str(), 0, nullptr, nullptr) != NVRTC_SUCCESS) {
+        error = "nvrtcCreateProgram failed for " + name;
+        return false;
+    }
+    vector<const char *> copts;
+    for (const string &o : opts) copts.push_back(o.c_str());
+    const nvrtcResult r = nvrtcCompileProgram(prog, static_cast<int>(copts.size()), copts.data());
+    if (r != NVRTC_SUCCESS) {
+        size_t logsz = 0;
+        nvrtcGetProgramLogSize(prog, &logsz);
+        string log(logsz, '\0');
+        nvrtcGetProgramLog(prog, &log[0]);
+        nvrtcDestroyProgram(&prog);
+        error = "NVRTC compilation of " + name + " failed:\n" + log + "\n--- source ---\n" + source;
+        return false;
+    }
+    size_t n = 0;
+    nvrtcGetCUBINSize(prog, &n);
+    cubin.resize(n);
+    const bool ok = nvrtcGetCUBIN(prog, cubin.data()) == NVRTC_SUCCESS;
+    nvrtcDestroyProgram(&prog);
+    if (!ok) error = "nvrtcGetCUBIN failed for " + name;
+    return ok;
+}
+
+} // namespace
+
+string EngineCUDA::disk_cache_path(const string &source, int maxrreg) const {
+    if (cache_dir.empty()) return "";
+    int nvrtc_major = 0, nvrtc_minor = 0;
+    nvrtcVersion(&nvrtc_major, &nvrtc_minor);
+    string key = source;
+    for (const string &o : nvrtc_options(fmad, maxrreg)) key += o;
+    key += to_string(nvrtc_major) + "." + to_string(nvrtc_minor);
+    stringstream ss;
+    ss << cache_dir << "/" << hex << fnv1a(key.data(), key.size()) << ".cubin";
+    return ss.str();
+}
+
+void EngineCUDA::precompile(const vector<const LaunchUnit *> &units) {
+    // Sources that are neither loaded, nor compiled ahead, nor in the disk cache.
+    vector<const LaunchUnit *> todo;
+    set<uint64_t> seen;
+    for (const LaunchUnit *u : units) {
+        const uint64_t h = fnv1a(u->source.data(), u->source.size());
+        if (functions.count(h) || ahead.count(h) || !seen.insert(h).second) continue;
+        const string path = disk_cache_path(u->source);
+        if (!path.empty() && access(path.c_str(), R_OK) == 0) continue;
+        todo.push_back(u);
+    }
+    if (todo.size() < 2) return;
+    const auto t0 = chrono::steady_clock::now();
+    const vector<string> opts = nvrtc_options(fmad);
+    vector<vector<char>> cubins(todo.size());
+    vector<string> errors(todo.size());
+    atomic<size_t> next{0};
+    const size_t nthreads = min<size_t>(todo.size(), max(1u, min(16u, thread::hardware_concurrency())));
+    vector<thread> pool;
+    for (size_t t = 0; t < nthreads; ++t) {
+        pool.emplace_back([&]() {
+            for (size_t i = next++; i < todo.size(); i = next++)
+                nvrtc_cubin(todo[i]->name, todo[i]->source, opts, cubins[i], errors[i]);
+        });
+    }
+    for (thread &th : pool) th.join();
+    for (size_t i = 0; i < todo.size(); ++i) {
+        if (!errors[i].empty()) throw runtime_error(errors[i]);
+        ahead[fnv1a(todo[i]->source.data(), todo[i]->source.size())] = std::move(cubins[i]);
+    }
+    _stats.time_compile += seconds_since(t0);
+    _stats.parallel_compiles += todo.size();
+}
+
+vector<char> EngineCUDA::cubin_for(const string &name, const string &source, int maxrreg) {
+    vector<char> cubin;
+    const string path = disk_cache_path(source, maxrreg);
+    if (!path.empty()) {
+        ifstream in(path, ios::binary);
+        if (in) cubin.assign(istreambuf_iterator<char>(in), istreambuf_iterator<char>());
+        if (!cubin.empty()) {
+            ++_stats.disk_cache_hits;
+            return cubin;
+        }
+    }
+    string error;
+    if (!nvrtc_cubin(name, source, nvrtc_options(fmad, maxrreg), cubin, error)) throw runtime_error(error);
+    if (!path.empty()) {
+        const string tmp = path + ".tmp" + to_string(getpid());
+        ofstream out(tmp, ios::binary);
+        out.write(cubin.data(), static_cast<streamsize>(cubin.size()));
+        out.close();
+        rename(tmp.c_str(), path.c_str());
+    }
+    return cubin;
+}
+
+EngineCUDA::Compiled::Variant EngineCUDA::load_variant(const vector<char> &cubin, const string &name, int maxrreg) {
+    CUmodule mod;
+    api->ck(api->cuModuleLoadData(&mod, cubin.data()), "cuModuleLoadData");
+    Compiled::Variant v;
+    CUfunction f, fb;
+    api->ck(api->cuModuleGetFunction(&f, mod, name.c_str()), "cuModuleGetFunction");
+    api->ck(api->cuModuleGetFunction(&fb, mod, (name + "_batch").c_str()), "cuModuleGetFunction(batch)");
+    v.fn = reinterpret_cast<void *>(f);
+    v.fn_batch = reinterpret_cast<void *>(fb);
+    api->ck(api->cuOccupancyMaxActiveBlocksPerMultiprocessor(&v.occ, f, kThreads, 0), "cuOccupancy");
+    api->ck(api->cuOccupancyMaxActiveBlocksPerMultiprocessor(&v.occ_batch, fb, kThreads, 0), "cuOccupancy");
+    api->ck(api->cuFuncGetAttribute(&v.regs, CU_FUNC_ATTRIBUTE_NUM_REGS, f), "cuFuncGetAttribute");
+    v.occ = max(v.occ, 1);
+    v.occ_batch = max(v.occ_batch, 1);
+    v.maxrreg = maxrreg;
+    return v;
+}
+
 EngineCUDA::Compiled *EngineCUDA::compiled_for(const LaunchUnit &u) {
     const uint64_t h = fnv1a(u.source.data(), u.source.size());
     auto it = functions.find(h);
@@ -340,45 +484,12 @@ EngineCUDA::Compiled *EngineCUDA::compiled_for(const LaunchUnit &u) {
     }
     ++_stats.kernel_cache_misses;
     const auto t0 = chrono::steady_clock::now();
-    int nvrtc_major = 0, nvrtc_minor = 0;
-    nvrtcVersion(&nvrtc_major, &nvrtc_minor);
-    vector<string> opts = {"-arch=sm_100a", "-std=c++17", fmad ? "--fmad=true" : "--fmad=false", "-lineinfo"};
-    string key = u.source;
-    for (const string &o : opts) key += o;
-    key += to_string(nvrtc_major) + "." + to_string(nvrtc_minor);
-    const uint64_t disk_hash = fnv1a(key.data(), key.size());
     vector<char> cubin;
-    string path;
-    if (!cache_dir.empty()) {
-        stringstream ss;
-        ss << cache_dir << "/" << hex << disk_hash << ".cubin";
-        path = ss.str();
-        ifstream in(path, ios::binary);
-        if (in) {
-            cubin.assign(istreambuf_iterator<char>(in), istreambuf_iterator<char>());
-            if (!cubin.empty()) ++_stats.disk_cache_hits;
-        }
-    }
-    if (cubin.empty()) {
-        nvrtcProgram prog;
-        check_nvrtc(nvrtcCreateProgram(&prog, u.source.c_str(), (u.name + ".cu").c_str(), 0, nullptr, nullptr),
-                    "nvrtcCreateProgram");
-        vector<const char *> copts;
-        for (const string &o : opts) copts.push_back(o.c_str());
-        const nvrtcResult r = nvrtcCompileProgram(prog, static_cast<int>(copts.size()), copts.data());
-        if (r != NVRTC_SUCCESS) {
-            size_t logsz = 0;
-            nvrtcGetProgramLogSize(prog, &logsz);
-            string log(logsz, '\0');
-            nvrtcGetProgramLog(prog, &log[0]);
-            nvrtcDestroyProgram(&prog);
-            throw runtime_error("NVRTC compilation of " + u.name + " failed:\n" + log + "\n--- source ---\n" + u.source);
-        }
-        size_t n = 0;
-        check_nvrtc(nvrtcGetCUBINSize(prog, &n), "nvrtcGetCUBINSize");
-        cubin.resize(n);
-        check_nvrtc(nvrtcGetCUBIN(prog, cubin.data()), "nvrtcGetCUBIN");
-        nvrtcDestroyProgram(&prog);
+    auto pre = ahead.find(h);
+    if (pre != ahead.end()) {
+        cubin = std::move(pre->second);
+        ahead.erase(pre);
+        const string path = disk_cache_path(u.source);
         if (!path.empty()) {
             const string tmp = path + ".tmp" + to_string(getpid());
             ofstream out(tmp, ios::binary);
@@ -386,22 +497,30 @@ EngineCUDA::Compiled *EngineCUDA::compiled_for(const LaunchUnit &u) {
             out.close();
             rename(tmp.c_str(), path.c_str());
         }
+    } else {
+        cubin = cubin_for(u.name, u.source, 0);
     }
-    CUmodule mod;
-    api->ck(api->cuModuleLoadData(&mod, cubin.data()), "cuModuleLoadData");
     Compiled c;
-    CUfunction f, fb;
-    api->ck(api->cuModuleGetFunction(&f, mod, u.name.c_str()), "cuModuleGetFunction");
-    api->ck(api->cuModuleGetFunction(&fb, mod, (u.name + "_batch").c_str()), "cuModuleGetFunction(batch)");
-    c.fn = reinterpret_cast<void *>(f);
-    c.fn_batch = reinterpret_cast<void *>(fb);
-    api->ck(api->cuOccupancyMaxActiveBlocksPerMultiprocessor(&c.occ, f, kThreads, 0), "cuOccupancy");
-    api->ck(api->cuOccupancyMaxActiveBlocksPerMultiprocessor(&c.occ_batch, fb, kThreads, 0), "cuOccupancy");
-    c.occ = max(c.occ, 1);
-    c.occ_batch = max(c.occ_batch, 1);
+    c.name = u.name;
+    c.source = u.source;
+    c.variants.push_back(load_variant(cubin, u.name, 0));
+    // A register cap chosen by an earlier tuning run of this source.
+    auto tc = tune_choices.find(h);
+    if (tc != tune_choices.end()) {
+        c.tuned = true;
+        if (tc->second > 0) {
+            c.variants.push_back(load_variant(cubin_for(u.name, u.source, tc->second), u.name, tc->second));
+            c.chosen = 1;
+        }
+    }
+    const Compiled::Variant &v = c.variants[static_cast<size_t>(c.chosen)];
+    c.fn = v.fn;
+    c.fn_batch = v.fn_batch;
+    c.occ = v.occ;
+    c.occ_batch = v.occ_batch;
     _stats.time_compile += seconds_since(t0);
     if (verbose) cerr << "[ve_cuda] compiled " << u.name << "\n" << u.source << endl;
-    return &functions.emplace(h, c).first->second;
+    return &functions.emplace(h, std::move(c)).first->second;
 }
 
 // ------------------------------------------------------------------------------------ launch
@@ -418,8 +537,11 @@ void EngineCUDA::pack_params(const PlanUnit &pu, const vector<bh_base *> &bases,
         uint8_t *slot = out + i * 8;
         switch (f.kind) {
             case ParamField::PTR: {
-                bh_base *b = pu.ptr_base[i] >= 0 ? bases[static_cast<size_t>(pu.ptr_base[i])] : f.base;
-                void *p = getBuffer(b);
+                const int idx = pu.ptr_base[i];
+                bh_base *b = idx >= 0 ? bases[static_cast<size_t>(idx)] : f.base;
+                void *p = ptr_override != nullptr && idx >= 0 && (*ptr_override)[static_cast<size_t>(idx)] != nullptr
+                              ? (*ptr_override)[static_cast<size_t>(idx)]
+                              : getBuffer(b);
                 memcpy(slot, &p, 8);
                 break;
             }
@@ -486,6 +608,11 @@ void EngineCUDA::launch_plain(const PlanUnit &pu, const vector<bh_base *> &bases
     const int64_t resident = static_cast<int64_t>(_sm_count) * pu.compiled->occ;
     const int64_t grid = max<int64_t>(1, min<int64_t>(work, resident));
     void *args[] = {params.data()};
+    if (autotune && !pu.compiled->tuned && u.elements >= tune_min_elements && !prof && !record &&
+        tune_launch(*pu.compiled, u, work, args)) {
+        ++_stats.launches;
+        return;
+    }
     UnitRecord rec{u.name, u.sched, u.elements, u.algorithmic_bytes, 1, 0.f};
     void *e0 = nullptr;
     record_begin(rec, e0);
@@ -495,6 +622,11 @@ void EngineCUDA::launch_plain(const PlanUnit &pu, const vector<bh_base *> &bases
     record_end(rec, e0);
     ++_stats.launches;
     if (u.sched == Sched::SERIAL) ++_stats.serial_units;
+}
+
+int EngineCUDA::launch_raw(void *fn, int64_t grid, void **args) {
+    return static_cast<int>(api->cuLaunchKernel(reinterpret_cast<CUfunction>(fn), static_cast<unsigned>(grid), 1, 1,
+                                                kThreads, 1, 1, 0, static_cast<CUstream>(_stream), args, nullptr));
 }
 
 void EngineCUDA::launch_batched(const vector<const PlanUnit *> &group, const vector<bh_base *> &bases,
@@ -794,12 +926,24 @@ EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const
     };
     // Dependency levels: a kernel runs after every earlier kernel it shares a written base with.
     vector<int> last_write_level(base_ids.size(), -1), last_read_level(base_ids.size(), -1);
-    for (const LoopB &kernel : kernels) {
+    // Lower every kernel first so that all new sources compile in parallel.
+    vector<vector<LaunchUnit>> lowered(kernels.size());
+    {
+        const auto tc = chrono::steady_clock::now();
+        vector<const LaunchUnit *> all;
+        for (size_t k = 0; k < kernels.size(); ++k) {
+            if (kernels[k].isSystemOnly()) continue;
+            lowered[k] = lower_kernel(kernels[k], cg_opt);
+            for (const LaunchUnit &u : lowered[k]) all.push_back(&u);
+        }
+        _stats.time_codegen += seconds_since(tc);
+        precompile(all);
+    }
+    for (size_t kidx = 0; kidx < kernels.size(); ++kidx) {
+        const LoopB &kernel = kernels[kidx];
         PlanKernel pk;
         if (!kernel.isSystemOnly()) {
-            const auto tc = chrono::steady_clock::now();
-            vector<LaunchUnit> units = lower_kernel(kernel, cg_opt);
-            _stats.time_codegen += seconds_since(tc);
+            vector<LaunchUnit> &units = lowered[kidx];
             for (LaunchUnit &u : units) {
                 PlanUnit pu;
                 pu.compiled = compiled_for(u);
@@ -832,6 +976,23 @@ EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const
             }
         }
         pk.writes.assign(writes.begin(), writes.end());
+        if ((record || learned_on) && !pk.units.empty()) pk.feat = jitk::block_features(kernel);
+        // Summation order of the floating-point sums and products: "seq" (one thread folds in
+        // index order) unless a unit reduces the sweep across threads.
+        for (const InstrPtr &instr : all_instr(kernel)) {
+            if (!bh_opcode_is_sweep(instr->opcode)) continue;
+            const bh_opcode op = instr->opcode;
+            if (op != BH_ADD_REDUCE && op != BH_MULTIPLY_REDUCE && op != BH_ADD_ACCUMULATE &&
+                op != BH_MULTIPLY_ACCUMULATE)
+                continue;
+            const bh_type t = instr->operand[0].base->dtype();
+            if (t != bh_type::FLOAT32 && t != bh_type::FLOAT64 && t != bh_type::COMPLEX64 && t != bh_type::COMPLEX128)
+                continue;
+            plan.orders[instr->origin_id] = "seq";
+        }
+        for (const PlanUnit &pu : pk.units)
+            for (const auto &ro : pu.unit.red_orders)
+                if (plan.orders.count(ro.first)) plan.orders[ro.first] = ro.second;
         int level = 0;
         for (int b : reads) level = max(level, last_write_level[b] + 1);
         for (int b : writes) level = max(level, max(last_write_level[b], last_read_level[b]) + 1);
@@ -846,6 +1007,10 @@ EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const
 }
 
 void EngineCUDA::run_plan(const FlushPlan &plan, const vector<bh_base *> &bases, const vector<bh_instruction *> &instrs) {
+    if (record) {
+        record_kernel_times(plan, bases, instrs);
+        return;
+    }
     if (batch_mode == "off" || plan.kernels.size() < 2) {
         for (const PlanKernel &pk : plan.kernels) {
             ++_stats.kernels;
@@ -891,10 +1056,25 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
     if (bhir->_fingerprint != 0) {
         auto rit = replays.find(bhir->_fingerprint);
         if (rit != replays.end() && replay_valid(rit->second)) {
-            const Replay &r = rit->second;
+            Replay &r = rit->second;
             for (bh_base *b : r.dead) free_base(b);
             const auto t1 = chrono::steady_clock::now();
             _stats.time_prepare += chrono::duration<double>(t1 - t0).count();
+            if (batch_mode == "graph" && !prof && !record) {
+                if (r.graph && !graph_usable(*r.graph)) r.graph.reset();
+                if (!r.graph && !r.graph_failed && r.valid_runs >= 1 && !build_graph(r)) r.graph_failed = true;
+                ++r.valid_runs;
+                if (r.graph) {
+                    ++_stats.plan_cache_hits;
+                    ++_stats.replays;
+                    graph_launch(*r.graph);
+                    _stats.time_launch += seconds_since(t1);
+                    copyToHost(bhir->_syncs, false);
+                    check_error_record();
+                    _stats.time_exec_host += seconds_since(t0);
+                    return;
+                }
+            }
             if (staging_used > 0 && staging_event)
                 check(cudaEventSynchronize(static_cast<cudaEvent_t>(staging_event)), "cudaEventSynchronize(staging)");
             staging_used = 0;
@@ -921,16 +1101,25 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
     }
     staging_used = 0;
     auto it = sliding ? plans.end() : plans.find(key);
+    auto tit = sliding ? trials.end() : trials.find(key);
     if (it != plans.end() && it->second.nbases == base_ids.size()) {
         ++_stats.plan_cache_hits;
         run_plan(it->second, base_ids, instr_list);
+    } else if (tit != trials.end() && tit->second.greedy.nbases == base_ids.size()) {
+        ++_stats.plan_cache_hits;
+        run_trial(key, tit->second, base_ids, instr_list);
     } else {
         ++_stats.plan_cache_misses;
         const vector<LoopB> kernels = kernels_for(instr_list, key, base_ids);
         FlushPlan plan = build_plan(kernels, base_ids);
         plan.nbases = base_ids.size();
-        run_plan(plan, base_ids, instr_list);
-        if (!sliding) plans[key] = std::move(plan);
+        if (!sliding && learned_on && cm != nullptr && !decided.count(key) &&
+            start_trial(key, instr_list, base_ids, plan)) {
+            run_trial(key, trials.at(key), base_ids, instr_list);
+        } else {
+            run_plan(plan, base_ids, instr_list);
+            if (!sliding) plans[key] = std::move(plan);
+        }
     }
     if (bhir->_fingerprint != 0 && !sliding) {
         auto pit = plans.find(key);
@@ -1071,10 +1260,17 @@ string EngineCUDA::statistics() const {
        << "\nkernel_cache_misses: " << _stats.kernel_cache_misses << "\ndisk_cache_hits: " << _stats.disk_cache_hits
        << "\nbytes_h2d: " << _stats.bytes_h2d << "\nbytes_d2h: " << _stats.bytes_d2h
        << "\ntime_fusion: " << _stats.time_fusion << "\ntime_codegen: " << _stats.time_codegen
-       << "\ntime_compile: " << _stats.time_compile << "\ntime_exec_host: " << _stats.time_exec_host
+       << "\ntime_compile: " << _stats.time_compile << "\nparallel_compiles: " << _stats.parallel_compiles
+       << "\ntuned_kernels: " << _stats.tuned_kernels << "\ntuned_capped: " << _stats.tuned_capped
+       << "\ntune_launches: " << _stats.tune_launches
+       << "\ntime_exec_host: " << _stats.time_exec_host
        << "\ntime_prepare: " << _stats.time_prepare << "\ntime_launch: " << _stats.time_launch
        << "\nplan_cache_hits: " << _stats.plan_cache_hits << "\nplan_cache_misses: " << _stats.plan_cache_misses
-       << "\nreplays: " << _stats.replays << "\n";
+       << "\nreplays: " << _stats.replays << "\nlearned_trials: " << _stats.learned_trials
+       << "\nlearned_kept: " << _stats.learned_kept << "\ngreedy_kept: " << _stats.greedy_kept
+       << "\nlearned_same_plan: " << _stats.learned_same << "\nlearned_order_differs: " << _stats.learned_order_differs
+       << "\nlearned_predictions: " << _stats.learned_predictions
+       << "\ntime_learned_fusion: " << _stats.time_learned_fusion << "\nrecords: " << record_count() << "\n";
     if (!_stats.records.empty()) {
         ss << "units:\n";
         for (const UnitRecord &r : _stats.records)

@@ -20,8 +20,11 @@
 #include <unordered_map>
 #include <vector>
 #include <bohrium/bh_component.hpp>
+#include "../jitk/costmodel.hpp"
 #include "../jitk/fuser.hpp"
 #include "codegen.hpp"
+
+struct bh_costmodel; // the cost model's network (mlp.cu)
 
 namespace bohrium {
 namespace cuda {
@@ -45,6 +48,13 @@ struct Stats {
     uint64_t kernel_cache_hits = 0, kernel_cache_misses = 0, disk_cache_hits = 0;
     uint64_t bytes_h2d = 0, bytes_d2h = 0;
     uint64_t serial_units = 0;
+    // learned fusion: structures tried with both plans, kept learned / kept greedy, learned plan
+    // identical to the greedy one, learned plan rejected because a reduction order differed
+    uint64_t learned_trials = 0, learned_kept = 0, greedy_kept = 0, learned_same = 0, learned_order_differs = 0;
+    uint64_t learned_predictions = 0;
+    uint64_t parallel_compiles = 0; // sources compiled ahead in parallel
+    uint64_t tuned_kernels = 0, tuned_capped = 0, tune_launches = 0;
+    double time_learned_fusion = 0;
     double time_fusion = 0, time_codegen = 0, time_compile = 0, time_exec_host = 0;
     double time_prepare = 0, time_launch = 0; // host time: list clean-up + hashing, plan execution
     std::vector<UnitRecord> records; // filled when profiling
@@ -88,14 +98,45 @@ public:
 
     // A compiled unit: the plain kernel, its batched twin and their resident CTAs per SM.
     struct Compiled {
-        void *fn = nullptr, *fn_batch = nullptr;
+        void *fn = nullptr, *fn_batch = nullptr; // the variant in use
         int occ = 1, occ_batch = 1;
+        // Autotuning (tune.cpp): register-capped variants of the same source, timed on their
+        // first launches; the fastest becomes fn/fn_batch. Variants compute identical results.
+        struct Variant {
+            void *fn = nullptr, *fn_batch = nullptr;
+            int occ = 1, occ_batch = 1, maxrreg = 0, regs = 0;
+            std::vector<float> ms;
+        };
+        std::vector<Variant> variants; // [0]: the default compilation
+        std::string name, source;
+        bool tuned = false, tuning = false;
+        int chosen = 0;
     };
     // Compiled kernels of a unit (NVRTC on first use, then the in-memory or disk cache).
     Compiled *compiled_for(const LaunchUnit &u);
 
     // Merge chooser used when the fuser list contains "learned" (set by the cost model).
     jitk::MergeChooser chooser;
+
+    // Learned fusion (learned.cpp). With a cost model loaded and `learned_on`, a flush structure
+    // seen for the first time also gets a learned plan (greedy contraction ordered by the model's
+    // predicted gain, every merge still legal by mergeable()). The learned plan is tried only when
+    // it folds every floating-point sum and product in the same order as the greedy plan (so its
+    // results are bit-identical); both plans are then timed on the device `learned_runs` times and
+    // the faster one is kept for that structure.
+    bool learned_on = false;
+    bool record = false;           // record (features, device microseconds) of every kernel run
+    int learned_runs = 2;
+    double learned_min_gain_us = 0.0;
+    // Load a model file written by bohrium_b200/costmodel.py (CostModel.save); throws on error.
+    void load_costmodel(const std::string &path);
+    bool has_costmodel() const { return cm != nullptr; }
+    // Replace the pre-fuser and transformer list (comma-separated names) and forget every plan.
+    void set_fusion(const std::string &pre_fuser, const std::string &fuser_list);
+    // Write the recorded rows (float32: features then microseconds); returns the row count.
+    size_t dump_records(const std::string &path) const;
+    void clear_records() { records.clear(); }
+    size_t record_count() const { return records.size() / (jitk::kCostFeatures + 1); }
 
     // Configuration
     bool prof = false;
@@ -104,6 +145,8 @@ public:
     jitk::FusionConfig fusion_config;
     std::string batch_mode = "off"; // off | grouped | graph
     bool fmad = false;
+    bool autotune = true;            // tune register caps of kernels with large work
+    int64_t tune_min_elements = 1 << 20;
     std::string cache_dir;
     uint64_t last_error_index = 0;
 
@@ -125,8 +168,19 @@ private:
     std::set<void *> pinned;        // host blocks from host_alloc()
     void *ev_begin = nullptr, *ev_end = nullptr, *tm_begin = nullptr, *tm_end = nullptr;
 
-    // Kernel cache: source hash -> compiled kernels
+    // Kernel cache: source hash -> compiled kernels; cubins compiled ahead of loading
     std::unordered_map<uint64_t, Compiled> functions;
+    std::unordered_map<uint64_t, std::vector<char>> ahead;
+    std::string disk_cache_path(const std::string &source, int maxrreg = 0) const; // "" without a cache dir
+    Compiled::Variant load_variant(const std::vector<char> &cubin, const std::string &name, int maxrreg);
+    std::vector<char> cubin_for(const std::string &name, const std::string &source, int maxrreg);
+    // Autotuning of plain launches (tune.cpp)
+    bool tune_launch(Compiled &c, const LaunchUnit &u, int64_t work, void **args);
+    std::map<uint64_t, int> tune_choices; // source hash -> chosen register cap (0: default)
+    void load_tune_choices();
+    void save_tune_choice(uint64_t hash, int maxrreg);
+    // NVRTC-compile the sources of `units` that are not cached yet, in parallel host threads.
+    void precompile(const std::vector<const LaunchUnit *> &units);
 
     // Scratch arena for grid reductions (tile partials), their completion counters and the error
     // record of bounds-checked kernels.
@@ -157,16 +211,33 @@ private:
         std::vector<PlanUnit> units;
         std::vector<int> frees, writes;
         int level = 0; // dependency level of the first unit
+        jitk::CostFeatures feat{}; // cost-model features (when recording or learning)
     };
     struct FlushPlan {
         std::vector<PlanKernel> kernels;
         int nlevels = 0;
         size_t nbases = 0;
+        // Summation order of every floating-point ADD/MULTIPLY sweep, by origin id.
+        std::map<int64_t, std::string> orders;
+        std::string signature() const; // kernel names by level (plans with equal signatures match)
     };
     std::unordered_map<uint64_t, FlushPlan> plans;
     // Replay of a fingerprinted BhIR (BhIR::_fingerprint): the plan, the bases in flush order,
     // the bases freed without being computed, and the bases whose constructor flag the plan
     // assumed (first used as an output) with that flag. A replay only has to re-check those flags.
+    // A replay's CUDA graph (batch mode "graph", graph.cpp).
+    struct ReplayGraph {
+        void *graph = nullptr, *exec = nullptr; // cudaGraph_t, cudaGraphExec_t
+        void *params_dev = nullptr;             // parameter blocks of grouped launches
+        void *stream = nullptr;
+        std::vector<void *> parked;             // buffers of arrays the flush creates and frees
+        std::vector<std::pair<bh_base *, void *>> persistent; // other arrays and their buffers
+        std::vector<bh_base *> written;         // arrays whose host copy a replay makes stale
+        void *scratch = nullptr;
+        unsigned int *counters = nullptr;
+        size_t nlaunches = 0;
+        ~ReplayGraph();
+    };
     struct Replay {
         const FlushPlan *plan = nullptr;
         std::vector<bh_base *> base_ids, dead;
@@ -175,9 +246,40 @@ private:
         // same structure, so constants and Random123 start/key must come from this flush.
         std::vector<bh_instruction> instr_copy;
         std::vector<bh_instruction *> instrs;
+        std::unique_ptr<ReplayGraph> graph;
+        bool graph_failed = false;
+        int valid_runs = 0;
     };
+    const std::vector<void *> *ptr_override = nullptr; // per base index: buffer to pack instead
+    bool graph_usable(const ReplayGraph &g) const;
+    void graph_launch(const ReplayGraph &g);
+    bool build_graph(Replay &r);
+    int launch_raw(void *fn, int64_t grid, void **args); // cuLaunchKernel on the engine's stream
     std::unordered_map<uint64_t, Replay> replays;
     bool replay_valid(const Replay &r) const;
+
+    // Learned fusion state (learned.cpp).
+    bh_costmodel *cm = nullptr;
+    std::vector<float> cm_mean, cm_std;
+    float cm_tmean = 0.f, cm_tstd = 1.f;
+    std::vector<float> records;
+    void *rec_e0 = nullptr, *rec_e1 = nullptr;
+    struct Trial {
+        FlushPlan greedy, learned;
+        std::vector<double> t_greedy, t_learned;
+    };
+    std::unordered_map<uint64_t, Trial> trials;
+    std::set<uint64_t> decided; // structures whose plan choice is final
+    std::unordered_map<uint64_t, float> pred_cache; // block key -> predicted microseconds
+    int choose_merge(const std::vector<std::pair<const jitk::Block *, const jitk::Block *>> &cands);
+    void predict_us(const std::vector<jitk::CostFeatures> &rows, std::vector<float> &out);
+    // The learned plan for a structure whose greedy plan was just built; true when a trial starts.
+    bool start_trial(uint64_t key, std::vector<bh_instruction *> &instr_list, const std::vector<bh_base *> &base_ids,
+                     FlushPlan &greedy);
+    void run_trial(uint64_t key, Trial &t, const std::vector<bh_base *> &bases,
+                   const std::vector<bh_instruction *> &instrs);
+    void record_kernel_times(const FlushPlan &plan, const std::vector<bh_base *> &bases,
+                             const std::vector<bh_instruction *> &instrs);
     FlushPlan build_plan(const std::vector<jitk::LoopB> &kernels, const std::vector<bh_base *> &base_ids);
     void run_plan(const FlushPlan &plan, const std::vector<bh_base *> &bases, const std::vector<bh_instruction *> &instrs);
     void pack_params(const PlanUnit &pu, const std::vector<bh_base *> &bases, const std::vector<bh_instruction *> &instrs,

@@ -82,6 +82,24 @@ public:
             engine.batch_mode = msg.substr(12);
         } else if (msg.rfind("CUDA: prof ", 0) == 0) {
             engine.prof = msg.substr(11) == "on";
+        } else if (msg.rfind("CUDA: record ", 0) == 0) {
+            engine.record = msg.substr(13) == "on";
+        } else if (msg.rfind("CUDA: records dump ", 0) == 0) {
+            ss << engine.dump_records(msg.substr(19));
+            return ss.str();
+        } else if (msg == "CUDA: records clear") {
+            engine.clear_records();
+        } else if (msg == "CUDA: records count") {
+            ss << engine.record_count();
+            return ss.str();
+        } else if (msg.rfind("CUDA: costmodel load ", 0) == 0) {
+            engine.load_costmodel(msg.substr(21));
+        } else if (msg.rfind("CUDA: fuser ", 0) == 0) {
+            engine.set_fusion("", msg.substr(12));
+        } else if (msg.rfind("CUDA: pre_fuser ", 0) == 0) {
+            engine.set_fusion(msg.substr(16), "");
+        } else if (msg.rfind("CUDA: learned ", 0) == 0) {
+            engine.learned_on = msg.substr(14) == "on";
         }
         return ss.str() + child.message(msg);
     }

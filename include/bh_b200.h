@@ -110,6 +110,32 @@ void bhb_set_last_error(const char *msg);
  * or NULL on error. `fuser_list` overrides the transformer list (NULL: the engine default). */
 const char *bh_ve_cuda_dry_run(bhb_ir *ir, int compile, const char *fuser_list);
 
+/* --- libbh_ve_cuda.so: the learned fusion cost model's network (no counterpart in the reference,
+ * whose fuser is the plain greedy one, core/jitk/graph.cpp:319-365). An MLP of
+ * bh_ve_cuda_costmodel_nfeatures() inputs -> 64 -> 64 -> 1 (ReLU, float32) on the current
+ * device; inference and minibatch Adam training run in hand-written kernels with deterministic
+ * (fixed-order) reductions. Host arrays in and out; the loss is the mean squared error. Functions
+ * returning int give 0 on success and -1 with bhb_last_error() set. --- */
+typedef struct bh_costmodel bh_costmodel;
+int bh_ve_cuda_costmodel_nfeatures(void);
+int64_t bh_ve_cuda_costmodel_nparams(void);
+/* He-initialised weights from `seed`; NULL on error. */
+bh_costmodel *bh_ve_cuda_costmodel_create(uint64_t seed);
+void bh_ve_cuda_costmodel_destroy(bh_costmodel *cm);
+/* Parameters as float32[nparams]: W1[64][F], b1[64], W2[64][64], b2[64], W3[64], b3. Setting them
+ * also resets the Adam moments. */
+int bh_ve_cuda_costmodel_get_params(bh_costmodel *cm, float *out);
+int bh_ve_cuda_costmodel_set_params(bh_costmodel *cm, const float *in);
+/* y[r] = network(x[r]) for `rows` rows of F floats. */
+int bh_ve_cuda_costmodel_predict(bh_costmodel *cm, const float *x, int64_t rows, float *y);
+/* Gradient (float32[nparams]) and loss over all rows, without an update. */
+int bh_ve_cuda_costmodel_gradient(bh_costmodel *cm, const float *x, const float *t, int64_t rows, float *grad,
+                                  float *loss);
+/* `epochs` passes of minibatch Adam (beta 0.9/0.999) over the rows in a seeded order; `loss_out`
+ * (may be NULL) receives the final loss over all rows. */
+int bh_ve_cuda_costmodel_train(bh_costmodel *cm, const float *x, const float *t, int64_t rows, int epochs,
+                               int batch, float lr, uint64_t seed, float *loss_out);
+
 /* libbh_ve_cuda.so: allocation-free sum of `n` contiguous float64 values at device address `in`,
  * written to the device address `out`, enqueued on `stream` (a cudaStream_t; NULL: the legacy
  * default stream). No counterpart in the reference: it is the engine's ADD_REDUCE grid reduction

@@ -108,3 +108,25 @@ def test_bounds_are_parameters_not_constants():
         _, units = plan(prog, compile=False)
         names.add(units[0]["name"])
     assert len(names) == 1
+
+
+def test_row_reductions_of_contiguous_rows_use_lanes():
+    """A reduction over the contiguous axis with enough rows lowers to LANE_REDUCE (C lanes of one
+    CTA per row); few rows keep SPLIT_REDUCE; a reduction over the strided axis never uses lanes."""
+    def prog_rows(rt):
+        x = bh.empty(rt, (300, 1000), np.float64)
+        return [(x * 2.0 + 1.0).sum(axis=1) * 3.0]
+    res, units = plan(prog_rows)
+    assert [u["sched"] for u in units] == ["lane_reduce"], [u["sched"] for u in units]
+
+    def prog_few(rt):
+        x = bh.empty(rt, (20, 100000), np.float32)
+        return [x.max(axis=1)]
+    res, units = plan(prog_few)
+    assert "lane_reduce" not in [u["sched"] for u in units]
+
+    def prog_cols(rt):
+        x = bh.empty(rt, (1000, 300), np.float64)
+        return [x.sum(axis=0)]
+    res, units = plan(prog_cols)
+    assert "lane_reduce" not in [u["sched"] for u in units]

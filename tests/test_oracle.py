@@ -126,3 +126,21 @@ def test_oracle_repeat_with_sliding_views():
     ins.slides[2] = ([ir.Slide(0, 1, 0, 1, 10)], {})
     rt.ex.execute(ir.Flush([ins], nrepeats=10))
     assert acc.numpy()[0] == A.sum()
+
+
+def test_costmodel_oracle_gradient_matches_finite_differences():
+    """Pins the float64 network restatement (the checker of the GPU backward kernel)."""
+    from oracle import costmodel as O
+    rng = np.random.default_rng(0)
+    p = rng.standard_normal(O.NPARAMS) * 0.3
+    X = rng.standard_normal((9, O.F))
+    t = rng.standard_normal(9)
+    loss, g = O.loss_and_grad(p, X, t)
+    assert abs(loss - np.mean((O.forward(p, X) - t) ** 2)) < 1e-12
+    idx = np.concatenate([rng.choice(O.NPARAMS, 40, replace=False), [O.OFF_B3, O.OFF_W3, O.OFF_B1]])
+    h = 1e-6
+    for i in idx:
+        e = np.zeros(O.NPARAMS)
+        e[i] = h
+        fd = (O.loss_and_grad(p + e, X, t)[0] - O.loss_and_grad(p - e, X, t)[0]) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd)), (i, fd, g[i])

@@ -245,3 +245,91 @@ def test_replayed_flushes_keep_their_own_constants(gpu_executor, oracle_rt):
         want = float(np.sum(host * float(k + 2) + float(k)))
         got = float(gpu_executor.peek(y.base)[0])
         assert abs(got - want) <= 1e-12 * abs(want), (k, got, want)
+
+
+@pytest.mark.parametrize("rows,cols,dtype,op", [
+    (300, 1000, np.float64, "sum"), (512, 4096, np.float32, "max"), (200, 37, np.float32, "sum"),
+    (1000, 3000, np.int32, "sum"), (149, 70001, np.float64, "min"), (4096, 64, np.float32, "prod"),
+])
+def test_row_reductions_lane_schedule(gpu_rt, oracle_rt, rows, cols, dtype, op):
+    """Reductions over the contiguous axis of many rows (LANE_REDUCE), fused with the map before
+    and the instruction after, against the oracle."""
+    rng = np.random.default_rng(rows + cols)
+    host = rng.random((rows, cols))
+    if op == "prod":
+        host = 1.0 + (host - 0.5) * 1e-3
+    host = (host * 100).astype(dtype) if np.dtype(dtype).kind == "i" else host.astype(dtype)
+
+    def prog(rt):
+        x = bh.array(rt, host)
+        y = getattr(x * dtype(2) + dtype(1), op)(axis=1)
+        return [y, y * dtype(3)]
+
+    g, o = both(gpu_rt, oracle_rt, prog)
+    rtol = reduce_tol(dtype)
+    for a, b, what in zip(g, o, ["reduce", "after"]):
+        assert_close(a, b, rtol, rtol, what)
+
+
+def test_graph_replay_is_bit_identical(gpu_executor):
+    """Batch mode "graph": a re-executed flush is captured into a CUDA graph (grouped launches,
+    arrays created and freed inside the flush parked) and replayed; results equal the plain
+    one-launch-per-kernel results bit for bit, on every replay."""
+    from bohrium_b200 import workloads as W
+    rt = bh.Runtime(gpu_executor)
+    lengths = W.batching_lengths(48, 256, 30000, 11)
+    hosts = [np.random.default_rng(i).random(int(n), dtype=np.float32) for i, n in enumerate(lengths)]
+    xs = [bh.array(rt, h) for h in hosts]
+    rt.flush()
+    outs = []
+    for x in xs:
+        y = W.batching_chain(x)
+        t = y * np.float32(2)          # a temporary that the flush creates and frees
+        outs += [y, t.sum(), y.max(), (t - y).min()]
+    ir = gpu_executor.compile(rt.take())
+    results = {}
+    try:
+        for mode in ["off", "graph"]:
+            gpu_executor.message(f"CUDA: batch {mode}")
+            r0 = _stat(gpu_executor, "graph_replays")
+            runs = []
+            for _ in range(4):
+                ir.execute()
+                runs.append([gpu_executor.peek(o.base).tobytes() for o in outs])
+            results[mode] = runs
+            if mode == "graph":
+                assert _stat(gpu_executor, "graph_replays") - r0 >= 2
+    finally:
+        gpu_executor.message("CUDA: batch off")
+    for run in results["off"] + results["graph"]:
+        assert run == results["off"][0]
+
+
+def _stat(ex, key):
+    for line in ex.message("statistic").splitlines():
+        if line.startswith(key + ":"):
+            return float(line.split(":")[1])
+    return 0.0
+
+
+def test_autotuned_variants_are_bit_identical(gpu_executor):
+    """The first launches of a large kernel rotate through register-capped variants (autotuning);
+    every launch gives the same bits."""
+    from bohrium_b200 import workloads as W
+    rt = bh.Runtime(gpu_executor)
+    n = 3 << 20
+    S, K, T = W.black_scholes_inputs(n, 5)
+    s, k, t = (bh.array(rt, x) for x in (S, K, T))
+    rt.flush()
+    m = W.black_scholes_iteration(rt, s, k, t, 1)
+    ir = gpu_executor.compile(rt.take())
+    t0 = _stat(gpu_executor, "tune_launches")
+    seen = set()
+    for _ in range(10):
+        ir.execute()
+        seen.add(gpu_executor.peek(m.base).tobytes())
+    assert len(seen) == 1
+    assert _stat(gpu_executor, "tune_launches") > t0
+    want = W.black_scholes_numpy(S, K, T, 1)
+    got = float(np.frombuffer(seen.pop(), dtype=np.float64)[0])
+    assert abs(got - want) <= 1e-11 * abs(want)  # NumPy's exp/log differ from CUDA's by ulps
