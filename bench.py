@@ -386,7 +386,89 @@ def extra_batching(bh, W, ex, rt, out):
     out["batching_4096_systems_f32"] = res
 
 
-EXTRAS = {"plain_chain": extra_plain_chain, "heat": extra_heat, "batching": extra_batching}
+def extra_stream(bh, W, ex, rt, out, n=100_000_000):
+    """One fused streaming block on a large array: the 12-operation float32 chain of the batching
+    workload over 1e8 elements, keeping y and reducing sum(y) and max(y) (8 B per element)."""
+    x = bh.random_sample(rt, (n,), start=0, key=7, dtype=np.float32)
+    rt.flush()
+    y = W.batching_chain(x)
+    outs = [y, y.sum(), y.max()]
+    ir = ex.compile(rt.take())
+    for _ in range(3):
+        ir.execute()
+    ex.message("CUDA: sync")
+    reps = 10
+    ex.message("CUDA: timer start")
+    for _ in range(reps):
+        ir.execute()
+    ms = float(ex.message("CUDA: timer stop")) / reps
+    ex.message("CUDA: prof on")
+    ex.message("statistic_enable_and_reset")
+    ir.execute()
+    ex.message("CUDA: sync")
+    stat = ex.message("statistic")
+    ex.message("CUDA: prof off")
+    kernels = [line for line in stat.splitlines() if line.strip().startswith("- {name")]
+    k_ms = max((float(k.split("ms:")[1].strip(" }")) for k in kernels), default=ms)
+    name = max(kernels, key=lambda k: float(k.split("ms:")[1].strip(" }"))).split("name:")[1].split(",")[0].strip() \
+        if kernels else ""
+    bytes_ = 8 * n + 8
+    out["stream_f32_1e8"] = {"flush_ms_device": round(ms, 4), "GB/s": round(bytes_ / (ms / 1e3) / 1e9, 1),
+                             "kernel": name, "kernel_ms": round(k_ms, 4),
+                             "kernel_GB/s": round(bytes_ / (k_ms / 1e3) / 1e9, 1),
+                             "frac_of_peak": round(bytes_ / (k_ms / 1e3) / 1e9 / peaks()[0], 3),
+                             "launches_per_flush": len(kernels)}
+    del ir, outs, x
+
+
+def extra_scan(bh, W, ex, rt, out, n=50_000_000):
+    """A fused 1-D cumulative sum (SCAN1D): y = cumsum(2x + 1) over 5e7 float64 (8 B read + 8 B
+    written per element, algorithmically)."""
+    x = bh.random_sample(rt, (n,), start=5, key=3, dtype=np.float64)
+    rt.flush()
+    y = bh.accumulate("ADD_ACCUMULATE", x * 2.0 + 1.0, 0)
+    ir = ex.compile(rt.take())
+    for _ in range(3):
+        ir.execute()
+    ex.message("CUDA: sync")
+    reps = 10
+    ex.message("CUDA: timer start")
+    for _ in range(reps):
+        ir.execute()
+    ms = float(ex.message("CUDA: timer stop")) / reps
+    out["scan_f64_5e7"] = {"flush_ms_device": round(ms, 4), "GB/s": round(16 * n / (ms / 1e3) / 1e9, 1),
+                           "frac_of_peak": round(16 * n / (ms / 1e3) / 1e9 / peaks()[0], 3)}
+    del ir, y, x
+
+
+def extra_learned(bh, W, ex, rt, out, train_seeds=24, eval_seeds=12):
+    """The learned-fuser workload: seeded random bytecode DAGs (50-400 operations, 1e3-1e8
+    elements, float32/float64/int32, transposed/reversed/broadcast views, 0-3 reductions). The
+    engine records per-kernel device times on the training DAGs, the cost model is trained on the
+    GPU, and held-out DAGs are timed under the plain engine (greedy plan, one launch per kernel),
+    the batched engine (CUDA-graph replay) and the batched + learned engine."""
+    from bohrium_b200 import learn
+    t0 = time.perf_counter()
+    X, t = learn.collect(ex, seeds=range(train_seeds), max_elems=1e7)
+    t1 = time.perf_counter()
+    model, loss = learn.train(X, t, epochs=300)
+    t2 = time.perf_counter()
+    fd, path = tempfile.mkstemp(suffix=".cm")
+    os.close(fd)
+    try:
+        model.save(path)
+        rows = learn.evaluate(ex, seeds=range(1000, 1000 + eval_seeds), model_path=path, max_elems=1e8, reps=3)
+    finally:
+        os.unlink(path)
+    res = learn.summary(rows)
+    res.update({"records": int(X.shape[0]), "train_loss": round(loss, 4), "collect_s": round(t1 - t0, 1),
+                "train_s": round(t2 - t1, 2), "eval_s": round(time.perf_counter() - t2, 1),
+                "per_dag_speedup_vs_plain": [round(r["plain_ms"] / r["learned_ms"], 2) for r in rows]})
+    out["learned_fuser_random_dags"] = res
+
+
+EXTRAS = {"plain_chain": extra_plain_chain, "heat": extra_heat, "batching": extra_batching, "stream": extra_stream,
+          "scan": extra_scan, "learned": extra_learned}
 
 
 def run_extra(bh, W, ex, rt, peak, only=None, heat_n=4096):

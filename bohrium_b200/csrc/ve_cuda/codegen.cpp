@@ -41,22 +41,26 @@ int64_t LaunchUnit::work_items() const {
             const int64_t per = static_cast<int64_t>(kThreads) * V;
             return rows * ((cols + per - 1) / per);
         }
-        case Sched::GRID_REDUCE: return (cols + kReduceTile - 1) / kReduceTile;
+        case Sched::GRID_REDUCE: {
+            const int64_t tiles = (cols + kReduceTile - 1) / kReduceTile;
+            return (tiles + chunks - 1) / chunks;  // chunks: tiles per work item
+        }
         case Sched::SPLIT_REDUCE: return (rows * cols + kThreads - 1) / kThreads * chunks;
         case Sched::LANE_REDUCE: {
             const int64_t per = kThreads / chunks;
             return (rows * cols + per - 1) / per;
         }
         case Sched::OUTER_REDUCE: return (rows * cols + kThreads - 1) / kThreads;
-        case Sched::SCAN1D: return (cols + kScanChunk - 1) / kScanChunk;
+        case Sched::SCAN1D: return chunks;  // chunks: work items of the phase
         case Sched::SERIAL: return 1;
     }
     return 1;
 }
 
 int64_t LaunchUnit::scratch_bytes() const {
-    if (sched == Sched::GRID_REDUCE) return work_items() * scratch_bytes_per_tile;
+    if (sched == Sched::GRID_REDUCE) return (cols + kReduceTile - 1) / kReduceTile * scratch_bytes_per_tile;
     if (sched == Sched::SPLIT_REDUCE) return 8 * static_cast<int64_t>(nred) * chunks * rows * cols;
+    if (sched == Sched::SCAN1D) return 0;  // totals/carries live in the engine's scan arena
     return 0;
 }
 
@@ -125,6 +129,20 @@ template <typename T> __device__ __forceinline__ T bh_shfl_xor(T v, int m) {
         T r; memcpy(&r, &x, sizeof(T)); return r;
     }
 }
+
+// Completion counter of a reduction: an acquire-release increment at device scope, so the
+// partials this thread stored before are visible to whichever CTA sees the final count.
+__device__ __forceinline__ unsigned bh_arrive(unsigned *counter) {
+    unsigned old;
+    asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(old) : "l"(counter) : "memory");
+    return old;
+}
+__device__ __forceinline__ unsigned bh_arrive_n(unsigned *counter, unsigned n) {
+    unsigned old;
+    asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], %2;" : "=r"(old) : "l"(counter), "r"(n) : "memory");
+    return old;
+}
+__device__ __forceinline__ void bh_acquire() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 // Load through L2 only (ld.global.cg): for values that other CTAs wrote during this launch.
 template <typename T> __device__ __forceinline__ T bh_ldcg(const T *ptr) {
@@ -783,14 +801,29 @@ extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME__(const __grid_c
 }
 extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME___batch(const P* __restrict__ items,
         const bh_i64* __restrict__ prefix, int nitems, bh_i64 total) {
+    // The parameters of the current item live in shared memory; consecutive work items of a CTA
+    // usually belong to the same item, which then needs neither a search nor a reload.
+    __shared__ P sp;
+    int have = -1;
+    bh_i64 have_lo = 0, have_hi = 0;
     for (bh_i64 g = blockIdx.x; g < total; g += gridDim.x) {
-        int lo = 0, hi = nitems - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (prefix[mid] <= g) lo = mid; else hi = mid - 1;
+        if (g < have_lo || g >= have_hi) {
+            int lo = 0, hi = nitems - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (prefix[mid] <= g) lo = mid; else hi = mid - 1;
+            }
+            __syncthreads();
+            for (int k = threadIdx.x; k < (int)(sizeof(P) / 8); k += blockDim.x)
+                ((unsigned long long*)&sp)[k] = ((const unsigned long long*)(items + lo))[k];
+            __syncthreads();
+            have = lo;
+            have_lo = prefix[lo];
+            have_hi = prefix[lo + 1];
         }
-        bh_work(items[lo], g - prefix[lo]);
+        bh_work(sp, g - have_lo);
     }
+    (void)have;
 }
 )CUDA";
 
@@ -843,6 +876,53 @@ void declare_chain_temps(Emitter &em, Symbols &sym, Scope &scope, const vector<c
 }
 
 // FLAT: `loop` has P >= 1 leading parallel ranks.
+// Views that an innermost element loop only reads: the view's base is an array (not a
+// temporary) that no instruction of the kernel writes, and the view is read by a plain
+// elementwise or reduction instruction. Their V elements per thread can be loaded into registers
+// before the computation, so that all V loads are in flight together (branches in the element
+// code, e.g. IEEE sqrt's special-case path, would otherwise keep the compiler from hoisting them).
+vector<bh_view> preloadable_views(const LoopB &inner, const LoopB &kernel, const Symbols &sym) {
+    set<const bh_base *> written;
+    for (const InstrPtr &i : jitk::all_instr(kernel))
+        if (!i->operand.empty() && !i->operand[0].isConstant()) written.insert(i->operand[0].base);
+    vector<bh_view> ret;
+    set<ViewKey> seen;
+    for (const Block &b : inner._block_list) {
+        if (!b.isInstr()) return {};  // not an innermost loop
+        const bh_instruction &in = *b.getInstr();
+        const bh_opcode op = in.opcode;
+        if (bh_opcode_is_system(op) || op == BH_GATHER || op == BH_SCATTER || op == BH_COND_SCATTER ||
+            op == BH_RANGE || op == BH_RANDOM || bh_opcode_is_accumulate(op))
+            continue;
+        for (size_t o = 1; o < in.operand.size(); ++o) {
+            const bh_view &v = in.operand[o];
+            if (v.isConstant() || sym.temps.count(v.base) || written.count(v.base)) continue;
+            if (bh_opcode_is_sweep(op) && o > 1) continue;
+            if (seen.insert(ViewKey(v)).second) ret.push_back(v);
+        }
+    }
+    return ret;
+}
+
+// Emit the register arrays and the load loop of `views` for V elements per thread; element j has
+// index `idx_init(j)` (a statement defining the innermost loop index). With `guard` the loads
+// stop at the loop bound. Registers the replacements in `scope`.
+void emit_preload(Emitter &em, const vector<bh_view> &views, int V, const string &index_decl, const string &guard,
+                  Scope &scope, ostream &out, int ind) {
+    if (views.empty()) return;
+    const string sp(static_cast<size_t>(ind), ' ');
+    for (size_t k = 0; k < views.size(); ++k)
+        out << sp << cuda_type(views[k].base->dtype()) << " pl" << k << "[" << V << "];\n";
+    out << sp << "#pragma unroll\n";
+    out << sp << "for (int j = 0; j < " << V << "; ++j) {\n";
+    out << sp << "    " << index_decl << "\n";
+    if (!guard.empty()) out << sp << "    if (" << guard << ") break;\n";
+    for (size_t k = 0; k < views.size(); ++k)
+        out << sp << "    pl" << k << "[j] = " << em.array_ref(views[k]) << ";\n";
+    out << sp << "}\n";
+    for (size_t k = 0; k < views.size(); ++k) scope.repl[ViewKey(views[k])] = "pl" + to_string(k) + "[j]";
+}
+
 LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) {
     LaunchUnit u;
     u.sched = Sched::FLAT;
@@ -882,25 +962,25 @@ LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) 
     body << "    const bh_i64 cbase = chunk * " << per << " + threadIdx.x;\n";
     // The element body is written once and used twice: full chunks run without bounds checks (so
     // the compiler can issue every load of the unrolled loop early), the last chunk with them.
-    stringstream elem;
-    {
-        Emitter eb(sym, elem, opt);
-        Scope scope;
-        declare_chain_temps(eb, sym, scope, chain, P - 1, elem, 12);
-        eb.write_body(inner, scope, 12);
-    }
     const string n_inner = "p.n" + to_string(sym.loop_id.at(&inner));
-    body << "    if ((chunk + 1) * " << per << " <= " << n_inner << ") {\n";
-    body << "#pragma unroll\n";
-    body << "        for (int j = 0; j < " << u.V << "; ++j) {\n";
-    body << "            const bh_i64 i" << (P - 1) << " = cbase + j * " << kThreads << ";\n";
-    body << elem.str();
-    body << "        }\n    } else {\n";
-    body << "        for (int j = 0; j < " << u.V << "; ++j) {\n";
-    body << "            const bh_i64 i" << (P - 1) << " = cbase + j * " << kThreads << ";\n";
-    body << "            if (i" << (P - 1) << " >= " << n_inner << ") break;\n";
-    body << elem.str();
-    body << "        }\n    }\n}\n" << kWrappers;
+    const string idx_decl = "const bh_i64 i" + to_string(P - 1) + " = cbase + j * " + to_string(kThreads) + ";";
+    const vector<bh_view> pre = u.V > 1 ? preloadable_views(inner, L, sym) : vector<bh_view>{};
+    for (int path = 0; path < 2; ++path) {
+        // path 0: full chunks without bounds checks; path 1: the last chunk, with them.
+        const string guard = path == 0 ? "" : "i" + to_string(P - 1) + " >= " + n_inner;
+        body << (path == 0 ? "    if ((chunk + 1) * " + to_string(per) + " <= " + n_inner + ") {\n" : "    } else {\n");
+        Scope scope;
+        Emitter eb(sym, body, opt);
+        emit_preload(eb, pre, u.V, idx_decl, guard, scope, body, 8);
+        if (path == 0) body << "#pragma unroll\n";
+        body << "        for (int j = 0; j < " << u.V << "; ++j) {\n";
+        body << "            " << idx_decl << "\n";
+        if (path == 1) body << "            if (" << guard << ") break;\n";
+        declare_chain_temps(eb, sym, scope, chain, P - 1, body, 12);
+        eb.write_body(inner, scope, 12);
+        body << "        }\n";
+    }
+    body << "    }\n}\n" << kWrappers;
     u.fields = pl.fields;
     u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
     u.elements = rows * u.cols;
@@ -1061,6 +1141,7 @@ LaunchUnit lower_lane_reduce(const LoopB &loop, unsigned P, const CodegenOptions
     {
         Scope scope;
         declare_chain_temps(em, sym, scope, chain, P, body, 8);
+        body << "/*@unroll@*/\n";
         body << "        for (bh_i64 i" << P << " = lane; i" << P << " < p.n" << sub_lid << "; i" << P << " += " << C
              << ") {\n";
         Scope s1;
@@ -1202,6 +1283,7 @@ LaunchUnit lower_split_reduce(const LoopB &loop, unsigned P, const CodegenOption
         for (size_t k = 0; k < reds.size(); ++k) body << "        " << ctypes[k] << " pacc" << k << " = " << idents[k] << ";\n";
         body << "        const bh_i64 lo = chunk * p.chunk_len;\n";
         body << "        const bh_i64 hi = min(lo + p.chunk_len, (bh_i64)p.n" << sub_lid << ");\n";
+        body << "/*@unroll@*/\n";  // the autotuner may put an unroll pragma here
         body << "        for (bh_i64 i" << P << " = lo; i" << P << " < hi; ++i" << P << ") {\n";
         Scope s1;
         s1.parent = &scope;
@@ -1213,12 +1295,11 @@ LaunchUnit lower_split_reduce(const LoopB &loop, unsigned P, const CodegenOption
     body << "    }\n";
     body << "    __syncthreads();\n";
     body << "    if (threadIdx.x == 0) {\n";
-    body << "        __threadfence();\n";
-    body << "        am_last = atomicAdd(p.counter + pb, 1u) == (unsigned)(p.chunks - 1);\n";
+    body << "        am_last = bh_arrive((unsigned*)(p.counter + pb)) == (unsigned)(p.chunks - 1);\n";
     body << "    }\n";
     body << "    __syncthreads();\n";
     body << "    if (!am_last) return;\n";
-    body << "    __threadfence();\n";
+    body << "    bh_acquire();\n";
     body << "    if (threadIdx.x == 0) p.counter[pb] = 0u;\n";
     body << "    if (pt >= p.points) return;\n";
     {
@@ -1301,6 +1382,60 @@ string block_reduce_fn(const string &ctype, const string &fname, bh_opcode op, c
 // `identities` are the kernel-level identity instructions of those reductions (folded). Work item
 // = one tile of kReduceTile elements; the CTA that completes the last tile of a unit folds the
 // unit's tile partials in tile order and writes the results.
+// Tiles per GRID_REDUCE work item: with many tiles a CTA takes K consecutive tiles at once so that
+// K x 8 loads per thread are in flight together. Every tile keeps its own partial, reduced in the
+// same order, so the result does not depend on K; K only depends on the tile count.
+int grid_tiles_per_item(int64_t ntiles, const LoopB &L) {
+    // Only light element code is memory-latency bound; a heavy body (many instructions, float64
+    // math) is compute bound and would only lose occupancy to the extra registers.
+    int n = 0, heavy = 0;
+    for (const InstrPtr &i : jitk::all_instr(L)) {
+        ++n;
+        const bh_opcode op = i->opcode;
+        const bool f64 = !i->operand.empty() && !i->operand[0].isConstant() &&
+                         i->operand[0].base->dtype() == bh_type::FLOAT64;
+        if (f64 && (op == BH_DIVIDE || op == BH_EXP || op == BH_LOG || op == BH_SQRT || op == BH_POWER ||
+                    op == BH_SIN || op == BH_COS || op == BH_TANH))
+            ++heavy;
+    }
+    if (n > 24 || heavy > 0) return 1;
+    const int64_t resident = 148 * 4;
+    if (ntiles >= 4 * 4 * resident) return 4;
+    if (ntiles >= 2 * 2 * resident) return 2;
+    return 1;
+}
+
+// Block reduction of K values per thread at once (one shared-memory round for all K): the same
+// tree as bh_block_reduce for every k.
+string block_reduce_k_fn(const string &ctype, const string &fname, bh_opcode op, const string &identity, int K) {
+    stringstream ss;
+    ss << "__device__ __forceinline__ void " << fname << "(" << ctype << " (&v)[" << K << "], " << ctype << " *sm) {\n";
+    ss << "#pragma unroll\n";
+    ss << "    for (int k = 0; k < " << K << "; ++k) {\n";
+    ss << "#pragma unroll\n";
+    ss << "        for (int m = 16; m >= 1; m >>= 1) { const " << ctype << " o = bh_shfl_xor(v[k], m); v[k] = "
+       << reduce_expr(op, "v[k]", "o") << "; }\n";
+    ss << "    }\n";
+    ss << "    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n";
+    ss << "    __syncthreads();\n";
+    ss << "    if (lane == 0) {\n";
+    ss << "#pragma unroll\n";
+    ss << "        for (int k = 0; k < " << K << "; ++k) sm[warp * " << K << " + k] = v[k];\n";
+    ss << "    }\n";
+    ss << "    __syncthreads();\n";
+    ss << "    if (warp == 0) {\n";
+    ss << "#pragma unroll\n";
+    ss << "        for (int k = 0; k < " << K << "; ++k) {\n";
+    ss << "            v[k] = lane < " << (kThreads / 32) << " ? sm[lane * " << K << " + k] : " << identity << ";\n";
+    ss << "#pragma unroll\n";
+    ss << "            for (int m = 16; m >= 1; m >>= 1) { const " << ctype << " o = bh_shfl_xor(v[k], m); v[k] = "
+       << reduce_expr(op, "v[k]", "o") << "; }\n";
+    ss << "        }\n";
+    ss << "    }\n";
+    ss << "}\n";
+    return ss.str();
+}
+
 LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identities, const CodegenOptions &opt) {
     LaunchUnit u;
     u.sched = Sched::GRID_REDUCE;
@@ -1315,9 +1450,12 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
     u.nred = static_cast<int>(reds.size());
     u.cols = L.size;
     const int64_t ntiles = (L.size + kReduceTile - 1) / kReduceTile;
+    const int K = grid_tiles_per_item(ntiles, L);
+    u.chunks = K;
     ParamLayout pl;
     add_common_fields(sym, pl, opt);
-    pl.add(work_field(ntiles), "bh_i64", "work");
+    pl.add(work_field(ntiles), "bh_i64", "ntiles");
+    pl.add(work_field((ntiles + K - 1) / K), "bh_i64", "work");
     ParamField fs{ParamField::SCRATCH};
     pl.add(fs, "unsigned char*", "scratch");
     ParamField fc{ParamField::COUNTER};
@@ -1333,55 +1471,87 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
         idents.push_back(constant_literal(jitk::sweep_identity(r->opcode, t)));
         accs.push_back("tacc" + to_string(k));
         helpers << block_reduce_fn(ctypes[k], "bh_block_reduce" + to_string(k), r->opcode, idents[k]);
-        em.external_acc[ViewKey(r->operand[0])] = accs[k];
+        helpers << block_reduce_k_fn(ctypes[k], "bh_block_reduce_k" + to_string(k), r->opcode, idents[k], K);
     }
     u.scratch_bytes_per_tile = 8 * static_cast<int64_t>(reds.size());
     for (const InstrPtr &r : reds) u.red_orders.emplace_back(r->origin_id, "tree:" + to_string(L.size));
     body << helpers.str();
-    body << "__device__ void bh_work(const P &p, bh_i64 tile) {\n";
+    body << "__device__ void bh_work(const P &p, bh_i64 w) {\n";
     body << pointer_locals(sym);
-    body << "    __shared__ unsigned long long sm_raw[" << (kThreads / 32) << "];\n";
+    body << "    __shared__ unsigned long long sm_raw[" << (kThreads / 32) * K << "];\n";
     body << "    __shared__ bool am_last;\n";
     for (size_t k = 0; k < reds.size(); ++k)
-        body << "    " << ctypes[k] << "* part" << k << " = (" << ctypes[k] << "*)(p.scratch + p.work * " << 8 * k
+        body << "    " << ctypes[k] << "* part" << k << " = (" << ctypes[k] << "*)(p.scratch + p.ntiles * " << 8 * k
              << ");\n";
-    for (size_t k = 0; k < reds.size(); ++k) body << "    " << ctypes[k] << " " << accs[k] << " = " << idents[k] << ";\n";
-    // Full tiles run without bounds checks; the accumulation order (j = 0..7) is the same in both.
-    stringstream elem;
-    {
-        Emitter eb(sym, elem, opt);
-        eb.external_acc = em.external_acc;
-        Scope scope;
-        eb.write_body(L, scope, 12);
-    }
-    const string n0 = "p.n" + to_string(sym.loop_id.at(&L));
-    body << "    if ((tile + 1) * " << kReduceTile << " <= " << n0 << ") {\n";
-    body << "#pragma unroll\n";
-    body << "        for (int j = 0; j < " << kReduceV << "; ++j) {\n";
-    body << "            const bh_i64 i0 = tile * " << kReduceTile << " + j * " << kThreads << " + threadIdx.x;\n";
-    body << elem.str();
-    body << "        }\n    } else {\n";
-    body << "        for (int j = 0; j < " << kReduceV << "; ++j) {\n";
-    body << "            const bh_i64 i0 = tile * " << kReduceTile << " + j * " << kThreads << " + threadIdx.x;\n";
-    body << "            if (i0 >= " << n0 << ") break;\n";
-    body << elem.str();
-    body << "        }\n    }\n";
     for (size_t k = 0; k < reds.size(); ++k) {
-        body << "    " << accs[k] << " = bh_block_reduce" << k << "(" << accs[k] << ", (" << ctypes[k] << "*)sm_raw);\n";
-        body << "    if (threadIdx.x == 0) part" << k << "[tile] = " << accs[k] << ";\n";
+        body << "    " << ctypes[k] << " " << accs[k] << "[" << K << "];\n";
+        body << "#pragma unroll\n";
+        body << "    for (int k = 0; k < " << K << "; ++k) " << accs[k] << "[k] = " << idents[k] << ";\n";
+    }
+    body << "    const bh_i64 tile0 = w * " << K << ";\n";
+    body << "    const int ktiles = (int)min((bh_i64)" << K << ", p.ntiles - tile0);\n";
+    // Full items (K full tiles) run without bounds checks, after loading the read-only inputs of
+    // all K x 8 elements of the thread; the last item checks every index. Tile k accumulates into
+    // slot k, elements j = 0..7 in order, in both paths.
+    const string n0 = "p.n" + to_string(sym.loop_id.at(&L));
+    const vector<bh_view> pre = preloadable_views(L, L, sym);
+    map<ViewKey, string> acc_k;
+    for (size_t k = 0; k < reds.size(); ++k) acc_k[ViewKey(reds[k]->operand[0])] = accs[k] + "[k]";
+    for (int path = 0; path < 2; ++path) {
+        body << (path == 0 ? "    if ((tile0 + " + to_string(K) + ") * " + to_string(kReduceTile) + " <= " + n0 + ") {\n"
+                           : "    } else {\n");
+        Scope scope;
+        Emitter eb(sym, body, opt);
+        eb.external_acc = acc_k;
+        if (path == 0 && !pre.empty()) {
+            for (size_t v = 0; v < pre.size(); ++v)
+                body << "        " << cuda_type(pre[v].base->dtype()) << " pl" << v << "[" << K * kReduceV << "];\n";
+            body << "#pragma unroll\n";
+            body << "        for (int k = 0; k < " << K << "; ++k) {\n";
+            body << "#pragma unroll\n";
+            body << "            for (int j = 0; j < " << kReduceV << "; ++j) {\n";
+            body << "                const bh_i64 i0 = (tile0 + k) * " << kReduceTile << " + j * " << kThreads
+                 << " + threadIdx.x;\n";
+            for (size_t v = 0; v < pre.size(); ++v)
+                body << "                pl" << v << "[k * " << kReduceV << " + j] = " << eb.array_ref(pre[v]) << ";\n";
+            body << "            }\n";
+            body << "        }\n";
+            for (size_t v = 0; v < pre.size(); ++v)
+                scope.repl[ViewKey(pre[v])] = "pl" + to_string(v) + "[k * " + to_string(kReduceV) + " + j]";
+        }
+        // k always runs to the constant K (unrolled), so the accumulator slots stay registers.
+        body << "#pragma unroll\n";
+        body << "        for (int k = 0; k < " << K << "; ++k) {\n";
+        if (path == 1) body << "            if (k >= ktiles) break;\n";
+        if (path == 0) body << "#pragma unroll\n";
+        body << "            for (int j = 0; j < " << kReduceV << "; ++j) {\n";
+        body << "                const bh_i64 i0 = (tile0 + k) * " << kReduceTile << " + j * " << kThreads
+             << " + threadIdx.x;\n";
+        if (path == 1) body << "                if (i0 >= " << n0 << ") break;\n";
+        eb.write_body(L, scope, 16);
+        body << "            }\n";
+        body << "        }\n";
+    }
+    body << "    }\n";
+    for (size_t k = 0; k < reds.size(); ++k) {
+        body << "    bh_block_reduce_k" << k << "(" << accs[k] << ", (" << ctypes[k] << "*)sm_raw);\n";
+        body << "    if (threadIdx.x == 0) {\n";
+        body << "#pragma unroll\n";
+        body << "        for (int k = 0; k < " << K << "; ++k)\n";
+        body << "            if (k < ktiles) part" << k << "[tile0 + k] = " << accs[k] << "[k];\n";
+        body << "    }\n";
     }
     body << "    if (threadIdx.x == 0) {\n";
-    body << "        __threadfence();\n";
-    body << "        am_last = atomicAdd(p.counter, 1u) == (unsigned)(p.work - 1);\n";
+    body << "        am_last = bh_arrive_n((unsigned*)p.counter, (unsigned)ktiles) + (unsigned)ktiles == (unsigned)p.ntiles;\n";
     body << "    }\n";
     body << "    __syncthreads();\n";
     body << "    if (!am_last) return;\n";
-    body << "    __threadfence();\n";
+    body << "    bh_acquire();\n";
     for (size_t k = 0; k < reds.size(); ++k) {
         const InstrPtr &r = reds[k];
         body << "    {\n";
         body << "        " << ctypes[k] << " acc = " << idents[k] << ";\n";
-        body << "        for (bh_i64 t = threadIdx.x; t < p.work; t += " << kThreads << ") {\n";
+        body << "        for (bh_i64 t = threadIdx.x; t < p.ntiles; t += " << kThreads << ") {\n";
         body << "            const " << ctypes[k] << " x = ((volatile " << ctypes[k] << "*)part" << k << ")[t];\n";
         body << "            acc = " << reduce_expr(r->opcode, "acc", "x") << ";\n";
         body << "        }\n";
@@ -1398,6 +1568,231 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
     u.elements = L.size;
     finish_source(u, pl.decl.str(), body.str(), opt);
     return u;
+}
+
+// ------------------------------------------------------------------------------------- SCAN1D
+// A 1-D innermost loop with one accumulate (cumulative sum/product) among elementwise
+// instructions. Three launch units, in a fixed order that depends on the length only:
+//   A  per chunk of 2048 elements: thread t folds elements 8t..8t+7 of the chunk in order (the
+//      instructions before the accumulate are computed on the fly), a fixed block scan of the 256
+//      thread totals gives the chunk total;
+//   B  one CTA: exclusive scan of the chunk totals (groups of 2048, the same block scan, a running
+//      carry) -> the carry into every chunk;
+//   C  per chunk: the same per-thread fold and block scan; element value = carry op (exclusive
+//      thread prefix op running thread prefix); written out, then the instructions after the
+//      accumulate run on it.
+constexpr int kScanPerThread = 8;
+constexpr int64_t kScanTile = kThreads * kScanPerThread;
+
+bh_opcode scan_reduce_op(bh_opcode acc) { return acc == BH_MULTIPLY_ACCUMULATE ? BH_MULTIPLY_REDUCE : BH_ADD_REDUCE; }
+
+// Deterministic block scan helper: returns the exclusive prefix of `v` over the CTA's threads in
+// thread order and writes the CTA total to `total` (all threads).
+string block_scan_fn(const string &T, const string &fname, bh_opcode op, const string &ident) {
+    stringstream ss;
+    ss << "__device__ __forceinline__ " << T << " " << fname << "(" << T << " v, " << T << " &total, " << T
+       << " *sm) {\n";
+    ss << "    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n";
+    ss << "    " << T << " x = v;\n";
+    ss << "#pragma unroll\n";
+    ss << "    for (int d = 1; d < 32; d <<= 1) {\n";
+    ss << "        " << T << " y = x;\n";
+    ss << "        { long long b; memcpy(&b, &y, sizeof(y) < 8 ? sizeof(y) : 8); b = __shfl_up_sync(0xffffffffu, b, d); "
+          "memcpy(&y, &b, sizeof(y) < 8 ? sizeof(y) : 8); }\n";
+    ss << "        if (lane >= d) x = " << reduce_expr(op, "y", "x") << ";\n";
+    ss << "    }\n";
+    ss << "    " << T << " ex = x;\n";
+    ss << "    { long long b; memcpy(&b, &ex, sizeof(ex) < 8 ? sizeof(ex) : 8); b = __shfl_up_sync(0xffffffffu, b, 1); "
+          "memcpy(&ex, &b, sizeof(ex) < 8 ? sizeof(ex) : 8); }\n";
+    ss << "    if (lane == 0) ex = " << ident << ";\n";
+    ss << "    __syncthreads();\n";
+    ss << "    if (lane == 31) sm[warp] = x;\n";
+    ss << "    __syncthreads();\n";
+    ss << "    if (threadIdx.x == 0) {\n";
+    ss << "        " << T << " run = " << ident << ";\n";
+    ss << "        for (int w = 0; w < " << kThreads / 32 << "; ++w) { const " << T << " t = sm[w]; sm[" << kThreads / 32
+       << " + w] = run; run = " << reduce_expr(op, "run", "t") << "; }\n";
+    ss << "        sm[" << 2 * (kThreads / 32) << "] = run;\n";
+    ss << "    }\n";
+    ss << "    __syncthreads();\n";
+    ss << "    total = sm[" << 2 * (kThreads / 32) << "];\n";
+    ss << "    const " << T << " wo = sm[" << kThreads / 32 << " + warp];\n";
+    ss << "    return " << reduce_expr(op, "wo", "ex") << ";\n";
+    ss << "}\n";
+    return ss.str();
+}
+
+// True when `loop` can be lowered as SCAN1D; `acc` receives the accumulate.
+bool scan1d_applicable(const LoopB &loop, InstrPtr &acc) {
+    if (loop.rank != 0 || !loop.isInnermost() || loop._sweeps.size() != 1) return false;
+    acc = *loop._sweeps.begin();
+    if (acc->opcode != BH_ADD_ACCUMULATE && acc->opcode != BH_MULTIPLY_ACCUMULATE) return false;
+    if (acc->operand[0].ndim != 1 || acc->operand[1].isConstant()) return false;
+    for (const Block &b : loop._block_list) {
+        if (!b.isInstr()) return false;
+        const bh_opcode op = b.getInstr()->opcode;
+        if (b.getInstr() == acc || bh_opcode_is_system(op)) continue;
+        if (bh_opcode_is_sweep(op) || op == BH_GATHER || op == BH_SCATTER || op == BH_COND_SCATTER) return false;
+    }
+    // The accumulate's output is only read by instructions after it, at the same element.
+    bool after = false;
+    for (const Block &b : loop._block_list) {
+        const InstrPtr &i = b.getInstr();
+        if (i == acc) {
+            after = true;
+            continue;
+        }
+        for (size_t o = 1; o < i->operand.size(); ++o) {
+            const bh_view &v = i->operand[o];
+            if (v.isConstant() || v.base != acc->operand[0].base) continue;
+            if (!after || !(v == acc->operand[0])) return false;
+        }
+        if (!i->operand.empty() && !i->operand[0].isConstant() && i->operand[0].base == acc->operand[0].base)
+            return false;
+    }
+    return true;
+}
+
+vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const CodegenOptions &opt) {
+    const Block holder(loop);
+    const LoopB &L = holder.getLoop();
+    const int64_t n = L.size;
+    const int64_t nchunks = (n + kScanTile - 1) / kScanTile;
+    const bh_type t = acc->operand[0].base->dtype();
+    const string T = cuda_type(t);
+    const bh_opcode rop = scan_reduce_op(acc->opcode);
+    const string ident = constant_literal(jitk::sweep_identity(rop, t));
+    vector<LaunchUnit> units;
+    for (int phase = 0; phase < 3; ++phase) {
+        LaunchUnit u;
+        u.sched = Sched::SCAN1D;
+        u.cols = n;
+        u.chunks = phase == 1 ? 1 : nchunks;  // work items
+        Symbols sym = build_symbols({&holder}, {});
+        ParamLayout pl;
+        add_common_fields(sym, pl, opt);
+        pl.add(work_field(nchunks), "bh_i64", "nchunks");
+        pl.add(work_field(phase == 1 ? 1 : nchunks), "bh_i64", "work");
+        ParamField fs{ParamField::SCRATCH};
+        pl.add(fs, "unsigned char*", "scratch");
+        stringstream body;
+        Emitter em(sym, body, opt);
+        body << block_scan_fn(T, "bh_block_scan", rop, ident);
+        body << "__device__ void bh_work(const P &p, bh_i64 c) {\n";
+        body << pointer_locals(sym);
+        body << "    __shared__ " << T << " sm[" << 2 * (kThreads / 32) + 1 << "];\n";
+        body << "    " << T << "* totals = (" << T << "*)p.scratch;\n";
+        body << "    " << T << "* carries = totals + p.nchunks;\n";
+        const string n0 = "p.n" + to_string(sym.loop_id.at(&L));
+        // The accumulate's input at element i0 (computed by the instructions before it).
+        auto emit_inputs = [&](Scope &scope, int ind) {
+            for (const Block &b : L._block_list) {
+                const InstrPtr &i = b.getInstr();
+                if (i == acc) break;
+                if (bh_opcode_is_system(i->opcode)) continue;
+                em.write_instr(*i, scope, ind);
+            }
+        };
+        auto declare_temps = [&](Scope &scope, int ind) {
+            for (const bh_base *b : em.sorted_temps(L)) {
+                if (sym.temps.count(b) && !scope.is_tmp(b)) {
+                    scope.tmps.insert(b);
+                    body << string(static_cast<size_t>(ind), ' ') << cuda_type(b->dtype()) << " t" << sym.base_index(b)
+                         << ";\n";
+                }
+            }
+        };
+        if (phase == 1) {
+            body << "    if (c != 0) return;\n";
+            body << "    " << T << " run = " << ident << ";\n";
+            body << "    for (bh_i64 base = 0; base < p.nchunks; base += " << kScanTile << ") {\n";
+            body << "        " << T << " v[" << kScanPerThread << "];\n";
+            body << "        " << T << " s = " << ident << ";\n";
+            body << "#pragma unroll\n";
+            body << "        for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+            body << "            const bh_i64 j = base + threadIdx.x * " << kScanPerThread << " + k;\n";
+            body << "            v[k] = s;\n";  // exclusive running prefix
+            body << "            if (j < p.nchunks) { const " << T << " x = totals[j]; s = " << reduce_expr(rop, "s", "x")
+                 << "; }\n";
+            body << "        }\n";
+            body << "        " << T << " total;\n";
+            body << "        const " << T << " e = bh_block_scan(s, total, sm);\n";
+            body << "#pragma unroll\n";
+            body << "        for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+            body << "            const bh_i64 j = base + threadIdx.x * " << kScanPerThread << " + k;\n";
+            body << "            const " << T << " inner = " << reduce_expr(rop, "e", "v[k]") << ";\n";
+            body << "            if (j < p.nchunks) carries[j] = " << reduce_expr(rop, "run", "inner") << ";\n";
+            body << "        }\n";
+            body << "        run = " << reduce_expr(rop, "run", "total") << ";\n";
+            body << "        __syncthreads();\n";
+            body << "    }\n";
+            body << "}\n" << kWrappers;
+        } else {
+            // Thread fold over its 8 elements (inputs computed on the fly).
+            body << "    " << T << " s = " << ident << ";\n";
+            body << "    " << T << " xs[" << kScanPerThread << "];\n";
+            {
+                Scope scope;
+                body << "#pragma unroll\n";
+                body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+                body << "        const bh_i64 i0 = c * " << kScanTile << " + threadIdx.x * " << kScanPerThread << " + k;\n";
+                body << "        xs[k] = " << ident << ";\n";
+                body << "        if (i0 < " << n0 << ") {\n";
+                declare_temps(scope, 12);
+                emit_inputs(scope, 12);
+                body << "            xs[k] = " << em.name(acc->operand[1], scope) << ";\n";
+                body << "            s = " << reduce_expr(rop, "s", "xs[k]") << ";\n";
+                body << "        }\n";
+                body << "    }\n";
+            }
+            body << "    " << T << " total;\n";
+            body << "    const " << T << " e = bh_block_scan(s, total, sm);\n";
+            if (phase == 0) {
+                body << "    if (threadIdx.x == 0) totals[c] = total;\n";
+                body << "}\n" << kWrappers;
+            } else {
+                body << "    const " << T << " carry = carries[c];\n";
+                body << "    " << T << " r = " << ident << ";\n";
+                Scope scope;
+                body << "#pragma unroll\n";
+                body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+                body << "        const bh_i64 i0 = c * " << kScanTile << " + threadIdx.x * " << kScanPerThread << " + k;\n";
+                body << "        if (i0 < " << n0 << ") {\n";
+                declare_temps(scope, 12);
+                emit_inputs(scope, 12);  // recomputed: instructions after the accumulate may read them
+                body << "            r = " << reduce_expr(rop, "r", "xs[k]") << ";\n";
+                body << "            const " << T << " inner = " << reduce_expr(rop, "e", "r") << ";\n";
+                body << "            const " << T << " out = " << reduce_expr(rop, "carry", "inner") << ";\n";
+                if (sym.temps.count(acc->operand[0].base)) {
+                    body << "            t" << sym.base_index(acc->operand[0].base) << " = out;\n";
+                } else {
+                    body << "            " << em.array_ref(acc->operand[0]) << " = out;\n";
+                    scope.repl[ViewKey(acc->operand[0])] = "out";
+                }
+                bool after = false;
+                for (const Block &b : L._block_list) {
+                    const InstrPtr &i = b.getInstr();
+                    if (i == acc) {
+                        after = true;
+                        continue;
+                    }
+                    if (after && !bh_opcode_is_system(i->opcode)) em.write_instr(*i, scope, 12);
+                }
+                body << "        }\n";
+                body << "    }\n";
+                body << "}\n" << kWrappers;
+            }
+        }
+        u.fields = pl.fields;
+        u.scratch_bytes_per_tile = 0;
+        u.algorithmic_bytes = phase == 2 ? unit_bytes(sym, vector<const Block *>{&holder}) : 0;
+        u.elements = phase == 1 ? nchunks : n;
+        if (phase == 2) u.red_orders.emplace_back(acc->origin_id, "scan:" + to_string(kScanTile) + ":" + to_string(n));
+        finish_source(u, pl.decl.str(), body.str(), opt);
+        u.scan_chunks = nchunks;
+        units.push_back(std::move(u));
+    }
+    return units;
 }
 
 // OUTER_REDUCE: rank 0 sweeps (reductions) with a single parallel sub-nest and no instructions
@@ -1548,6 +1943,20 @@ vector<LaunchUnit> lower_kernel(const LoopB &kernel, const CodegenOptions &opt) 
                 units.push_back(lower_flat(L, P, opt));
             }
             continue;
+        }
+        InstrPtr scan_acc;
+        if (scan1d_applicable(L, scan_acc) && pending_identities.empty()) {
+            // Identity loops that only seed the accumulate's output are subsumed by the scan.
+            bool ok = true;
+            for (const Block *il : pending_id_loops) {
+                const bh_view &v = jitk::all_instr(*il)[0]->operand[0];
+                ok = ok && v.base == scan_acc->operand[0].base;
+            }
+            if (ok) {
+                pending_id_loops.clear();
+                for (LaunchUnit &su : lower_scan1d(L, scan_acc, opt)) units.push_back(std::move(su));
+                continue;
+            }
         }
         bool all_reduce = !L._sweeps.empty();
         for (const InstrPtr &s : L._sweeps) all_reduce = all_reduce && bh_opcode_is_reduction(s->opcode);

@@ -24,9 +24,9 @@
 //                 combines the lanes; one pass, no scratch.
 //   OUTER_REDUCE  a nest that reduces its outermost axis into an array: threads own the output
 //                 elements (the inner parallel ranks) and loop over the reduced axis.
-//   SCAN1D        a 1-D nest whose outermost axis is an accumulate (cumulative sum/product):
-//                 chunked three-phase scan (chunk totals, serial exclusive scan of the totals,
-//                 re-scan with carry).
+//   SCAN1D        a 1-D nest with one accumulate (cumulative sum/product) among elementwise
+//                 instructions: three units -- chunk totals, one-CTA exclusive scan of the totals,
+//                 re-scan with the carry -- each with a fixed block scan (order set by the length).
 //   SERIAL        anything else: one thread runs the nest in program order (always correct).
 //
 // All loop sizes, view offsets/strides and constants are kernel parameters, so one compiled
@@ -68,7 +68,10 @@ struct LaunchUnit {
     int64_t rows = 1, cols = 1; // FLAT / OUTER_REDUCE index space; GRID_REDUCE/SCAN1D: cols = length
     int nred = 0;               // GRID_REDUCE / SPLIT_REDUCE: number of reductions
     int64_t scratch_bytes_per_tile = 0; // GRID_REDUCE: bytes of partials per tile (all reductions)
-    int64_t chunks = 1;         // SPLIT_REDUCE: chunks of the swept axis; LANE_REDUCE: lanes per point
+    int64_t chunks = 1;         // SPLIT_REDUCE: chunks of the swept axis; LANE_REDUCE: lanes per point;
+                                // GRID_REDUCE: tiles per work item; SCAN1D: work items of the phase
+    int64_t scan_chunks = 0;    // SCAN1D: chunks of 2048 elements
+    int64_t scan_offset = 0;    // SCAN1D: offset of its totals/carries in the scan arena (set by the plan)
     int64_t work_items() const;
     int64_t scratch_bytes() const;   // partials in the scratch arena
     int64_t counters_needed() const; // completion counters

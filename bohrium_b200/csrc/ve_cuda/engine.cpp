@@ -105,7 +105,8 @@ EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
     if (cache_dir == "NONE") cache_dir.clear();
     _device = cfg.defaultGet<int>("device_number", 0);
     learned_on = cfg.defaultGet<bool>("learned", false);
-    learned_runs = cfg.defaultGet<int>("learned_runs", 2);
+    learned_runs = cfg.defaultGet<int>("learned_runs", 3);
+    learned_margin = cfg.defaultGet<double>("learned_margin", 0.03);
     record = cfg.defaultGet<bool>("record", false);
     chooser = [this](const vector<pair<const Block *, const Block *>> &cands) { return choose_merge(cands); };
 
@@ -150,8 +151,10 @@ EngineCUDA::~EngineCUDA() {
         if (scratch) cudaFree(scratch);
         if (counters) cudaFree(counters);
         if (staging_dev) cudaFree(staging_dev);
+        if (scan_arena) cudaFree(scan_arena);
         if (staging_host) cudaFreeHost(staging_host);
         for (void *p : staging_retired) cudaFreeHost(p);
+        for (void *e : busy_events) cudaEventDestroy(static_cast<cudaEvent_t>(e));
         if (staging_event) cudaEventDestroy(static_cast<cudaEvent_t>(staging_event));
         if (err_record) cudaFree(err_record);
         if (rec_e0) cudaEventDestroy(static_cast<cudaEvent_t>(rec_e0));
@@ -180,6 +183,7 @@ void EngineCUDA::copyToDevice(bh_base *base) {
         }
     }
     buffers[base] = b;
+    ++buffer_epoch;
 }
 
 void *EngineCUDA::getBuffer(bh_base *base) {
@@ -199,13 +203,15 @@ void EngineCUDA::delBuffer(bh_base *base) {
         }
     }
     buffers.erase(it);
-    host_stale.erase(base);
+    if (host_stale.erase(base)) ++stale_epoch;
+    ++buffer_epoch;
 }
 
 void EngineCUDA::free_base(bh_base *base) {
     delBuffer(base);
     void *p = base->getDataPtr();
     if (p == nullptr) return;
+    ++buffer_epoch;
     auto it = pinned.find(p);
     if (it != pinned.end()) {
         // Copies from page-locked memory are asynchronous: wait before releasing it.
@@ -277,6 +283,7 @@ void EngineCUDA::copyToHost(const set<bh_base *> &bases, bool evict) {
         auto it = buffers.find(base);
         if (it == buffers.end()) continue;
         if (host_stale.count(base) || base->getDataPtr() == nullptr) {
+            if (base->getDataPtr() == nullptr) ++buffer_epoch;
             bh_data_malloc(base);
             if (it->second.nbytes > 0) {
                 check(cudaMemcpyAsync(base->getDataPtr(), it->second.ptr, static_cast<size_t>(it->second.nbytes),
@@ -285,7 +292,7 @@ void EngineCUDA::copyToHost(const set<bh_base *> &bases, bool evict) {
                 _stats.bytes_d2h += static_cast<uint64_t>(it->second.nbytes);
                 any = true;
             }
-            host_stale.erase(base);
+            if (host_stale.erase(base)) ++stale_epoch;
         }
     }
     if (any) synchronize();
@@ -300,6 +307,7 @@ void EngineCUDA::copyAllBasesToHost() {
 }
 
 void *EngineCUDA::getMemoryPointer(bh_base &base, bool copy2host, bool force_alloc, bool nullify) {
+    ++buffer_epoch;
     if (copy2host) {
         // The caller may write to the host data: the host copy becomes the master copy.
         copyToHost({&base}, true);
@@ -312,6 +320,7 @@ void *EngineCUDA::getMemoryPointer(bh_base &base, bool copy2host, bool force_all
 }
 
 void EngineCUDA::setMemoryPointer(bh_base *base, bool host_ptr, void *mem) {
+    ++buffer_epoch;
     if (host_ptr) {
         delBuffer(base);
         if (base->getDataPtr() != nullptr && base->getDataPtr() != mem) bh_data_free(base);
@@ -334,6 +343,15 @@ void *EngineCUDA::ensure_scratch(int64_t bytes) {
     check(cudaMallocAsync(&scratch, static_cast<size_t>(nb), static_cast<cudaStream_t>(_stream)), "cudaMallocAsync(scratch)");
     scratch_bytes = nb;
     return scratch;
+}
+
+void *EngineCUDA::ensure_scan_arena(int64_t bytes) {
+    if (bytes <= scan_arena_bytes) return scan_arena;
+    const int64_t nb = max<int64_t>(bytes, max<int64_t>(scan_arena_bytes * 2, 1 << 16));
+    if (scan_arena) check(cudaFreeAsync(scan_arena, static_cast<cudaStream_t>(_stream)), "cudaFreeAsync(scan)");
+    check(cudaMallocAsync(&scan_arena, static_cast<size_t>(nb), static_cast<cudaStream_t>(_stream)), "cudaMallocAsync(scan)");
+    scan_arena_bytes = nb;
+    return scan_arena;
 }
 
 unsigned int *EngineCUDA::ensure_counters(int64_t n) {
@@ -508,8 +526,8 @@ EngineCUDA::Compiled *EngineCUDA::compiled_for(const LaunchUnit &u) {
     auto tc = tune_choices.find(h);
     if (tc != tune_choices.end()) {
         c.tuned = true;
-        if (tc->second > 0) {
-            c.variants.push_back(load_variant(cubin_for(u.name, u.source, tc->second), u.name, tc->second));
+        if (tc->second.first > 0 || tc->second.second > 0) {
+            c.variants.push_back(make_variant(c, tc->second.first, tc->second.second));
             c.chosen = 1;
         }
     }
@@ -561,8 +579,9 @@ void EngineCUDA::pack_params(const PlanUnit &pu, const vector<bh_base *> &bases,
                 break;
             }
             case ParamField::SCRATCH: {
-                void *p = f.i64 == -1 ? static_cast<void *>(err_record)
-                                      : static_cast<void *>(static_cast<uint8_t *>(scratch) + scratch_off);
+                void *p = f.i64 == -1              ? static_cast<void *>(err_record)
+                          : u.sched == Sched::SCAN1D ? static_cast<void *>(static_cast<uint8_t *>(scan_arena) + u.scan_offset)
+                                                     : static_cast<void *>(static_cast<uint8_t *>(scratch) + scratch_off);
                 memcpy(slot, &p, 8);
                 break;
             }
@@ -573,6 +592,38 @@ void EngineCUDA::pack_params(const PlanUnit &pu, const vector<bh_base *> &bases,
             }
         }
     }
+}
+
+void EngineCUDA::busy_begin() {
+    if (!busy_timing) return;
+    while (busy_events.size() < busy_used + 2) {
+        cudaEvent_t e;
+        check(cudaEventCreate(&e), "cudaEventCreate");
+        busy_events.push_back(e);
+    }
+    check(cudaEventRecord(static_cast<cudaEvent_t>(busy_events[busy_used]), static_cast<cudaStream_t>(_stream)),
+          "cudaEventRecord");
+}
+
+void EngineCUDA::busy_end() {
+    if (!busy_timing) return;
+    check(cudaEventRecord(static_cast<cudaEvent_t>(busy_events[busy_used + 1]), static_cast<cudaStream_t>(_stream)),
+          "cudaEventRecord");
+    busy_used += 2;
+}
+
+double EngineCUDA::busy_ms() {
+    synchronize();
+    double total = 0;
+    for (size_t i = 0; i + 1 < busy_used; i += 2) {
+        float ms = 0;
+        check(cudaEventElapsedTime(&ms, static_cast<cudaEvent_t>(busy_events[i]),
+                                   static_cast<cudaEvent_t>(busy_events[i + 1])),
+              "cudaEventElapsedTime");
+        total += ms;
+    }
+    busy_used = 0;
+    return total;
 }
 
 void EngineCUDA::record_begin(UnitRecord &r, void *&e0) {
@@ -616,9 +667,11 @@ void EngineCUDA::launch_plain(const PlanUnit &pu, const vector<bh_base *> &bases
     UnitRecord rec{u.name, u.sched, u.elements, u.algorithmic_bytes, 1, 0.f};
     void *e0 = nullptr;
     record_begin(rec, e0);
+    busy_begin();
     api->ck(api->cuLaunchKernel(reinterpret_cast<CUfunction>(pu.compiled->fn), static_cast<unsigned>(grid), 1, 1,
                                 kThreads, 1, 1, 0, static_cast<CUstream>(_stream), args, nullptr),
             "cuLaunchKernel");
+    busy_end();
     record_end(rec, e0);
     ++_stats.launches;
     if (u.sched == Sched::SERIAL) ++_stats.serial_units;
@@ -679,11 +732,19 @@ void EngineCUDA::launch_batched(const vector<const PlanUnit *> &group, const vec
         rec.elements += pu->unit.elements;
         rec.bytes += pu->unit.algorithmic_bytes;
     }
+    if (autotune && !proto.compiled->tuned_batch && rec.elements >= tune_min_elements && !prof && !record &&
+        tune_batch_launch(*proto.compiled, total, args)) {
+        ++_stats.launches;
+        ++_stats.grouped_launches;
+        return;
+    }
     void *e0 = nullptr;
     record_begin(rec, e0);
+    busy_begin();
     api->ck(api->cuLaunchKernel(reinterpret_cast<CUfunction>(proto.compiled->fn_batch), static_cast<unsigned>(grid),
                                 1, 1, kThreads, 1, 1, 0, static_cast<CUstream>(_stream), args, nullptr),
             "cuLaunchKernel(batch)");
+    busy_end();
     record_end(rec, e0);
     ++_stats.launches;
     ++_stats.grouped_launches;
@@ -944,6 +1005,13 @@ EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const
         PlanKernel pk;
         if (!kernel.isSystemOnly()) {
             vector<LaunchUnit> &units = lowered[kidx];
+            int64_t scan_need = 0;
+            for (LaunchUnit &u : units) {
+                if (u.sched != Sched::SCAN1D) continue;
+                u.scan_offset = plan.scan_bytes;
+                scan_need = max<int64_t>(scan_need, (16 * u.scan_chunks + 255) / 256 * 256);
+            }
+            plan.scan_bytes += scan_need;
             for (LaunchUnit &u : units) {
                 PlanUnit pu;
                 pu.compiled = compiled_for(u);
@@ -1007,6 +1075,7 @@ EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const
 }
 
 void EngineCUDA::run_plan(const FlushPlan &plan, const vector<bh_base *> &bases, const vector<bh_instruction *> &instrs) {
+    if (plan.scan_bytes > 0) ensure_scan_arena(plan.scan_bytes);
     if (record) {
         record_kernel_times(plan, bases, instrs);
         return;
@@ -1055,13 +1124,18 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
     // A repeated, unmodified BhIR replays its plan without scanning the instruction list.
     if (bhir->_fingerprint != 0) {
         auto rit = replays.find(bhir->_fingerprint);
-        if (rit != replays.end() && replay_valid(rit->second)) {
+        // A graph replay whose arrays and host copies are untouched since its last launch needs
+        // no checks at all.
+        const bool graph_mode = batch_mode == "graph" && !prof && !record;
+        const bool unchanged = rit != replays.end() && graph_mode && rit->second.graph &&
+                               rit->second.checked_epoch == buffer_epoch;
+        if (rit != replays.end() && (unchanged || replay_valid(rit->second))) {
             Replay &r = rit->second;
             for (bh_base *b : r.dead) free_base(b);
             const auto t1 = chrono::steady_clock::now();
             _stats.time_prepare += chrono::duration<double>(t1 - t0).count();
-            if (batch_mode == "graph" && !prof && !record) {
-                if (r.graph && !graph_usable(*r.graph)) r.graph.reset();
+            if (graph_mode) {
+                if (r.graph && !unchanged && !graph_usable(*r.graph)) r.graph.reset();
                 if (!r.graph && !r.graph_failed && r.valid_runs >= 1 && !build_graph(r)) r.graph_failed = true;
                 ++r.valid_runs;
                 if (r.graph) {
@@ -1071,6 +1145,7 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
                     _stats.time_launch += seconds_since(t1);
                     copyToHost(bhir->_syncs, false);
                     check_error_record();
+                    r.checked_epoch = buffer_epoch;
                     _stats.time_exec_host += seconds_since(t0);
                     return;
                 }

@@ -104,13 +104,13 @@ public:
         // first launches; the fastest becomes fn/fn_batch. Variants compute identical results.
         struct Variant {
             void *fn = nullptr, *fn_batch = nullptr;
-            int occ = 1, occ_batch = 1, maxrreg = 0, regs = 0;
-            std::vector<float> ms;
+            int occ = 1, occ_batch = 1, maxrreg = 0, unroll = 0, regs = 0;
+            std::vector<float> ms, ms_batch;
         };
         std::vector<Variant> variants; // [0]: the default compilation
         std::string name, source;
-        bool tuned = false, tuning = false;
-        int chosen = 0;
+        bool tuned = false, tuning = false, tuned_batch = false;
+        int chosen = 0, chosen_batch = 0; // fn_batch/occ_batch come from variants[chosen_batch]
     };
     // Compiled kernels of a unit (NVRTC on first use, then the in-memory or disk cache).
     Compiled *compiled_for(const LaunchUnit &u);
@@ -126,7 +126,8 @@ public:
     // the faster one is kept for that structure.
     bool learned_on = false;
     bool record = false;           // record (features, device microseconds) of every kernel run
-    int learned_runs = 2;
+    int learned_runs = 3;
+    double learned_margin = 0.03; // the learned plan is kept when at least this much faster
     double learned_min_gain_us = 0.0;
     // Load a model file written by bohrium_b200/costmodel.py (CostModel.save); throws on error.
     void load_costmodel(const std::string &path);
@@ -176,9 +177,12 @@ private:
     std::vector<char> cubin_for(const std::string &name, const std::string &source, int maxrreg);
     // Autotuning of plain launches (tune.cpp)
     bool tune_launch(Compiled &c, const LaunchUnit &u, int64_t work, void **args);
-    std::map<uint64_t, int> tune_choices; // source hash -> chosen register cap (0: default)
+    bool tune_batch_launch(Compiled &c, int64_t total, void **args);
+    void ensure_variants(Compiled &c);
+    std::map<uint64_t, std::pair<int, int>> tune_choices; // source hash -> (register cap, unroll); 0: default
     void load_tune_choices();
-    void save_tune_choice(uint64_t hash, int maxrreg);
+    void save_tune_choice(uint64_t hash, int maxrreg, int unroll);
+    Compiled::Variant make_variant(const Compiled &c, int maxrreg, int unroll);
     // NVRTC-compile the sources of `units` that are not cached yet, in parallel host threads.
     void precompile(const std::vector<const LaunchUnit *> &units);
 
@@ -189,6 +193,10 @@ private:
     unsigned int *counters = nullptr;
     int64_t counter_capacity = 0;
     unsigned long long *err_record = nullptr;
+    // SCAN1D chunk totals and carries: regions assigned per plan, kept across the scan's launches.
+    void *scan_arena = nullptr;
+    int64_t scan_arena_bytes = 0;
+    void *ensure_scan_arena(int64_t bytes);
     void *ensure_scratch(int64_t bytes);
     unsigned int *ensure_counters(int64_t n);
 
@@ -219,6 +227,7 @@ private:
         size_t nbases = 0;
         // Summation order of every floating-point ADD/MULTIPLY sweep, by origin id.
         std::map<int64_t, std::string> orders;
+        int64_t scan_bytes = 0; // scan arena the plan's SCAN1D units need
         std::string signature() const; // kernel names by level (plans with equal signatures match)
     };
     std::unordered_map<uint64_t, FlushPlan> plans;
@@ -233,9 +242,10 @@ private:
         std::vector<void *> parked;             // buffers of arrays the flush creates and frees
         std::vector<std::pair<bh_base *, void *>> persistent; // other arrays and their buffers
         std::vector<bh_base *> written;         // arrays whose host copy a replay makes stale
-        void *scratch = nullptr;
+        void *scratch = nullptr, *scan_arena = nullptr;
         unsigned int *counters = nullptr;
         size_t nlaunches = 0;
+        uint64_t stale_epoch = 0; // host_stale already holds `written` while stale_epoch matches
         ~ReplayGraph();
     };
     struct Replay {
@@ -249,10 +259,14 @@ private:
         std::unique_ptr<ReplayGraph> graph;
         bool graph_failed = false;
         int valid_runs = 0;
+        uint64_t checked_epoch = 0; // buffer_epoch after the last graph replay
     };
+    // Bumped on every change of a device buffer or a host data pointer, and on every removal from
+    // host_stale; a graph replay that sees both unchanged skips its checks.
+    uint64_t buffer_epoch = 1, stale_epoch = 1;
     const std::vector<void *> *ptr_override = nullptr; // per base index: buffer to pack instead
     bool graph_usable(const ReplayGraph &g) const;
-    void graph_launch(const ReplayGraph &g);
+    void graph_launch(ReplayGraph &g);
     bool build_graph(Replay &r);
     int launch_raw(void *fn, int64_t grid, void **args); // cuLaunchKernel on the engine's stream
     std::unordered_map<uint64_t, Replay> replays;
@@ -289,6 +303,14 @@ private:
                         const std::vector<bh_instruction *> &instrs);
     void record_begin(UnitRecord &r, void *&e0);
     void record_end(UnitRecord &r, void *e0);
+    // While set, every launch is bracketed by a pair of events from this pool (device busy time
+    // of a learned-fusion trial in graph mode, where launch gaps disappear in the replay).
+    std::vector<void *> busy_events;
+    size_t busy_used = 0;
+    bool busy_timing = false;
+    void busy_begin();
+    void busy_end();
+    double busy_ms();
 
     // Fuse cache: instruction-list hash -> block list and base order
     struct FusePayload {

@@ -54,7 +54,7 @@ struct GLaunch {
 } // namespace
 
 bool EngineCUDA::graph_usable(const ReplayGraph &g) const {
-    if (g.scratch != scratch || g.counters != counters) return false;
+    if (g.scratch != scratch || g.counters != counters || g.scan_arena != scan_arena) return false;
     for (const auto &bp : g.persistent) {
         auto it = buffers.find(bp.first);
         if (it == buffers.end() || it->second.ptr != bp.second) return false;
@@ -62,9 +62,12 @@ bool EngineCUDA::graph_usable(const ReplayGraph &g) const {
     return true;
 }
 
-void EngineCUDA::graph_launch(const ReplayGraph &g) {
+void EngineCUDA::graph_launch(ReplayGraph &g) {
     check(cudaGraphLaunch(static_cast<cudaGraphExec_t>(g.exec), static_cast<cudaStream_t>(_stream)), "cudaGraphLaunch");
-    for (bh_base *b : g.written) host_stale.insert(b);
+    if (g.stale_epoch != stale_epoch) {
+        for (bh_base *b : g.written) host_stale.insert(b);
+        g.stale_epoch = stale_epoch;
+    }
     _stats.launches += g.nlaunches;
     ++_stats.graph_replays;
 }
@@ -136,6 +139,7 @@ bool EngineCUDA::build_graph(Replay &r) {
     }
     ensure_scratch(scratch_need);
     ensure_counters(counter_need);
+    if (plan.scan_bytes > 0) ensure_scan_arena(plan.scan_bytes);
     ptr_override = &ptr;
     vector<GLaunch> gl;
     size_t dev_bytes = 0;
@@ -183,6 +187,7 @@ bool EngineCUDA::build_graph(Replay &r) {
     ptr_override = nullptr;
     g->scratch = scratch;
     g->counters = counters;
+    g->scan_arena = scan_arena;
     cudaStream_t s = static_cast<cudaStream_t>(_stream);
     if (dev_bytes > 0) {
         check(cudaMalloc(&g->params_dev, dev_bytes), "cudaMalloc(graph params)");

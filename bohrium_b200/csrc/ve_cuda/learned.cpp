@@ -257,19 +257,33 @@ void EngineCUDA::run_trial(uint64_t key, Trial &t, const vector<bh_base *> &base
         rec_e0 = a;
         rec_e1 = b;
     }
-    check_cuda(cudaEventRecord(static_cast<cudaEvent_t>(rec_e0), s), "cudaEventRecord");
-    run_plan(plan, bases, instrs);
-    check_cuda(cudaEventRecord(static_cast<cudaEvent_t>(rec_e1), s), "cudaEventRecord");
-    check_cuda(cudaEventSynchronize(static_cast<cudaEvent_t>(rec_e1)), "cudaEventSynchronize");
     float ms = 0.f;
-    check_cuda(cudaEventElapsedTime(&ms, static_cast<cudaEvent_t>(rec_e0), static_cast<cudaEvent_t>(rec_e1)),
-               "cudaEventElapsedTime");
+    // The autotuner's variant rotation would distort the comparison: trials use the variants in
+    // place, and tuning resumes once the plan is chosen.
+    const bool tune = autotune;
+    autotune = false;
+    if (batch_mode == "graph") {
+        // Replays will run as a CUDA graph without launch gaps: compare device busy time.
+        busy_timing = true;
+        busy_used = 0;
+        run_plan(plan, bases, instrs);
+        busy_timing = false;
+        ms = static_cast<float>(busy_ms());
+    } else {
+        check_cuda(cudaEventRecord(static_cast<cudaEvent_t>(rec_e0), s), "cudaEventRecord");
+        run_plan(plan, bases, instrs);
+        check_cuda(cudaEventRecord(static_cast<cudaEvent_t>(rec_e1), s), "cudaEventRecord");
+        check_cuda(cudaEventSynchronize(static_cast<cudaEvent_t>(rec_e1)), "cudaEventSynchronize");
+        check_cuda(cudaEventElapsedTime(&ms, static_cast<cudaEvent_t>(rec_e0), static_cast<cudaEvent_t>(rec_e1)),
+                   "cudaEventElapsedTime");
+    }
+    autotune = tune;
     (use_learned ? t.t_learned : t.t_greedy).push_back(ms);
     const size_t runs = static_cast<size_t>(max(learned_runs, 1));
     if (t.t_greedy.size() >= runs && t.t_learned.size() >= runs) {
         const double g = *min_element(t.t_greedy.begin(), t.t_greedy.end());
         const double l = *min_element(t.t_learned.begin(), t.t_learned.end());
-        if (l < g) {
+        if (l < g * (1.0 - learned_margin)) {
             ++_stats.learned_kept;
             plans[key] = std::move(t.learned);
         } else {

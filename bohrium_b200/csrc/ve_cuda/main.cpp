@@ -98,6 +98,8 @@ public:
             engine.set_fusion("", msg.substr(12));
         } else if (msg.rfind("CUDA: pre_fuser ", 0) == 0) {
             engine.set_fusion(msg.substr(16), "");
+        } else if (msg.rfind("CUDA: autotune ", 0) == 0) {
+            engine.autotune = msg.substr(15) == "on";
         } else if (msg.rfind("CUDA: learned ", 0) == 0) {
             engine.learned_on = msg.substr(14) == "on";
         }

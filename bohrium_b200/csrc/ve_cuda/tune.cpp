@@ -1,12 +1,14 @@
-// Autotuning of launch shapes: register caps.
+// Autotuning of launch shapes: register caps and inner-loop unrolling.
 //
-// A kernel with large work (at least `tune_min_elements` elements) is compiled a few more times
+// A kernel with large work (at least `tune_min_elements` elements) is compiled a few more times:
 // with NVRTC's --maxrregcount below its natural register count (more resident CTAs per SM,
-// possibly at the cost of spills), and its first plain launches rotate through the variants,
-// each timed alone with CUDA events. After two timings of every variant the fastest one is kept
-// for that source, and the choice is written to the kernel cache directory (tune.txt) so that
-// later processes start with it. All variants come from the same source and the same options
-// but the register cap (FMA contraction off), so they compute bit-identical results.
+// possibly at the cost of spills) and, where the source marks its element loop, with that loop
+// unrolled 2 or 4 times (more loads in flight per thread). Its first plain launches rotate through
+// the variants, each timed alone with CUDA events. After three timings of every variant the fastest
+// one is kept for that source, and the choice is written to the kernel cache directory
+// (tune.txt) so that later processes start with it. Register caps and unrolling change neither
+// the operations nor their order on any value (FMA contraction is off), so every variant
+// computes bit-identical results.
 #include <algorithm>
 #include <cstdio>
 #include <fstream>
@@ -35,35 +37,113 @@ uint64_t source_hash(const string &s) {
 }
 } // namespace
 
+const char kUnrollMarker[] = "/*@unroll@*/";
+constexpr size_t kTuneSamples = 3;  // timed launches per variant (the fastest counts)
+
 void EngineCUDA::load_tune_choices() {
     if (cache_dir.empty()) return;
     ifstream in(cache_dir + "/tune.txt");
     string hex_hash;
-    int cap = 0;
-    while (in >> hex_hash >> cap) tune_choices[stoull(hex_hash, nullptr, 16)] = cap;
+    int cap = 0, unroll = 0;
+    while (in >> hex_hash >> cap >> unroll) tune_choices[stoull(hex_hash, nullptr, 16)] = {cap, unroll};
 }
 
-void EngineCUDA::save_tune_choice(uint64_t hash, int maxrreg) {
-    tune_choices[hash] = maxrreg;
+void EngineCUDA::save_tune_choice(uint64_t hash, int maxrreg, int unroll) {
+    tune_choices[hash] = {maxrreg, unroll};
     if (cache_dir.empty()) return;
     ofstream out(cache_dir + "/tune.txt", ios::app);
-    out << hex << hash << " " << dec << maxrreg << "\n";
+    out << hex << hash << " " << dec << maxrreg << " " << unroll << "\n";
+}
+
+EngineCUDA::Compiled::Variant EngineCUDA::make_variant(const Compiled &c, int maxrreg, int unroll) {
+    string src = c.source;
+    if (unroll > 0) {
+        const string pragma = "#pragma unroll " + to_string(unroll);
+        for (size_t pos = src.find(kUnrollMarker); pos != string::npos; pos = src.find(kUnrollMarker, pos))
+            src.replace(pos, sizeof(kUnrollMarker) - 1, pragma);
+    }
+    Compiled::Variant v = load_variant(cubin_for(c.name, src, maxrreg), c.name, maxrreg);
+    v.unroll = unroll;
+    return v;
+}
+
+void EngineCUDA::ensure_variants(Compiled &c) {
+    if (!c.tuning) {
+        c.tuning = true;
+        const int regs = c.variants[0].regs;
+        vector<int> caps;
+        for (int cap : {128, 96, 80, 64, 48, 40, 32})
+            if (cap < regs && caps.size() < 2) caps.push_back(cap);
+        for (int cap : caps) c.variants.push_back(make_variant(c, cap, 0));
+        if (c.source.find(kUnrollMarker) != string::npos) {
+            for (int unroll : {2, 4}) c.variants.push_back(make_variant(c, 0, unroll));
+            if (!caps.empty()) c.variants.push_back(make_variant(c, caps.back(), 4));
+        }
+    }
+}
+
+namespace {
+// Time one launch of `fn` alone on `stream` (milliseconds).
+float time_launch(EngineCUDA &e, void *&e0, void *&e1, void *stream, void *fn, int64_t grid, void **args,
+                  int (EngineCUDA::*launch)(void *, int64_t, void **)) {
+    if (e0 == nullptr) {
+        cudaEvent_t a, b;
+        check_rt(cudaEventCreate(&a), "cudaEventCreate");
+        check_rt(cudaEventCreate(&b), "cudaEventCreate");
+        e0 = a;
+        e1 = b;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    check_rt(cudaEventRecord(static_cast<cudaEvent_t>(e0), s), "cudaEventRecord");
+    if ((e.*launch)(fn, grid, args) != 0) throw runtime_error("cuLaunchKernel failed while tuning");
+    check_rt(cudaEventRecord(static_cast<cudaEvent_t>(e1), s), "cudaEventRecord");
+    check_rt(cudaEventSynchronize(static_cast<cudaEvent_t>(e1)), "cudaEventSynchronize");
+    float ms = 0.f;
+    check_rt(cudaEventElapsedTime(&ms, static_cast<cudaEvent_t>(e0), static_cast<cudaEvent_t>(e1)), "cudaEventElapsedTime");
+    return ms;
+}
+} // namespace
+
+bool EngineCUDA::tune_batch_launch(Compiled &c, int64_t total, void **args) {
+    ensure_variants(c);
+    if (c.variants.size() == 1) {
+        c.tuned_batch = true;
+        return false;
+    }
+    size_t k = 0;
+    for (size_t i = 1; i < c.variants.size(); ++i)
+        if (c.variants[i].ms_batch.size() < c.variants[k].ms_batch.size()) k = i;
+    Compiled::Variant &v = c.variants[k];
+    const int64_t grid = max<int64_t>(1, min<int64_t>(total, static_cast<int64_t>(_sm_count) * v.occ_batch));
+    v.ms_batch.push_back(time_launch(*this, rec_e0, rec_e1, _stream, v.fn_batch, grid, args, &EngineCUDA::launch_raw));
+    ++_stats.tune_launches;
+    bool done = true;
+    for (const Compiled::Variant &x : c.variants) done = done && x.ms_batch.size() >= kTuneSamples;
+    if (done) {
+        size_t best = 0;
+        float best_ms = *min_element(c.variants[0].ms_batch.begin(), c.variants[0].ms_batch.end());
+        for (size_t i = 1; i < c.variants.size(); ++i) {
+            const float m = *min_element(c.variants[i].ms_batch.begin(), c.variants[i].ms_batch.end());
+            if (m < best_ms * 0.98f) {
+                best = i;
+                best_ms = m;
+            }
+        }
+        c.chosen_batch = static_cast<int>(best);
+        c.fn_batch = c.variants[best].fn_batch;
+        c.occ_batch = c.variants[best].occ_batch;
+        c.tuned_batch = true;
+    }
+    return true;
 }
 
 bool EngineCUDA::tune_launch(Compiled &c, const LaunchUnit &u, int64_t work, void **args) {
     const uint64_t h = source_hash(c.source);
-    if (!c.tuning) {
-        c.tuning = true;
-        const int regs = c.variants[0].regs;
-        for (int cap : {128, 96, 80, 64, 48, 40, 32}) {
-            if (cap >= regs || c.variants.size() >= 4) continue;
-            c.variants.push_back(load_variant(cubin_for(c.name, c.source, cap), c.name, cap));
-        }
-        if (c.variants.size() == 1) {
-            c.tuned = true;
-            save_tune_choice(h, 0);
-            return false;
-        }
+    ensure_variants(c);
+    if (c.variants.size() == 1) {
+        c.tuned = true;
+        save_tune_choice(h, 0, 0);
+        return false;
     }
     // The variant with the fewest timings runs next.
     size_t k = 0;
@@ -89,7 +169,7 @@ bool EngineCUDA::tune_launch(Compiled &c, const LaunchUnit &u, int64_t work, voi
     v.ms.push_back(ms);
     ++_stats.tune_launches;
     bool done = true;
-    for (const Compiled::Variant &x : c.variants) done = done && x.ms.size() >= 2;
+    for (const Compiled::Variant &x : c.variants) done = done && x.ms.size() >= kTuneSamples;
     if (done) {
         size_t best = 0;
         float best_ms = *min_element(c.variants[0].ms.begin(), c.variants[0].ms.end());
@@ -103,13 +183,15 @@ bool EngineCUDA::tune_launch(Compiled &c, const LaunchUnit &u, int64_t work, voi
         c.chosen = static_cast<int>(best);
         const Compiled::Variant &b = c.variants[best];
         c.fn = b.fn;
-        c.fn_batch = b.fn_batch;
         c.occ = b.occ;
-        c.occ_batch = b.occ_batch;
+        if (!c.tuned_batch) {
+            c.fn_batch = b.fn_batch;
+            c.occ_batch = b.occ_batch;
+        }
         c.tuned = true;
         ++_stats.tuned_kernels;
-        if (b.maxrreg > 0) ++_stats.tuned_capped;
-        save_tune_choice(h, b.maxrreg);
+        if (b.maxrreg > 0 || b.unroll > 0) ++_stats.tuned_capped;
+        save_tune_choice(h, b.maxrreg, b.unroll);
     }
     return true;
 }

@@ -26,7 +26,7 @@ from .costmodel import CostModel, read_records
 from .workloads import random_dag
 
 GREEDY = "greedy,push_reductions_inwards,collapse_redundant_axes"
-WARMUP = 6  # executions before timing: plan building, the learned trials, replay set-up
+WARMUP = 9  # executions before timing: plan building, the learned trials (3 + 3), graph capture
 # Plans used to collect training timings: the greedy plan, no DAG fusion (pre-fuser groups
 # only), no fusion at all, and two other contraction orders.
 VARIANTS = [
@@ -65,6 +65,7 @@ def _set_fusion(ex, pre: str, fusers: str):
 def collect(ex, seeds, max_elems: float = 2e7, variants=VARIANTS):
     """Per-kernel (features, microseconds) rows of every DAG under every plan variant."""
     ex.message("CUDA: records clear")
+    ex.message("CUDA: autotune off")  # no variant compilation while collecting
     for seed in seeds:
         rt, dag, outs, _ = build(ex, seed, max_elems)
         for pre, fusers in variants:
@@ -75,6 +76,7 @@ def collect(ex, seeds, max_elems: float = 2e7, variants=VARIANTS):
             ex.message("CUDA: record off")
         del dag, outs, rt
     _set_fusion(ex, "lossy", GREEDY)
+    ex.message("CUDA: autotune on")
     fd, path = tempfile.mkstemp(suffix=".rec")
     os.close(fd)
     try:
@@ -99,34 +101,54 @@ def _timed(ex, dag, reps: int) -> float:
 
 
 def evaluate(ex, seeds, model_path: str, max_elems: float = 1e8, reps: int = 5):
-    """Device ms per flush, greedy vs learned, for every DAG; outputs compared bit for bit."""
+    """Device ms per flush of every DAG under three engines -- plain (greedy plan, one launch per
+    kernel), batched (greedy plan replayed as a CUDA graph of grouped launches) and batched +
+    learned (the learned plan where it is bit-identical and measured faster) -- with the outputs
+    of all three compared bit for bit."""
     rows = []
     for seed in seeds:
         rt, dag, outs, shape = build(ex, seed, max_elems)
-        _set_fusion(ex, "lossy", GREEDY)
-        ex.message("CUDA: learned off")
-        for _ in range(WARMUP):  # the same warm-up as the learned engine gets below
-            dag.execute()
-        greedy_ms = _timed(ex, dag, reps)
-        want = [ex.peek(o.base) for o in outs]
-        _set_fusion(ex, "lossy", GREEDY)  # forget plans
-        ex.message(f"CUDA: costmodel load {model_path}")
-        ex.message("CUDA: learned on")
+        times, results = {}, {}
         stats0 = _stats(ex)
-        for _ in range(WARMUP):  # trials: greedy and learned plans timed, the faster kept
-            dag.execute()
-        learned_ms = _timed(ex, dag, reps)
-        got = [ex.peek(o.base) for o in outs]
+        for name, batch, learned in (("plain", "off", False), ("batched", "graph", False),
+                                     ("batched_learned", "graph", True)):
+            _set_fusion(ex, "lossy", GREEDY)  # forget plans, replays and graphs
+            ex.message(f"CUDA: batch {batch}")
+            if learned:
+                ex.message(f"CUDA: costmodel load {model_path}")
+            ex.message("CUDA: learned " + ("on" if learned else "off"))
+            for _ in range(WARMUP):  # plan building, learned trials, graph capture
+                dag.execute()
+            times[name] = _timed(ex, dag, reps)
+            results[name] = [ex.peek(o.base).tobytes() for o in outs]
         stats1 = _stats(ex)
         ex.message("CUDA: learned off")
-        same = all(a.dtype == b.dtype and a.tobytes() == b.tobytes() for a, b in zip(want, got))
+        ex.message("CUDA: batch off")
         rows.append({"seed": seed, "ops": shape[0], "elements": shape[1], "dtype": shape[2], "reductions": shape[3],
-                     "greedy_ms": greedy_ms, "learned_ms": learned_ms, "identical": same,
+                     "plain_ms": times["plain"], "batched_ms": times["batched"],
+                     "learned_ms": times["batched_learned"],
+                     "identical": results["plain"] == results["batched"] == results["batched_learned"],
                      "learned_kept": stats1.get("learned_kept", 0) - stats0.get("learned_kept", 0),
                      "tried": stats1.get("learned_trials", 0) - stats0.get("learned_trials", 0)})
         del dag, outs, rt
     _set_fusion(ex, "lossy", GREEDY)
     return rows
+
+
+def summary(rows) -> dict:
+    """Geometric-mean speed-ups over the DAGs and the total flush times."""
+    p = np.array([r["plain_ms"] for r in rows])
+    b = np.array([r["batched_ms"] for r in rows])
+    l = np.array([r["learned_ms"] for r in rows])
+    g = lambda x: float(np.exp(np.mean(np.log(x))))
+    return {"dags": len(rows), "geomean_speedup_batched_learned_vs_plain": round(g(p / l), 3),
+            "geomean_speedup_batched_vs_plain": round(g(p / b), 3),
+            "geomean_speedup_learned_vs_batched": round(g(b / l), 3),
+            "total_ms": {"plain": round(float(p.sum()), 3), "batched": round(float(b.sum()), 3),
+                         "batched_learned": round(float(l.sum()), 3)},
+            "learned_plans_kept": int(sum(r["learned_kept"] for r in rows)),
+            "learned_plans_tried": int(sum(r["tried"] for r in rows)),
+            "bit_identical": all(r["identical"] for r in rows)}
 
 
 def _stats(ex) -> dict:

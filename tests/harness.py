@@ -43,3 +43,41 @@ def compare(a_results, b_results, tol=None, what=""):
         else:
             rtol, atol = tol
         assert_close(x, y, rtol, atol, f"{what}[{k}]")
+
+
+def grid_reduce_sum(x: np.ndarray) -> np.ndarray:
+    """Exact model of the summation order of the engine's GRID_REDUCE schedule for an ADD_REDUCE
+    of a contiguous 1-D array: tiles of 256 threads x 8 elements (thread t adds elements
+    t, t+256, ..., t+1792 of its tile in order, starting from 0), a halving tree over the 32 lanes
+    of each warp and over the 8 warp sums (padded with 0), then the same per-thread fold and trees
+    over the tile partials (thread t adds partials t, t+256, ...). Vectorised NumPy in the array's
+    own dtype, so the result is bit-exact."""
+    dt = x.dtype
+    zero = dt.type(0)
+    n = x.size
+    ntiles = -(-n // 2048)
+    pad = np.zeros(ntiles * 2048, dtype=dt)
+    pad[:n] = x
+    t = pad.reshape(ntiles, 8, 256)
+    acc = np.full((ntiles, 256), zero, dtype=dt)
+    for j in range(8):
+        acc = acc + t[:, j, :]
+
+    def cta_tree(a):  # a: (rows, 256) -> (rows,)
+        w = a.reshape(a.shape[0], 8, 32)
+        for m in (16, 8, 4, 2, 1):
+            w = w[:, :, :m] + w[:, :, m:2 * m]
+        ws = np.full((a.shape[0], 32), zero, dtype=dt)
+        ws[:, :8] = w[:, :, 0]
+        for m in (16, 8, 4, 2, 1):
+            ws = ws[:, :m] + ws[:, m:2 * m]
+        return ws[:, 0]
+
+    parts = cta_tree(acc)
+    fold = np.full(256, zero, dtype=dt)
+    for start in range(0, ntiles, 256):
+        chunk = np.full(256, zero, dtype=dt)
+        c = parts[start:start + 256]
+        chunk[:c.size] = c
+        fold = np.where(np.arange(256) < c.size, fold + chunk, fold)
+    return cta_tree(fold[None, :])[0]

@@ -130,3 +130,11 @@ def test_row_reductions_of_contiguous_rows_use_lanes():
         return [x.sum(axis=0)]
     res, units = plan(prog_cols)
     assert "lane_reduce" not in [u["sched"] for u in units]
+
+
+def test_one_dimensional_accumulate_lowers_to_three_scan_units():
+    def prog(rt):
+        a = bh.empty(rt, (100000,), np.float64)
+        return [bh.accumulate("ADD_ACCUMULATE", a * 2.0 + 1.0, 0) * 3.0]
+    res, units = plan(prog)
+    assert [u["sched"] for u in units] == ["scan1d", "scan1d", "scan1d"], [u["sched"] for u in units]

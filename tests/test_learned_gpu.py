@@ -21,7 +21,8 @@ def test_records_train_and_bit_identical_learned_plans(gpu_executor, tmp_path):
     assert len(rows) == 4
     for r in rows:
         assert r["identical"], r
-        assert r["greedy_ms"] > 0 and r["learned_ms"] > 0
+        assert r["plain_ms"] > 0 and r["batched_ms"] > 0 and r["learned_ms"] > 0
+    assert learn.summary(rows)["bit_identical"]
 
 
 def test_learned_mode_without_a_model_is_the_greedy_engine(gpu_executor):

@@ -333,3 +333,39 @@ def test_autotuned_variants_are_bit_identical(gpu_executor):
     want = W.black_scholes_numpy(S, K, T, 1)
     got = float(np.frombuffer(seen.pop(), dtype=np.float64)[0])
     assert abs(got - want) <= 1e-11 * abs(want)  # NumPy's exp/log differ from CUDA's by ulps
+
+
+@pytest.mark.parametrize("n,dtype", [(1_000_003, np.float32), (16_000_000, np.float64), (45_000_001, np.float32)])
+def test_grid_reduce_order_is_canonical(gpu_rt, n, dtype):
+    """GRID_REDUCE sums in one fixed order whatever the number of tiles a work item takes (1, 2 or
+    4 at these sizes): the GPU result equals the exact order model bit for bit."""
+    from tests.harness import grid_reduce_sum
+    x = np.random.default_rng(n).standard_normal(n).astype(dtype)
+    got = bh.array(gpu_rt, x).sum().numpy()
+    want = grid_reduce_sum(x)
+    assert np.asarray(got).tobytes() == np.asarray(want).tobytes(), (got, want)
+
+
+@pytest.mark.parametrize("n,dtype,name", [(1_000_003, np.float64, "ADD_ACCUMULATE"), (4_000_000, np.int64, "ADD_ACCUMULATE"),
+                                          (2049, np.float32, "ADD_ACCUMULATE"), (300_001, np.float64, "MULTIPLY_ACCUMULATE"),
+                                          (5_000_000, np.int32, "ADD_ACCUMULATE")])
+def test_scan1d(gpu_rt, oracle_rt, n, dtype, name):
+    """1-D cumulative sums/products with the instructions around them fused (SCAN1D: chunk totals,
+    carries, re-scan), against the oracle's sequential scan."""
+    rng = np.random.default_rng(n)
+    if name == "MULTIPLY_ACCUMULATE":
+        host = (1.0 + (rng.random(n) - 0.5) * 1e-5).astype(dtype)
+    elif np.dtype(dtype).kind == "i":
+        host = rng.integers(-50, 50, n).astype(dtype)
+    else:
+        host = rng.random(n).astype(dtype)
+
+    def prog(rt):
+        x = bh.array(rt, host)
+        c = bh.accumulate(name, x * dtype(1) + dtype(0), 0)
+        return [c, c * dtype(2)]
+
+    g, o = both(gpu_rt, oracle_rt, prog)
+    tol = 0 if np.dtype(dtype).kind == "i" else (1e-4 if np.dtype(dtype) == np.float32 else 1e-11)
+    for a, b, what in zip(g, o, ["scan", "after"]):
+        assert_close(a, b, tol, tol, what)
