@@ -9,10 +9,10 @@ from . import ir
 from .runtime import NativeExecutor, Runtime, load_library
 from .array import (BhArray, empty, full, zeros, ones, array, arange, random123, random_sample, binary, unary,
                     reduce, accumulate, gather, scatter, sqrt, exp, log, sin, cos, tanh, absolute, floor, sign,
-                    maximum, minimum, where, true_divide)
+                    maximum, minimum, where, true_divide, matmul, extmethod_opcode)
 from .inspect import DryRunExecutor, dry_run
 
 __all__ = ["ir", "NativeExecutor", "Runtime", "load_library", "BhArray", "empty", "full", "zeros", "ones", "array",
            "arange", "random123", "random_sample", "binary", "unary", "reduce", "accumulate", "gather", "scatter",
            "sqrt", "exp", "log", "sin", "cos", "tanh", "absolute", "floor", "sign", "maximum", "minimum", "where",
-           "true_divide", "DryRunExecutor", "dry_run"]
+           "true_divide", "matmul", "extmethod_opcode", "DryRunExecutor", "dry_run"]

@@ -360,8 +360,12 @@ def reduce(name: str, a: BhArray, axis=None) -> BhArray:
         out = empty(a.rt, shape, a.dtype)
         a.rt.enqueue(ir.Instr(OP[name], [out.view(), a.view(), None], ir.Constant(ax, ir.INT64)))
         return out
-    # Largest stride first (column-major order, as the reference bridge does for GPU stacks).
-    order = sorted(axes, key=lambda i: abs(a.strides[i]), reverse=True)
+    # Largest stride first (column-major order, as the reference bridge does for GPU stacks) where
+    # the order can change the result (floating-point sums and products); reductions whose result
+    # does not depend on the order (max, min, logical and bitwise ones, integer sums and
+    # products) go smallest stride first, so the first one sweeps the contiguous axis.
+    order_free = name not in ("ADD_REDUCE", "MULTIPLY_REDUCE") or a.dtype.kind in "biu"
+    order = sorted(axes, key=lambda i: abs(a.strides[i]), reverse=not order_free)
     first = order[0]
     tmp = reduce(name, a, first)
     rest = [i if i < first else i - 1 for i in order[1:]]
@@ -418,3 +422,30 @@ def where(cond: BhArray, a, b):
     """a if cond else b, written with arithmetic on the 0/1 mask (no select opcode exists)."""
     m = cond.astype(_result_type(a, b))
     return m * a + (1 - m) * b
+
+
+# ------------------------------------------------------------------------------ extension methods
+_EXT_BASE = ir.MAX_OPCODE_ID + 1
+
+
+def extmethod_opcode(rt: Runtime, name: str) -> int:
+    """The opcode of extension method `name`, registered with the runtime's stack on first use
+    (bhc_extmethod of the reference's C bridge). The table lives with the executor (the stack),
+    which keeps its registrations for its whole life."""
+    table = rt.ex.__dict__.setdefault("_extmethods", {})
+    if name not in table:
+        opcode = _EXT_BASE + len(table)
+        rt.ex.extmethod(name, opcode)
+        table[name] = opcode
+    return table[name]
+
+
+def matmul(a: BhArray, b: BhArray, trans_a: bool = False) -> BhArray:
+    """C = A @ B (or A^T @ B) of contiguous 2-D float32/float64 arrays through the stack's BLAS
+    extension methods `blas_gemm` / `blas_gemmt` (operands C, A, B as in the reference's
+    extmethods/blas)."""
+    m = a.shape[1] if trans_a else a.shape[0]
+    out = empty(a.rt, (m, b.shape[1]), a.dtype)
+    op = extmethod_opcode(a.rt, "blas_gemmt" if trans_a else "blas_gemm")
+    a.rt.enqueue(ir.Instr(op, [out.view(), a.view(), b.view()]))
+    return out

@@ -8,6 +8,8 @@ Produces (under bohrium_b200/lib/):
   libbh_ve_cuda.so  the `cuda` vector engine component (NVRTC code generation for sm_100a plus
                     the hand-written sm_100a kernels compiled here with nvcc)
   libbh_vem_node.so the pass-through `node` component
+  libbh_filter_bcexp.so, libbh_filter_bccon.so the bytecode filter components
+  libbh_ext_cublas.so BLAS extension methods (blas_gemm, blas_gemmt) on cuBLAS for the cuda engine
 
 C++ sources are compiled with g++ (-std=c++17 -O2 -fPIC); .cu sources with
 nvcc -gencode arch=compute_100a,code=sm_100a. Objects are rebuilt when a source or any header
@@ -102,10 +104,21 @@ def build(verbose: bool = False) -> dict:
     _link(ve, cuda_objs, ["-lbh_core", "-L" + cuda_lib, "-lcudart_static", "-lnvrtc", "-ldl", "-lpthread", "-lrt"],
           verbose)
 
+    ext_objs = [_compile(s, verbose) for s in sources("ext_cublas")]
+    ext = os.path.join(LIB, "libbh_ext_cublas.so")
+    _link(ext, ext_objs, ["-lbh_core", "-L" + cuda_lib, "-lcublas", "-lcudart_static", "-ldl", "-lpthread", "-lrt"],
+          verbose)
+
+    filters = {}
+    for name in ("bcexp", "bccon"):
+        obj = _compile(os.path.join(CSRC, "filter", name + ".cpp"), verbose)
+        filters[name] = os.path.join(LIB, "libbh_filter_" + name + ".so")
+        _link(filters[name], [obj], ["-lbh_core"], verbose)
+
     node_objs = [_compile(s, verbose) for s in sources("vem_node")]
     node = os.path.join(LIB, "libbh_vem_node.so")
     _link(node, node_objs, ["-lbh_core"], verbose)
-    return {"core": core, "ve_cuda": ve, "vem_node": node, "seconds": time.time() - t0}
+    return {"core": core, "ve_cuda": ve, "vem_node": node, "ext_cublas": ext, **filters, "seconds": time.time() - t0}
 
 
 if __name__ == "__main__":

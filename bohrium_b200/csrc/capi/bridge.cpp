@@ -8,6 +8,9 @@
 #include <bh_b200.h>
 #include <bohrium/bh_component.hpp>
 #include <bohrium/bh_main_memory.hpp>
+#include <map>
+#include <sstream>
+#include "../core/filters.hpp"
 
 using namespace std;
 using namespace bohrium;
@@ -38,6 +41,8 @@ struct bhb_runtime {
 
 struct bhb_ir {
     unique_ptr<BhIR> ir;
+    bohrium::filter::BaseStore created;  // temporaries made by bhb_ir_filter
+    string text;                          // last bhb_ir_text result
 };
 
 namespace {
@@ -270,3 +275,55 @@ extern "C" void bhb_set_last_error(const char *msg) { g_last_error = msg ? msg :
 
 // Host data pointer of a base (valid after a sync; NULL when the base has no host storage).
 extern "C" void *bhb_base_data(const bh_base *base) { return const_cast<void *>(base->getDataPtr()); }
+
+// Apply a bytecode filter to a decoded BhIR in place (test hook of the filter components):
+// "bcexp" (powk), "bcexp+sign" (powk and sign), "bccon" (stupidmath, collect, muladd). Returns
+// the number of rewrites, or -1 on error.
+extern "C" int bhb_ir_filter(bhb_ir *ir, const char *name) {
+    int n = -1;
+    guarded([&] {
+        const string f = name ? name : "";
+        if (f == "bcexp" || f == "bcexp+sign") {
+            bohrium::filter::ExpandOptions o;
+            o.sign = f == "bcexp+sign";
+            n = bohrium::filter::expand(*ir->ir, o, ir->created);
+        } else if (f == "bccon") {
+            n = bohrium::filter::contract(*ir->ir, bohrium::filter::ContractOptions());
+        } else {
+            throw runtime_error("bhb_ir_filter: unknown filter " + f);
+        }
+    });
+    return n;
+}
+
+// A text listing of a decoded BhIR, one instruction per line: the opcode number, then each
+// operand as `c` (the constant) or `b<k>[start;shape;stride]` with bases numbered by first
+// appearance, then the constant's value for instructions that have one.
+extern "C" const char *bhb_ir_text(bhb_ir *ir) {
+    const char *ret = nullptr;
+    guarded([&] {
+        stringstream ss;
+        std::map<const bh_base *, int> ids;
+        for (const bh_instruction &in : ir->ir->instr_list) {
+            if (in.opcode == BH_NONE) continue;
+            ss << in.opcode;
+            for (const bh_view &v : in.operand) {
+                if (v.isConstant()) {
+                    ss << " c";
+                    continue;
+                }
+                auto it = ids.emplace(v.base, static_cast<int>(ids.size())).first;
+                ss << " b" << it->second << "[" << v.start << ";";
+                for (int64_t d = 0; d < v.ndim; ++d) ss << (d ? "," : "") << v.shape[d];
+                ss << ";";
+                for (int64_t d = 0; d < v.ndim; ++d) ss << (d ? "," : "") << v.stride[d];
+                ss << "]";
+            }
+            if (in.has_constant()) ss << " = " << in.constant.get_double();
+            ss << "\n";
+        }
+        ir->text = ss.str();
+        ret = ir->text.c_str();
+    });
+    return ret;
+}

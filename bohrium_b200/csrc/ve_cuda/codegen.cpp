@@ -495,19 +495,27 @@ public:
         const int vid = sym.view_id.at(v);
         const int gid = sym.view_group.at(static_cast<size_t>(vid));
         if (v.is_scalar() || v.ndim == 0) return "(p.v" + to_string(vid) + "_o)";
+        // Unit and zero strides are structural (part of the plan key), so they are written as
+        // literals: no multiply for a contiguous axis, no term for a broadcast one.
+        const vector<int64_t> &st = sym.stride_groups.at(static_cast<size_t>(gid));
         stringstream ss;
         ss << "((";
+        bool any = false;
         for (int64_t i = 0; i < v.ndim; ++i) {
             int t = static_cast<int>(i);
             if (t >= hidden_axis) ++t;
-            if (i > 0) ss << " + ";
+            const int64_t stride = st.at(static_cast<size_t>(i));
+            if (stride == 0) continue;
+            if (any) ss << " + ";
+            any = true;
             if (axis_offset.first == t) {
                 ss << "(i" << t << " == 0 ? 0 : i" << t << " + (" << axis_offset.second << "))";
             } else {
                 ss << "i" << t;
             }
-            ss << " * p.g" << gid << "_s" << i;
+            if (stride != 1) ss << " * p.g" << gid << "_s" << i;
         }
+        if (!any) ss << "0";
         ss << ") + p.v" << vid << "_o)";
         return ss.str();
     }

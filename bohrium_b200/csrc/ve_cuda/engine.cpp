@@ -1236,9 +1236,14 @@ void EngineCUDA::handleExtmethod(BhIR *bhir) {
             handleExecution(&b);
             instr_list.clear();
             if (ext != comp.extmethods.end()) {
-                ext->second.execute(&instr, this);
-                for (const bh_view &v : instr.operand)
-                    if (!v.isConstant() && &v == &instr.operand[0]) host_stale.insert(v.base);
+                bh_ve_cuda_ext_context ctx;
+                ctx.version = 1;
+                ctx.engine = this;
+                ctx.stream = _stream;
+                ctx.device_pointer = [](void *e, bh_base *b) { return static_cast<EngineCUDA *>(e)->getBuffer(b); };
+                ctx.written = [](void *e, bh_base *b) { static_cast<EngineCUDA *>(e)->mark_device_written(b); };
+                ext->second.execute(&instr, &ctx);
+                if (!instr.operand.empty() && !instr.operand[0].isConstant()) mark_device_written(instr.operand[0].base);
             } else {
                 set<bh_base *> bases = instr.get_bases();
                 copyToHost(bases, true);

@@ -75,6 +75,7 @@ public:
     void copyToHost(const std::set<bh_base *> &bases, bool evict);
     void copyAllBasesToHost();
     void *getBuffer(bh_base *base); // device pointer (allocated/uploaded on demand)
+    void mark_device_written(bh_base *base) { host_stale.insert(base); }
     void delBuffer(bh_base *base);
     void synchronize();
 

@@ -74,3 +74,30 @@ class DryRunExecutor:
 
     def message(self, msg: str) -> str:
         return ""
+
+
+def filter_text(flush: ir.Flush, filters=("bcexp", "bccon")) -> tuple[list, str]:
+    """Apply the bytecode filters of the filter components to `flush` (decoded natively) and
+    return (rewrites per filter, the text listing of the result, see bhb_ir_text)."""
+    lib = load_library()
+    lib.bhb_ir_filter.restype = ctypes.c_int
+    lib.bhb_ir_filter.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+    lib.bhb_ir_text.restype = ctypes.c_char_p
+    lib.bhb_ir_text.argtypes = [ctypes.c_void_p]
+    words = ir.encode(flush.instrs)
+    slides = ir.encode_slides(flush.instrs)
+    syncs = (ctypes.c_void_p * max(len(flush.syncs), 1))(*[b.handle for b in flush.syncs])
+    h = lib.bhb_ir_create(words.ctypes.data, len(words), syncs, len(flush.syncs), flush.nrepeats, None,
+                          slides.ctypes.data, len(slides))
+    if not h:
+        raise RuntimeError("bhb_ir_create: " + lib.bhb_last_error().decode())
+    try:
+        counts = []
+        for f in filters:
+            n = lib.bhb_ir_filter(h, f.encode())
+            if n < 0:
+                raise RuntimeError("bhb_ir_filter: " + lib.bhb_last_error().decode())
+            counts.append(n)
+        return counts, lib.bhb_ir_text(h).decode()
+    finally:
+        lib.bhb_ir_destroy(h)

@@ -105,10 +105,31 @@ void *bhb_base_data(const bh_base *base);
 void *bhb_ir_bhir(bhb_ir *ir);
 /* Set the message returned by bhb_last_error() on this thread. */
 void bhb_set_last_error(const char *msg);
+/* Apply a bytecode filter of the filter components in place: "bcexp" (powk), "bcexp+sign",
+ * "bccon" (stupidmath, collect, muladd). Returns the number of rewrites, -1 on error. (The filters
+ * restate filter/bcexp/expander.cpp:42-87 and filter/bccon/contracter.cpp:46-52.) */
+int bhb_ir_filter(bhb_ir *ir, const char *name);
+/* Text listing of a decoded BhIR (opcode, operands with bases numbered by first appearance,
+ * constant), valid until the next call on the same handle. */
+const char *bhb_ir_text(bhb_ir *ir);
 /* libbh_ve_cuda.so: fuse `ir`, generate the kernel sources and, if `compile` is set, compile them
  * with NVRTC for sm_100a, all without a GPU. Returns a JSON document (valid until the next call)
  * or NULL on error. `fuser_list` overrides the transformer list (NULL: the engine default). */
 const char *bh_ve_cuda_dry_run(bhb_ir *ir, int compile, const char *fuser_list);
+
+/* --- Extension methods run by the cuda engine (reference: include/bohrium/bh_extmethod.hpp:57-134;
+ * the reference's GPU engines pass themselves as the `arg` of ExtmethodImpl::execute). The cuda
+ * engine passes a pointer to this plain struct instead, so that an extmethod library needs no C++
+ * type of the engine. --- */
+typedef struct bh_ve_cuda_ext_context {
+    int version;   /* 1 */
+    void *engine;  /* opaque; first argument of the callbacks */
+    void *stream;  /* cudaStream_t the engine runs its kernels on; extmethods enqueue on it */
+    /* Device buffer of a base array (allocated, and uploaded from the host copy, on demand). */
+    void *(*device_pointer)(void *engine, bh_base *base);
+    /* Tell the engine that the device copy of `base` was written (its host copy is now stale). */
+    void (*written)(void *engine, bh_base *base);
+} bh_ve_cuda_ext_context;
 
 /* --- libbh_ve_cuda.so: the learned fusion cost model's network (no counterpart in the reference,
  * whose fuser is the plain greedy one, core/jitk/graph.cpp:319-365). An MLP of

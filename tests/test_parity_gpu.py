@@ -369,3 +369,20 @@ def test_scan1d(gpu_rt, oracle_rt, n, dtype, name):
     tol = 0 if np.dtype(dtype).kind == "i" else (1e-4 if np.dtype(dtype) == np.float32 else 1e-11)
     for a, b, what in zip(g, o, ["scan", "after"]):
         assert_close(a, b, tol, tol, what)
+
+
+@pytest.mark.parametrize("m,k,n,dtype,trans", [(64, 48, 80, np.float64, False), (300, 200, 100, np.float32, False),
+                                               (128, 256, 64, np.float64, True)])
+def test_blas_extmethods_on_cublas(gpu_rt, m, k, n, dtype, trans):
+    """blas_gemm / blas_gemmt extension methods run on cuBLAS on the engine's device buffers, between
+    regular bytecode before and after (NumPy is the witness, as in the reference's tests)."""
+    rng = np.random.default_rng(m + n)
+    A = rng.standard_normal((k, m) if trans else (m, k)).astype(dtype)
+    B = rng.standard_normal((k, n)).astype(dtype)
+    a = bh.array(gpu_rt, A) * dtype(2)
+    b = bh.array(gpu_rt, B)
+    c = bh.matmul(a, b, trans_a=trans) + dtype(1)
+    got = c.numpy()
+    want = (2 * (A.T if trans else A)).astype(np.float64) @ B.astype(np.float64) + 1
+    rtol = 1e-4 if dtype == np.float32 else 1e-11
+    np.testing.assert_allclose(got, want, rtol=rtol, atol=rtol * np.abs(want).max())
