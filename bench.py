@@ -421,6 +421,28 @@ def extra_stream(bh, W, ex, rt, out, n=100_000_000):
     del ir, outs, x
 
 
+def extra_axpy(bh, W, ex, rt, out, n=200_000_000):
+    """A memory-bound fused map: z = 2.5 * x + y over 2e8 float32 (FLAT, 12 B per element:
+    x and y read, z written)."""
+    x = bh.random_sample(rt, (n,), start=1, key=11, dtype=np.float32)
+    y = bh.random_sample(rt, (n,), start=2, key=12, dtype=np.float32)
+    rt.flush()
+    z = x * np.float32(2.5) + y
+    ir = ex.compile(rt.take())
+    for _ in range(3):
+        ir.execute()
+    ex.message("CUDA: sync")
+    reps = 10
+    ex.message("CUDA: timer start")
+    for _ in range(reps):
+        ir.execute()
+    ms = float(ex.message("CUDA: timer stop")) / reps
+    gbs = 12 * n / (ms / 1e3) / 1e9
+    out["axpy_f32_2e8"] = {"flush_ms_device": round(ms, 4), "GB/s": round(gbs, 1),
+                           "frac_of_peak": round(gbs / peaks()[0], 3)}
+    del ir, z, x, y
+
+
 def extra_scan(bh, W, ex, rt, out, n=50_000_000):
     """A fused 1-D cumulative sum (SCAN1D): y = cumsum(2x + 1) over 5e7 float64 (8 B read + 8 B
     written per element, algorithmically)."""
@@ -468,7 +490,7 @@ def extra_learned(bh, W, ex, rt, out, train_seeds=24, eval_seeds=12):
 
 
 EXTRAS = {"plain_chain": extra_plain_chain, "heat": extra_heat, "batching": extra_batching, "stream": extra_stream,
-          "scan": extra_scan, "learned": extra_learned}
+          "axpy": extra_axpy, "scan": extra_scan, "learned": extra_learned}
 
 
 def run_extra(bh, W, ex, rt, peak, only=None, heat_n=4096):
