@@ -217,7 +217,7 @@ class BhArray:
     def __eq__(self, o): return binary("EQUAL", self, o, out_dtype=np.bool_)
     def __ne__(self, o): return binary("NOT_EQUAL", self, o, out_dtype=np.bool_)
     def __neg__(self): return binary("MULTIPLY", self, -1)
-    def __abs__(self): return unary("ABSOLUTE", self)
+    def __abs__(self): return absolute(self)
     def __invert__(self): return unary("INVERT", self)
     __hash__ = object.__hash__
 
@@ -301,7 +301,11 @@ def _result_type(a, b):
     if isinstance(s, numbers.Integral):
         return t
     if isinstance(s, numbers.Real):
-        return t if np.issubdtype(t, np.floating) else np.dtype(np.float64)
+        return t if np.issubdtype(t, np.inexact) else np.dtype(np.float64)
+    if isinstance(s, numbers.Complex):
+        if np.issubdtype(t, np.complexfloating):
+            return t
+        return np.dtype(np.complex64) if t == np.float32 else np.dtype(np.complex128)
     return np.result_type(t, np.asarray(s).dtype)
 
 
@@ -338,7 +342,7 @@ def unary(name: str, a: BhArray, out_dtype=None, out: Optional[BhArray] = None) 
 
 def true_divide(a, b):
     def f(x):
-        if isinstance(x, BhArray) and not np.issubdtype(x.dtype, np.floating):
+        if isinstance(x, BhArray) and not np.issubdtype(x.dtype, np.inexact):
             return x.astype(np.float64)
         return x
     return binary("DIVIDE", f(a), f(b))
@@ -392,9 +396,22 @@ def scatter(dst: BhArray, values: BhArray, index: BhArray) -> None:
 
 def _make_unary(name, float_only=False):
     def f(a, out=None):
-        if float_only and not np.issubdtype(a.dtype, np.floating):
+        if float_only and not np.issubdtype(a.dtype, np.inexact):
             a = a.astype(np.float64)
         return unary(name, a, out=out)
+    f.__name__ = name.lower()
+    return f
+
+
+def _real_dtype(dt):
+    return np.dtype(np.float32) if dt == np.complex64 else np.dtype(np.float64)
+
+
+def _complex_part(name):
+    def f(a, out=None):
+        if not np.issubdtype(a.dtype, np.complexfloating):
+            raise TypeError(f"{name.lower()}(): complex array expected")
+        return unary(name, a, out_dtype=_real_dtype(a.dtype), out=out)
     f.__name__ = name.lower()
     return f
 
@@ -405,9 +422,28 @@ log = _make_unary("LOG", True)
 sin = _make_unary("SIN", True)
 cos = _make_unary("COS", True)
 tanh = _make_unary("TANH", True)
-absolute = _make_unary("ABSOLUTE")
 floor = _make_unary("FLOOR", True)
 sign = _make_unary("SIGN")
+tan = _make_unary("TAN", True)
+sinh = _make_unary("SINH", True)
+cosh = _make_unary("COSH", True)
+log10 = _make_unary("LOG10", True)
+real = _complex_part("REAL")
+imag = _complex_part("IMAG")
+
+
+def absolute(a, out=None):
+    """|a| (BH_ABSOLUTE); the modulus, a real array, for complex input."""
+    if np.issubdtype(a.dtype, np.complexfloating):
+        return unary("ABSOLUTE", a, out_dtype=_real_dtype(a.dtype), out=out)
+    return unary("ABSOLUTE", a, out=out)
+
+
+def conj(a, out=None):
+    """Complex conjugate (BH_CONJ)."""
+    if not np.issubdtype(a.dtype, np.complexfloating):
+        raise TypeError("conj(): complex array expected")
+    return unary("CONJ", a, out=out)
 
 
 def maximum(a, b):

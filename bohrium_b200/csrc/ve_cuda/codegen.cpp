@@ -59,7 +59,7 @@ int64_t LaunchUnit::work_items() const {
 
 int64_t LaunchUnit::scratch_bytes() const {
     if (sched == Sched::GRID_REDUCE) return (cols + kReduceTile - 1) / kReduceTile * scratch_bytes_per_tile;
-    if (sched == Sched::SPLIT_REDUCE) return 8 * static_cast<int64_t>(nred) * chunks * rows * cols;
+    if (sched == Sched::SPLIT_REDUCE) return slot_bytes * static_cast<int64_t>(nred) * chunks * rows * cols;
     if (sched == Sched::SCAN1D) return 0;  // totals/carries live in the engine's scan arena
     return 0;
 }
@@ -101,8 +101,6 @@ const char *kPrelude = R"CUDA(
 typedef long long bh_i64;
 typedef unsigned long long bh_u64;
 struct bh_r123 { bh_u64 start, key; };
-struct bh_c64 { float re, im; };
-struct bh_c128 { double re, im; };
 
 __device__ __forceinline__ bh_u64 bh_random123(bh_u64 start, bh_u64 key, bh_u64 index) {
     const bh_u64 c = start + index;
@@ -119,7 +117,12 @@ __device__ __forceinline__ bh_u64 bh_random123(bh_u64 start, bh_u64 key, bh_u64 
 }
 
 template <typename T> __device__ __forceinline__ T bh_shfl_xor(T v, int m) {
-    if (sizeof(T) == 8) {
+    if (sizeof(T) == 16) {
+        long long x[2]; memcpy(x, &v, 16);
+        x[0] = __shfl_xor_sync(0xffffffffu, x[0], m);
+        x[1] = __shfl_xor_sync(0xffffffffu, x[1], m);
+        T r; memcpy(&r, x, 16); return r;
+    } else if (sizeof(T) == 8) {
         long long x; memcpy(&x, &v, 8);
         x = __shfl_xor_sync(0xffffffffu, x, m);
         T r; memcpy(&r, &x, 8); return r;
@@ -128,6 +131,14 @@ template <typename T> __device__ __forceinline__ T bh_shfl_xor(T v, int m) {
         x = __shfl_xor_sync(0xffffffffu, x, m);
         T r; memcpy(&r, &x, sizeof(T)); return r;
     }
+}
+
+template <typename T> __device__ __forceinline__ T bh_shfl_up(T v, int d) {
+    long long x[2] = {0, 0};
+    memcpy(x, &v, sizeof(T));
+    x[0] = __shfl_up_sync(0xffffffffu, x[0], d);
+    if (sizeof(T) > 8) x[1] = __shfl_up_sync(0xffffffffu, x[1], d);
+    T r; memcpy(&r, x, sizeof(T)); return r;
 }
 
 // Completion counter of a reduction: an acquire-release increment at device scope, so the
@@ -147,7 +158,12 @@ __device__ __forceinline__ void bh_acquire() { asm volatile("fence.acq_rel.gpu;"
 // Load through L2 only (ld.global.cg): for values that other CTAs wrote during this launch.
 template <typename T> __device__ __forceinline__ T bh_ldcg(const T *ptr) {
     T r;
-    if (sizeof(T) == 8) {
+    if (sizeof(T) == 16) {
+        long long x[2];
+        x[0] = __ldcg((const long long *)ptr);
+        x[1] = __ldcg((const long long *)ptr + 1);
+        memcpy(&r, x, 16);
+    } else if (sizeof(T) == 8) {
         const long long x = __ldcg((const long long *)ptr); memcpy(&r, &x, 8);
     } else if (sizeof(T) == 4) {
         const int x = __ldcg((const int *)ptr); memcpy(&r, &x, 4);
@@ -178,6 +194,148 @@ template <typename T> __device__ __forceinline__ T bh_ipow(T b, T e) {
 }
 )CUDA";
 
+// Complex element types (added to the sources of units that use them). bh_c64/bh_c128 have the
+// memory layout of C99's float/double complex and of the bh_constant union (real, imaginary).
+// Arithmetic is written from the definitions; division is Smith's algorithm (R. L. Smith,
+// "Algorithm 116: Complex division", CACM 5(8), 1962), which scales by the larger component of
+// the divisor. The elementary functions use the textbook identities:
+//   exp(x+iy) = e^x (cos y + i sin y);  log z = ln|z| + i atan2(y, x), with ln|z| taken as
+//   log1p((x-1)(x+1) + y^2)/2 near |z| = 1 (where log(hypot) loses the small result);
+//   sqrt z: t = sqrt((|x| + |z|)/2), z^(1/2) = t + iy/(2t) for x >= 0, |y|/(2t) + i sign(y) t else;
+//   sin, cos, sinh, cosh by the addition theorems; tan z = (sin x cos x + i sinh y cosh y) /
+//   (cos^2 x + sinh^2 y) and tanh z = (sinh x cosh x + i sin y cos y) / (sinh^2 x + cos^2 y),
+//   which stay accurate near the poles, with the limit +-i (tan) or +-1 (tanh) once the hyperbolic
+//   terms would overflow; a^b = exp(b log a).
+const char *kComplexPrelude = R"CUDA(
+struct bh_c128;
+struct alignas(8) bh_c64 {
+    float re, im;
+    bh_c64() = default;
+    __device__ __forceinline__ constexpr bh_c64(float r, float i = 0.0f) : re(r), im(i) {}
+    __device__ __forceinline__ bh_c64(const bh_c128 &z);
+};
+struct alignas(16) bh_c128 {
+    double re, im;
+    bh_c128() = default;
+    __device__ __forceinline__ constexpr bh_c128(double r, double i = 0.0) : re(r), im(i) {}
+    __device__ __forceinline__ bh_c128(const bh_c64 &z) : re(z.re), im(z.im) {}
+};
+__device__ __forceinline__ bh_c64::bh_c64(const bh_c128 &z) : re((float)z.re), im((float)z.im) {}
+
+template <typename C> struct bh_cpart;
+template <> struct bh_cpart<bh_c64> { typedef float R; static constexpr float hyp_max = 40.0f; };
+template <> struct bh_cpart<bh_c128> { typedef double R; static constexpr double hyp_max = 300.0; };
+
+__device__ __forceinline__ void bh_sincos(float x, float *s, float *c) { sincosf(x, s, c); }
+__device__ __forceinline__ void bh_sincos(double x, double *s, double *c) { sincos(x, s, c); }
+
+#define BH_COMPLEX_OPERATORS(C)                                                                    \
+    __device__ __forceinline__ C operator+(C a, C b) { return C(a.re + b.re, a.im + b.im); }        \
+    __device__ __forceinline__ C operator-(C a, C b) { return C(a.re - b.re, a.im - b.im); }        \
+    __device__ __forceinline__ C operator*(C a, C b) {                                             \
+        return C(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);                            \
+    }                                                                                              \
+    __device__ __forceinline__ C operator/(C a, C b) {                                             \
+        if (fabs(b.re) >= fabs(b.im)) {                                                            \
+            const auto r = b.im / b.re, d = b.re + b.im * r;                                       \
+            return C((a.re + a.im * r) / d, (a.im - a.re * r) / d);                                \
+        }                                                                                          \
+        const auto r = b.re / b.im, d = b.re * r + b.im;                                           \
+        return C((a.re * r + a.im) / d, (a.im * r - a.re) / d);                                    \
+    }                                                                                              \
+    __device__ __forceinline__ bool operator==(C a, C b) { return a.re == b.re && a.im == b.im; }  \
+    __device__ __forceinline__ bool operator!=(C a, C b) { return a.re != b.re || a.im != b.im; }
+BH_COMPLEX_OPERATORS(bh_c64)
+BH_COMPLEX_OPERATORS(bh_c128)
+
+template <typename C> __device__ __forceinline__ typename bh_cpart<C>::R bh_cabs(C z) { return hypot(z.re, z.im); }
+template <typename C> __device__ __forceinline__ C bh_conj(C z) { return C(z.re, -z.im); }
+template <typename C> __device__ __forceinline__ C bh_csign(C z) {
+    typedef typename bh_cpart<C>::R R;
+    const R v = z.re == (R)0 ? (R)((z.im > (R)0) - ((R)0 > z.im)) : (R)((z.re > (R)0) - ((R)0 > z.re));
+    return C(v, (R)0);
+}
+template <typename C> __device__ __forceinline__ C bh_cexp(C z) {
+    typedef typename bh_cpart<C>::R R;
+    const R e = exp(z.re);
+    R s, c;
+    bh_sincos(z.im, &s, &c);
+    return C(e * c, e * s);
+}
+template <typename C> __device__ __forceinline__ C bh_clog(C z) {
+    typedef typename bh_cpart<C>::R R;
+    const R h = hypot(z.re, z.im);
+    const R lr = (h > (R)0.75 && h < (R)1.25)
+                     ? (R)0.5 * log1p((z.re - (R)1) * (z.re + (R)1) + z.im * z.im)
+                     : log(h);
+    return C(lr, atan2(z.im, z.re));
+}
+template <typename C> __device__ __forceinline__ C bh_clog10(C z) {
+    // the complex log divided by log(10.0f): ln 10 rounded to float, as the reference's engines do
+    typedef typename bh_cpart<C>::R R;
+    const C l = bh_clog(z);
+    const R ln10 = (R)logf(10.0f);
+    return C(l.re / ln10, l.im / ln10);
+}
+template <typename C> __device__ __forceinline__ C bh_csqrt(C z) {
+    typedef typename bh_cpart<C>::R R;
+    if (z.re == (R)0 && z.im == (R)0) return C((R)0, z.im);
+    const R t = sqrt((fabs(z.re) + hypot(z.re, z.im)) * (R)0.5);
+    if (z.re >= (R)0) return C(t, z.im / (t + t));
+    return C(fabs(z.im) / (t + t), copysign(t, z.im));
+}
+template <typename C> __device__ __forceinline__ C bh_csin(C z) {
+    typedef typename bh_cpart<C>::R R;
+    R s, c;
+    bh_sincos(z.re, &s, &c);
+    return C(s * cosh(z.im), c * sinh(z.im));
+}
+template <typename C> __device__ __forceinline__ C bh_ccos(C z) {
+    typedef typename bh_cpart<C>::R R;
+    R s, c;
+    bh_sincos(z.re, &s, &c);
+    return C(c * cosh(z.im), -(s * sinh(z.im)));
+}
+template <typename C> __device__ __forceinline__ C bh_csinh(C z) {
+    typedef typename bh_cpart<C>::R R;
+    R s, c;
+    bh_sincos(z.im, &s, &c);
+    return C(sinh(z.re) * c, cosh(z.re) * s);
+}
+template <typename C> __device__ __forceinline__ C bh_ccosh(C z) {
+    typedef typename bh_cpart<C>::R R;
+    R s, c;
+    bh_sincos(z.im, &s, &c);
+    return C(cosh(z.re) * c, sinh(z.re) * s);
+}
+template <typename C> __device__ __forceinline__ C bh_ctan(C z) {
+    typedef typename bh_cpart<C>::R R;
+    R s, c;
+    bh_sincos(z.re, &s, &c);
+    if (fabs(z.im) > bh_cpart<C>::hyp_max) return C(copysign((R)0, s * c), copysign((R)1, z.im));
+    const R sh = sinh(z.im), ch = cosh(z.im);
+    const R d = c * c + sh * sh;
+    return C(s * c / d, sh * ch / d);
+}
+template <typename C> __device__ __forceinline__ C bh_ctanh(C z) {
+    typedef typename bh_cpart<C>::R R;
+    R s, c;
+    bh_sincos(z.im, &s, &c);
+    if (fabs(z.re) > bh_cpart<C>::hyp_max) return C(copysign((R)1, z.re), copysign((R)0, s * c));
+    const R sh = sinh(z.re), ch = cosh(z.re);
+    const R d = sh * sh + c * c;
+    return C(sh * ch / d, s * c / d);
+}
+template <typename C> __device__ __forceinline__ C bh_cpow(C a, C b) {
+    typedef typename bh_cpart<C>::R R;
+    if (a.re == (R)0 && a.im == (R)0) {
+        if (b.re == (R)0 && b.im == (R)0) return C((R)1, (R)0);
+        if (b.im == (R)0 && b.re > (R)0) return C((R)0, (R)0);
+    }
+    return bh_cexp(b * bh_clog(a));
+}
+)CUDA";
+
 // ---------------------------------------------------------------------------- operation emitting
 bool is_float(bh_type t) { return t == bh_type::FLOAT32 || t == bh_type::FLOAT64; }
 
@@ -186,6 +344,13 @@ bool is_float(bh_type t) { return t == bh_type::FLOAT32 || t == bh_type::FLOAT64
 string fn(const char *name, bh_type t) { return t == bh_type::FLOAT32 ? string(name) + "f" : string(name); }
 
 string sign_expr(const string &x) { return "((" + x + " > 0) - (0 > " + x + "))"; }
+
+// Bytes of one reduction partial in scratch: 8, or 16 when a reduction is complex128.
+int red_slot_bytes(const vector<InstrPtr> &reds) {
+    for (const InstrPtr &r : reds)
+        if (r->operand[0].base->dtype() == bh_type::COMPLEX128) return 16;
+    return 8;
+}
 
 // The combine expression of a reduction: `acc op x`.
 string reduce_expr(bh_opcode op, const string &acc, const string &x) {
@@ -204,15 +369,62 @@ string reduce_expr(bh_opcode op, const string &acc, const string &x) {
     }
 }
 
+// One statement for an instruction with a complex operand (the complex type signatures of
+// core/codegen/opcodes.json; semantics of core/jitk/instruction.cpp:58-544 for C99 complex:
+// ISNAN/ISINF/ISFINITE test the real part, SIGN is csgn with a zero imaginary part). Arithmetic,
+// comparisons, reductions, accumulates and conversions use the operators and converting
+// constructors of bh_c64/bh_c128.
+string complex_statement(const bh_instruction &instr, const vector<string> &ops) {
+    const bh_opcode op = instr.opcode;
+    const string &o = ops[0];
+    auto call = [&](const char *f) { return o + " = " + f + "(" + ops[1] + ");"; };
+    switch (op) {
+        case BH_ADD: return o + " = " + ops[1] + " + " + ops[2] + ";";
+        case BH_SUBTRACT: return o + " = " + ops[1] + " - " + ops[2] + ";";
+        case BH_MULTIPLY: return o + " = " + ops[1] + " * " + ops[2] + ";";
+        case BH_DIVIDE: return o + " = " + ops[1] + " / " + ops[2] + ";";
+        case BH_POWER: return o + " = bh_cpow(" + ops[1] + ", " + ops[2] + ");";
+        case BH_EQUAL: return o + " = " + ops[1] + " == " + ops[2] + ";";
+        case BH_NOT_EQUAL: return o + " = " + ops[1] + " != " + ops[2] + ";";
+        case BH_ABSOLUTE: return call("bh_cabs");
+        case BH_COS: return call("bh_ccos");
+        case BH_SIN: return call("bh_csin");
+        case BH_TAN: return call("bh_ctan");
+        case BH_COSH: return call("bh_ccosh");
+        case BH_SINH: return call("bh_csinh");
+        case BH_TANH: return call("bh_ctanh");
+        case BH_EXP: return call("bh_cexp");
+        case BH_LOG: return call("bh_clog");
+        case BH_LOG10: return call("bh_clog10");
+        case BH_SQRT: return call("bh_csqrt");
+        case BH_SIGN: return call("bh_csign");
+        case BH_CONJ: return call("bh_conj");
+        case BH_REAL: return o + " = " + ops[1] + ".re;";
+        case BH_IMAG: return o + " = " + ops[1] + ".im;";
+        case BH_ISNAN: return o + " = isnan(" + ops[1] + ".re);";
+        case BH_ISINF: return o + " = isinf(" + ops[1] + ".re);";
+        case BH_ISFINITE: return o + " = isfinite(" + ops[1] + ".re);";
+        case BH_IDENTITY:
+        case BH_GATHER:
+        case BH_SCATTER: return o + " = " + ops[1] + ";";
+        case BH_COND_SCATTER: return "if (" + ops[2] + ") { " + o + " = " + ops[1] + "; }";
+        case BH_ADD_ACCUMULATE: return o + " = " + ops[1] + " + " + ops[2] + ";";
+        case BH_MULTIPLY_ACCUMULATE: return o + " = " + ops[1] + " * " + ops[2] + ";";
+        case BH_ADD_REDUCE:
+        case BH_MULTIPLY_REDUCE: return o + " = " + reduce_expr(op, o, ops[1]) + ";";
+        default: break;
+    }
+    throw runtime_error(string("Instruction not supported for complex element types by the CUDA engine: ") +
+                        bh_opcode_text(op));
+}
+
 // One statement computing `instr` given its operand expressions (ops[0] is the output lvalue).
 string op_statement(const bh_instruction &instr, const vector<string> &ops) {
     const bh_opcode op = instr.opcode;
     const bh_type t0 = instr.operand_type(0);
     const bh_type t1 = instr.operand.size() > 1 ? instr.operand_type(1) : t0;
     for (size_t i = 0; i < instr.operand.size(); ++i)
-        if (bh_type_is_complex(instr.operand_type(static_cast<int>(i))))
-            throw runtime_error(string("complex element types are not supported by the CUDA engine: ") +
-                                bh_opcode_text(op));
+        if (bh_type_is_complex(instr.operand_type(static_cast<int>(i)))) return complex_statement(instr, ops);
     const string &o = ops[0];
     auto un = [&](const char *f) { return o + " = " + fn(f, t1) + "(" + ops[1] + ");"; };
     auto bin = [&](const char *sym) { return o + " = " + ops[1] + " " + sym + " " + ops[2] + ";"; };
@@ -340,6 +552,21 @@ string constant_literal(const bh_constant &c) {
             int64_t bits;
             memcpy(&bits, &c.value.float64, 8);
             ss << "__longlong_as_double(" << static_cast<uint64_t>(bits) << "LL)";
+            break;
+        }
+        case bh_type::COMPLEX64: {
+            uint32_t re, im;
+            memcpy(&re, &c.value.complex64.real, 4);
+            memcpy(&im, &c.value.complex64.imag, 4);
+            ss << "bh_c64(__int_as_float(" << static_cast<int32_t>(re) << "), __int_as_float(" << static_cast<int32_t>(im)
+               << "))";
+            break;
+        }
+        case bh_type::COMPLEX128: {
+            uint64_t re, im;
+            memcpy(&re, &c.value.complex128.real, 8);
+            memcpy(&im, &c.value.complex128.imag, 8);
+            ss << "bh_c128(__longlong_as_double(" << re << "LL), __longlong_as_double(" << im << "LL))";
             break;
         }
         default: throw runtime_error("constant_literal(): unsupported constant type");
@@ -541,7 +768,11 @@ public:
         return !(s.is_tmp(v.base) || s.replaced(v) || external_acc.count(ViewKey(v)));
     }
 
-    string const_ref(const bh_instruction &instr) { return "p.c" + to_string(sym.const_id.at(&instr)); }
+    string const_ref(const bh_instruction &instr) {
+        const string c = "p.c" + to_string(sym.const_id.at(&instr));
+        if (instr.constant.type == bh_type::COMPLEX128) return "bh_c128(" + c + "_re, " + c + "_im)";
+        return c;
+    }
 
     void write_instr(const bh_instruction &instr, const Scope &s, int ind) {
         if (bh_opcode_is_system(instr.opcode) || instr.operand.empty()) return;
@@ -694,9 +925,15 @@ void add_common_fields(Symbols &sym, ParamLayout &pl, const CodegenOptions &opt)
             pl.add(f, "bh_u64", "c" + to_string(i) + "_start");
             f.kind = ParamField::R123_KEY;
             pl.add(f, "bh_u64", "c" + to_string(i) + "_key");
+        } else if (instr->constant.type == bh_type::COMPLEX128) {
+            // 16 bytes: two 8-byte parameter slots, the real and the imaginary part
+            ParamField f{ParamField::CONST};
+            f.c = instr->constant;
+            f.origin = instr->origin_id;
+            pl.add(f, "double", "c" + to_string(i) + "_re");
+            f.part = 1;
+            pl.add(f, "double", "c" + to_string(i) + "_im");
         } else {
-            if (bh_type_is_complex(instr->constant.type))
-                throw runtime_error("complex constants are not supported by the CUDA engine");
             ParamField f{ParamField::CONST};
             f.c = instr->constant;
             f.origin = instr->origin_id;
@@ -736,6 +973,8 @@ uint64_t fnv1a(const string &s) {
 void finish_source(LaunchUnit &u, const string &params_decl, const string &body, const CodegenOptions &opt) {
     stringstream src;
     src << kPrelude;
+    auto uses = [&](const char *name) { return params_decl.find(name) != string::npos || body.find(name) != string::npos; };
+    if (uses("bh_c64") || uses("bh_c128")) src << kComplexPrelude;
     if (opt.bounds_check) src << bounds_check_helper();
     src << "struct P {\n" << params_decl << "};\n";
     src << body;
@@ -1266,8 +1505,9 @@ LaunchUnit lower_split_reduce(const LoopB &loop, unsigned P, const CodegenOption
     body << "    __shared__ bool am_last;\n";
     body << "    const bh_i64 pb = w / p.chunks, chunk = w - pb * p.chunks;\n";
     body << "    const bh_i64 pt = pb * " << kThreads << " + threadIdx.x;\n";
+    u.slot_bytes = red_slot_bytes(reds);
     for (size_t k = 0; k < reds.size(); ++k)
-        body << "    " << ctypes[k] << "* part" << k << " = (" << ctypes[k] << "*)(p.scratch + " << 8 * k
+        body << "    " << ctypes[k] << "* part" << k << " = (" << ctypes[k] << "*)(p.scratch + " << u.slot_bytes * k
              << " * p.chunks * p.points);\n";
     // Decompose the point into the threaded indices i0..i{P-1}.
     auto decompose = [&](int ind) {
@@ -1481,16 +1721,17 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
         helpers << block_reduce_fn(ctypes[k], "bh_block_reduce" + to_string(k), r->opcode, idents[k]);
         helpers << block_reduce_k_fn(ctypes[k], "bh_block_reduce_k" + to_string(k), r->opcode, idents[k], K);
     }
-    u.scratch_bytes_per_tile = 8 * static_cast<int64_t>(reds.size());
+    u.slot_bytes = red_slot_bytes(reds);
+    u.scratch_bytes_per_tile = u.slot_bytes * static_cast<int64_t>(reds.size());
     for (const InstrPtr &r : reds) u.red_orders.emplace_back(r->origin_id, "tree:" + to_string(L.size));
     body << helpers.str();
     body << "__device__ void bh_work(const P &p, bh_i64 w) {\n";
     body << pointer_locals(sym);
-    body << "    __shared__ unsigned long long sm_raw[" << (kThreads / 32) * K << "];\n";
+    body << "    __shared__ alignas(16) unsigned long long sm_raw[" << (kThreads / 32) * K * (u.slot_bytes / 8) << "];\n";
     body << "    __shared__ bool am_last;\n";
     for (size_t k = 0; k < reds.size(); ++k)
-        body << "    " << ctypes[k] << "* part" << k << " = (" << ctypes[k] << "*)(p.scratch + p.ntiles * " << 8 * k
-             << ");\n";
+        body << "    " << ctypes[k] << "* part" << k << " = (" << ctypes[k] << "*)(p.scratch + p.ntiles * "
+             << u.slot_bytes * k << ");\n";
     for (size_t k = 0; k < reds.size(); ++k) {
         body << "    " << ctypes[k] << " " << accs[k] << "[" << K << "];\n";
         body << "#pragma unroll\n";
@@ -1560,7 +1801,7 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
         body << "    {\n";
         body << "        " << ctypes[k] << " acc = " << idents[k] << ";\n";
         body << "        for (bh_i64 t = threadIdx.x; t < p.ntiles; t += " << kThreads << ") {\n";
-        body << "            const " << ctypes[k] << " x = ((volatile " << ctypes[k] << "*)part" << k << ")[t];\n";
+        body << "            const " << ctypes[k] << " x = bh_ldcg(part" << k << " + t);\n";
         body << "            acc = " << reduce_expr(r->opcode, "acc", "x") << ";\n";
         body << "        }\n";
         body << "        acc = bh_block_reduce" << k << "(acc, (" << ctypes[k] << "*)sm_raw);\n";
@@ -1605,13 +1846,11 @@ string block_scan_fn(const string &T, const string &fname, bh_opcode op, const s
     ss << "#pragma unroll\n";
     ss << "    for (int d = 1; d < 32; d <<= 1) {\n";
     ss << "        " << T << " y = x;\n";
-    ss << "        { long long b; memcpy(&b, &y, sizeof(y) < 8 ? sizeof(y) : 8); b = __shfl_up_sync(0xffffffffu, b, d); "
-          "memcpy(&y, &b, sizeof(y) < 8 ? sizeof(y) : 8); }\n";
+    ss << "        y = bh_shfl_up(y, d);\n";
     ss << "        if (lane >= d) x = " << reduce_expr(op, "y", "x") << ";\n";
     ss << "    }\n";
     ss << "    " << T << " ex = x;\n";
-    ss << "    { long long b; memcpy(&b, &ex, sizeof(ex) < 8 ? sizeof(ex) : 8); b = __shfl_up_sync(0xffffffffu, b, 1); "
-          "memcpy(&ex, &b, sizeof(ex) < 8 ? sizeof(ex) : 8); }\n";
+    ss << "    ex = bh_shfl_up(ex, 1);\n";
     ss << "    if (lane == 0) ex = " << ident << ";\n";
     ss << "    __syncthreads();\n";
     ss << "    if (lane == 31) sm[warp] = x;\n";
@@ -1793,6 +2032,7 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
         }
         u.fields = pl.fields;
         u.scratch_bytes_per_tile = 0;
+        u.scan_bytes_per_chunk = 2 * static_cast<int64_t>(bh_type_size(t));
         u.algorithmic_bytes = phase == 2 ? unit_bytes(sym, vector<const Block *>{&holder}) : 0;
         u.elements = phase == 1 ? nchunks : n;
         if (phase == 2) u.red_orders.emplace_back(acc->origin_id, "scan:" + to_string(kScanTile) + ":" + to_string(n));

@@ -57,6 +57,7 @@ struct ParamField {
     int64_t i64 = 0;         // I64
     bh_constant c{};         // CONST / R123_*
     int64_t origin = -1;     // CONST / R123_*: origin id of the instruction holding the constant
+    int part = 0;            // CONST: which 8 bytes of the constant (1: the imaginary part of a complex128)
 };
 
 struct LaunchUnit {
@@ -68,6 +69,8 @@ struct LaunchUnit {
     int64_t rows = 1, cols = 1; // FLAT / OUTER_REDUCE index space; GRID_REDUCE/SCAN1D: cols = length
     int nred = 0;               // GRID_REDUCE / SPLIT_REDUCE: number of reductions
     int64_t scratch_bytes_per_tile = 0; // GRID_REDUCE: bytes of partials per tile (all reductions)
+    int slot_bytes = 8;         // GRID_REDUCE / SPLIT_REDUCE: bytes of one partial (16 with complex128)
+    int64_t scan_bytes_per_chunk = 16; // SCAN1D: total + carry of one chunk in the scan arena
     int64_t chunks = 1;         // SPLIT_REDUCE: chunks of the swept axis; LANE_REDUCE: lanes per point;
                                 // GRID_REDUCE: tiles per work item; SCAN1D: work items of the phase
     int64_t scan_chunks = 0;    // SCAN1D: chunks of 2048 elements

@@ -326,6 +326,12 @@ void EngineCUDA::setMemoryPointer(bh_base *base, bool host_ptr, void *mem) {
         if (base->getDataPtr() != nullptr && base->getDataPtr() != mem) bh_data_free(base);
         base->resetDataPtr(mem);
     } else {
+        // Kernels load whole elements (16 bytes at once for complex128): an address that is not a
+        // multiple of the element size would be a misaligned access on the device.
+        const int64_t esize = bh_type_size(base->dtype());
+        if (mem != nullptr && reinterpret_cast<uintptr_t>(mem) % static_cast<uintptr_t>(esize) != 0)
+            throw runtime_error("setMemoryPointer(): device pointer is not aligned to the element size (" +
+                                to_string(esize) + " bytes)");
         delBuffer(base);
         DevBuf b;
         b.ptr = mem;
@@ -567,7 +573,8 @@ void EngineCUDA::pack_params(const PlanUnit &pu, const vector<bh_base *> &bases,
             case ParamField::CONST: {
                 const bh_constant &c =
                     f.origin >= 0 && f.origin < static_cast<int64_t>(instrs.size()) ? instrs[f.origin]->constant : f.c;
-                memcpy(slot, &c.value, static_cast<size_t>(bh_type_size(f.c.type)));
+                memcpy(slot, reinterpret_cast<const uint8_t *>(&c.value) + 8 * f.part,
+                       static_cast<size_t>(min<int64_t>(bh_type_size(f.c.type), 8)));
                 break;
             }
             case ParamField::R123_START:
@@ -1009,7 +1016,7 @@ EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const
             for (LaunchUnit &u : units) {
                 if (u.sched != Sched::SCAN1D) continue;
                 u.scan_offset = plan.scan_bytes;
-                scan_need = max<int64_t>(scan_need, (16 * u.scan_chunks + 255) / 256 * 256);
+                scan_need = max<int64_t>(scan_need, (u.scan_bytes_per_chunk * u.scan_chunks + 255) / 256 * 256);
             }
             plan.scan_bytes += scan_need;
             for (LaunchUnit &u : units) {

@@ -33,7 +33,8 @@ CFLAGS = ["-x", "c", "-fPIC", "-shared", "-std=gnu99", "-O3", "-march=native", "
 _CTYPE = {np.dtype(np.bool_): "bool", np.dtype(np.int8): "int8_t", np.dtype(np.int16): "int16_t",
           np.dtype(np.int32): "int32_t", np.dtype(np.int64): "int64_t", np.dtype(np.uint8): "uint8_t",
           np.dtype(np.uint16): "uint16_t", np.dtype(np.uint32): "uint32_t", np.dtype(np.uint64): "uint64_t",
-          np.dtype(np.float32): "float", np.dtype(np.float64): "double"}
+          np.dtype(np.float32): "float", np.dtype(np.float64): "double",
+          np.dtype(np.complex64): "float complex", np.dtype(np.complex128): "double complex"}
 
 _RED = {"ADD_REDUCE": "+", "MULTIPLY_REDUCE": "*", "BITWISE_AND_REDUCE": "&", "BITWISE_OR_REDUCE": "|",
         "BITWISE_XOR_REDUCE": "^", "MAXIMUM_REDUCE": "max", "MINIMUM_REDUCE": "min"}
@@ -49,6 +50,10 @@ def ctype(dt) -> str:
 
 def _isfloat(dt):
     return np.issubdtype(np.dtype(dt), np.floating)
+
+
+def _iscomplex(dt):
+    return dt is not None and np.issubdtype(np.dtype(dt), np.complexfloating)
 
 
 def _is_signed(dt):
@@ -93,7 +98,7 @@ def op_statement(ins: I, ops, atomic=False) -> str:
           "ARCCOS": "acos", "ARCTAN": "atan", "ARCSINH": "asinh", "ARCCOSH": "acosh", "ARCTANH": "atanh",
           "EXP": "exp", "EXP2": "exp2", "EXPM1": "expm1", "LOG": "log", "LOG2": "log2", "LOG10": "log10",
           "LOG1P": "log1p", "SQRT": "sqrt", "CEIL": "ceil", "TRUNC": "trunc", "FLOOR": "floor", "RINT": "rint"}
-    if name in fn:
+    if name in fn and not (name == "LOG10" and _iscomplex(t0)):
         return f"{o} = {fn[name]}({ops[1]});"
     a = ops[1] if len(ops) > 1 else None
     b = ops[2] if len(ops) > 2 else None
@@ -102,13 +107,13 @@ def op_statement(ins: I, ops, atomic=False) -> str:
             return (f"{o} = (({a} > 0) != ({b} > 0) && ({a} % {b}) != 0) ? ({a} / {b} - 1) : ({a} / {b});")
         return f"{o} = {a} / {b};"
     if name == "POWER":
-        if not _isfloat(t0):
+        if not _isfloat(t0) and not _iscomplex(t0):
             return f"{o} = pow((double) {a}, (double) {b});"
         return f"{o} = pow({a}, {b});"
     if name == "ABSOLUTE":
         if t1 == np.bool_ or _is_unsigned(t1):
             return f"{o} = {a};"
-        if _isfloat(t1):
+        if _isfloat(t1) or _iscomplex(t1):  # <tgmath.h>: fabs of a complex value is cabs
             return f"{o} = fabs({a});"
         if t1 == np.int64:
             return f"{o} = llabs({a});"
@@ -134,6 +139,8 @@ def op_statement(ins: I, ops, atomic=False) -> str:
             return f"{o} = {a} % {b};"
         return f"{o} = (({a} > 0) == ({b} > 0) || ({a} % {b}) == 0) ? ({a} % {b}) : ({a} % {b}) + {b};"
     if name in ("ISNAN", "ISINF", "ISFINITE"):
+        if _iscomplex(t1):  # the real part only (instruction.cpp:212-258)
+            return f"{o} = {name.lower()}(creal({a}));"
         if _isfloat(t1):
             return f"{o} = {name.lower()}({a});"
         return f"{o} = {'true' if name == 'ISFINITE' else 'false'};"
@@ -142,7 +149,21 @@ def op_statement(ins: I, ops, atomic=False) -> str:
     if name == "COND_SCATTER":
         return f"if ({ops[2]}) {{ {o} = {a}; }}"
     if name == "SIGN":
+        if _iscomplex(t0):  # csgn: sgn(Re z), or sgn(Im z) where Re z == 0 (instruction.cpp:493-527)
+            rt = "float" if t0 == np.complex64 else "double"
+            return (f"{{ {rt} re_ = creal({a}), im_ = cimag({a}); "
+                    f"{o} = (re_ == 0 ? ((im_ > 0) - (0 > im_)) : ((re_ > 0) - (0 > re_))); }}")
         return f"{o} = (({a} > 0) - (0 > {a}));"
+    if name == "REAL":
+        return f"{o} = creal({a});"
+    if name == "IMAG":
+        return f"{o} = cimag({a});"
+    if name == "CONJ":
+        return f"{o} = conj({a});"
+    if name == "LOG10" and _iscomplex(t0):
+        # C99 has no complex log10; the reference divides by log(10.0f), a float under <tgmath.h>
+        # (instruction.cpp:459-475).
+        return f"{o} = clog({a}) / log(10.0f);"
     if name == "ADD_ACCUMULATE":
         return f"{o} = {a} + {b};"
     if name == "MULTIPLY_ACCUMULATE":
@@ -235,7 +256,8 @@ class _Kernel:
     # -- writing ---------------------------------------------------------------------------
     def _write(self):
         L = self.lines
-        L += ["#include <stdint.h>", "#include <stdlib.h>", "#include <stdbool.h>", "#include <tgmath.h>",
+        L += ["#include <stdint.h>", "#include <stdlib.h>", "#include <stdbool.h>", "#include <complex.h>",
+              "#include <tgmath.h>",
               "#include <math.h>", '#include "kernel_deps.h"', "",
               "void kernel(void **data, const int64_t *m, const unsigned char *c) {"]
         for k, b in enumerate(self.params):
@@ -290,7 +312,9 @@ class _Kernel:
                 local = scope.repl(v) is not None or scope.is_tmp(v.base.id)
                 if nm in _RED and local:
                     clauses.append(f"reduction({_RED[nm]}:{self.name(v, scope)})")
-                elif nm in _ATOMIC:
+                elif nm in _ATOMIC and not _iscomplex(v.base.dtype):
+                    # gcc rejects `omp atomic` on complex lvalues, which the reference would emit
+                    # (openmp_util.hpp:82-94); complex outputs take the critical section instead.
                     self.atomic.add(id(s))
                 else:
                     self.critical.add(id(s))

@@ -237,3 +237,140 @@ def empty_program():
         b = a * 2 + 1
         return [b]
     return prog
+
+
+# ----------------------------------------------------------------------------- complex numbers
+# The reference's complex type signatures (core/codegen/opcodes.json): ADD, SUBTRACT, MULTIPLY,
+# DIVIDE, POWER; COS ... TANH, EXP, LOG, LOG10, SQRT, SIGN, CONJ (complex -> complex); ABSOLUTE,
+# REAL, IMAG (complex -> real); ISNAN, ISINF, ISFINITE, EQUAL, NOT_EQUAL (-> bool); IDENTITY from
+# every type; ADD/MULTIPLY reductions and accumulates; GATHER, SCATTER, COND_SCATTER.
+COMPLEX_TYPES = [np.complex64, np.complex128]
+COMPLEX_BINARY = ["ADD", "SUBTRACT", "MULTIPLY", "DIVIDE", "POWER"]
+COMPLEX_UNARY = ["COS", "SIN", "TAN", "COSH", "SINH", "TANH", "EXP", "LOG", "LOG10", "SQRT", "SIGN", "CONJ"]
+COMPLEX_TO_REAL = ["ABSOLUTE", "REAL", "IMAG"]
+COMPLEX_PREDICATES = ["ISNAN", "ISINF", "ISFINITE"]
+COMPLEX_TRANSCENDENTAL = {"COS", "SIN", "TAN", "COSH", "SINH", "TANH", "EXP", "LOG", "LOG10", "SQRT", "POWER",
+                          "ABSOLUTE", "DIVIDE"}
+
+
+def real_dtype(dtype):
+    return np.dtype(np.float32) if np.dtype(dtype) == np.complex64 else np.dtype(np.float64)
+
+
+def cdata(shape, dtype, seed, lo=-2.0, hi=2.0):
+    """Seeded complex values with real and imaginary parts uniform in [lo, hi)."""
+    rng = np.random.default_rng(seed)
+    re = rng.random(shape) * (hi - lo) + lo
+    im = rng.random(shape) * (hi - lo) + lo
+    return (re + 1j * im).astype(dtype)
+
+
+def complex_binary_program(name, dtype, n=1000, seed=0):
+    def prog(rt):
+        A = cdata(n, dtype, seed, 0.1, 2.0)
+        B = cdata(n, dtype, seed + 1, 0.1 if name in ("DIVIDE", "POWER") else -2.0, 1.5)
+        a, b = bh.array(rt, A), bh.array(rt, B)
+        out = bh.empty(rt, (n,), dtype)
+        rt.enqueue(ir.Instr(ir.OPCODES[name], [out.view(), a.view(), b.view()]))
+        out2 = bh.empty(rt, (n,), dtype)
+        rt.enqueue(ir.Instr(ir.OPCODES[name], [out2.view(), a.view(), None],
+                            ir.Constant(complex(B[3]), ir.bh_type(np.dtype(dtype)))))
+        return [out, out2]
+    return prog
+
+
+def complex_unary_program(name, dtype, n=1000, seed=0):
+    dt = np.dtype(dtype)
+    out_dt = {**{k: real_dtype(dt) for k in COMPLEX_TO_REAL},
+              **{k: np.dtype(np.bool_) for k in COMPLEX_PREDICATES}}.get(name, dt)
+
+    def prog(rt):
+        A = cdata(n, dt, seed)
+        if name == "SIGN":
+            A.real[::5] = 0  # the imaginary part decides there
+            A[::25] = 0
+        if name in COMPLEX_PREDICATES:
+            A.real[::7] = np.nan
+            A.imag[3::7] = np.nan  # a NaN imaginary part alone: the reference tests the real part
+            A.real[1::11] = np.inf
+            A.imag[5::11] = np.inf
+        a = bh.array(rt, A)
+        out = bh.empty(rt, (n,), out_dt)
+        rt.enqueue(ir.Instr(ir.OPCODES[name], [out.view(), a.view()]))
+        return [out]
+    return prog
+
+
+def complex_compare_program(name, dtype, n=1000, seed=0):
+    def prog(rt):
+        A = cdata(n, dtype, seed)
+        B = cdata(n, dtype, seed + 1)
+        B[::3] = A[::3]
+        B.real[1::5] = A.real[1::5]  # equal real parts, different imaginary parts
+        a, b = bh.array(rt, A), bh.array(rt, B)
+        out = bh.empty(rt, (n,), np.bool_)
+        rt.enqueue(ir.Instr(ir.OPCODES[name], [out.view(), a.view(), b.view()]))
+        return [out]
+    return prog
+
+
+def complex_identity_program(src_dt, dst_dt, n=500, seed=0):
+    def prog(rt):
+        s = np.dtype(src_dt)
+        if s.kind == "c":
+            A = cdata(n, s, seed, -100.0, 100.0)
+        elif s.kind == "f":
+            A = data(n, s, seed, -100.0, 100.0)
+        else:
+            A = data(n, s, seed)
+        return [bh.array(rt, A).astype(dst_dt)]
+    return prog
+
+
+def complex_reduce_program(name, dtype, shape, axis, seed=0):
+    def prog(rt):
+        if name == "MULTIPLY_REDUCE":
+            # |z| near 1 and small phases, so long products stay finite
+            rng = np.random.default_rng(seed)
+            A = ((0.95 + 0.1 * rng.random(shape)) * np.exp(0.05j * (rng.random(shape) - 0.5))).astype(dtype)
+        else:
+            A = cdata(shape, dtype, seed)
+        return [bh.reduce(name, bh.array(rt, A), axis)]
+    return prog
+
+
+def complex_accumulate_program(name, dtype, shape, axis, seed=0):
+    def prog(rt):
+        rng = np.random.default_rng(seed)
+        if name == "MULTIPLY_ACCUMULATE":
+            A = ((0.98 + 0.04 * rng.random(shape)) * np.exp(0.05j * (rng.random(shape) - 0.5))).astype(dtype)
+        else:
+            A = cdata(shape, dtype, seed)
+        return [bh.accumulate(name, bh.array(rt, A), axis)]
+    return prog
+
+
+def complex_gather_scatter_program(dtype, n=1000, seed=0):
+    def prog(rt):
+        rng = np.random.default_rng(seed)
+        src = bh.array(rt, cdata(n, dtype, seed))
+        idx = bh.array(rt, rng.permutation(n).astype(np.uint64))
+        g = bh.gather(src, idx)
+        dst = bh.zeros(rt, (n,), dtype)
+        bh.scatter(dst, g, idx)
+        return [g, dst]
+    return prog
+
+
+def complex_chain_program(n, dtype=np.complex128, seed=0):
+    """A fused complex chain: twiddle factors exp(i*theta) applied to a signal, a complex sum,
+    the power |z|^2 as a real array and its sum."""
+    def prog(rt):
+        rdt = real_dtype(dtype)
+        x = bh.array(rt, cdata(n, dtype, seed))
+        theta = bh.array(rt, data(n, rdt, seed + 1, -3.0, 3.0))
+        w = bh.exp(theta.astype(dtype) * 1j)
+        z = w * x + bh.conj(x) * 0.5
+        p = bh.real(z) * bh.real(z) + bh.imag(z) * bh.imag(z)
+        return [z, z.sum(), p, p.sum(), bh.absolute(z)]
+    return prog

@@ -138,3 +138,23 @@ def test_one_dimensional_accumulate_lowers_to_three_scan_units():
         return [bh.accumulate("ADD_ACCUMULATE", a * 2.0 + 1.0, 0) * 3.0]
     res, units = plan(prog)
     assert [u["sched"] for u in units] == ["scan1d", "scan1d", "scan1d"], [u["sched"] for u in units]
+
+
+def test_complex_programs_compile_for_every_schedule():
+    """Complex64/complex128 kernels compile with NVRTC: every elementwise opcode of the complex
+    type signatures, and reductions/accumulates on the GRID_REDUCE, SPLIT_REDUCE, LANE_REDUCE and
+    SCAN1D schedules (16-byte partials, shuffles and scan totals for complex128)."""
+    seen = set()
+    for dt in P.COMPLEX_TYPES:
+        progs = [P.complex_binary_program(n, dt) for n in P.COMPLEX_BINARY]
+        progs += [P.complex_unary_program(n, dt) for n in P.COMPLEX_UNARY + P.COMPLEX_TO_REAL + P.COMPLEX_PREDICATES]
+        progs += [P.complex_compare_program("EQUAL", dt), P.complex_gather_scatter_program(dt)]
+        progs += [P.complex_reduce_program(n, dt, shape, ax) for n in ("ADD_REDUCE", "MULTIPLY_REDUCE")
+                  for shape, ax in [((1 << 20,), 0), ((4096, 64), 0), ((4096, 4096), 1), ((40, 30), 1)]]
+        progs += [P.complex_accumulate_program("ADD_ACCUMULATE", dt, (1 << 20,), 0)]
+        for prog in progs:
+            _, units = plan(prog)
+            seen.update(u["sched"] for u in units)
+    _, units = plan(P.complex_chain_program(1 << 20))
+    assert [u["sched"] for u in units] == ["grid_reduce"]
+    assert {"flat", "grid_reduce", "split_reduce", "lane_reduce", "scan1d"} <= seen, seen
