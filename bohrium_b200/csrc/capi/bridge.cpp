@@ -283,9 +283,22 @@ extern "C" int bhb_ir_filter(bhb_ir *ir, const char *name) {
     int n = -1;
     guarded([&] {
         const string f = name ? name : "";
-        if (f == "bcexp" || f == "bcexp+sign") {
+        if (f.compare(0, 5, "bcexp") == 0 && (f.size() == 5 || f[5] == '+')) {
+            // "bcexp" with "+"-separated options: "sign", "reduce1d=<thread limit>"
             bohrium::filter::ExpandOptions o;
-            o.sign = f == "bcexp+sign";
+            size_t pos = 5;
+            while (pos < f.size()) {
+                const size_t next = f.find('+', pos + 1);
+                const string opt = f.substr(pos + 1, next == string::npos ? string::npos : next - pos - 1);
+                if (opt == "sign") {
+                    o.sign = true;
+                } else if (opt.compare(0, 9, "reduce1d=") == 0) {
+                    o.reduce1d = stoll(opt.substr(9));
+                } else {
+                    throw runtime_error("bhb_ir_filter: unknown bcexp option " + opt);
+                }
+                pos = next == string::npos ? f.size() : next;
+            }
             n = bohrium::filter::expand(*ir->ir, o, ir->created);
         } else if (f == "bccon") {
             n = bohrium::filter::contract(*ir->ir, bohrium::filter::ContractOptions());

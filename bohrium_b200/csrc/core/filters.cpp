@@ -37,6 +37,29 @@ bh_view fresh_view(BaseStore &created, const bh_view &like, bh_type t) {
 
 bool int_type(bh_type t) { return bh_type_is_integer(t) != 0; }
 
+bool reduce1d_opcode(bh_opcode op) {
+    switch (op) {
+        case BH_ADD_REDUCE:
+        case BH_MULTIPLY_REDUCE:
+        case BH_MINIMUM_REDUCE:
+        case BH_MAXIMUM_REDUCE:
+        case BH_LOGICAL_AND_REDUCE:
+        case BH_BITWISE_AND_REDUCE:
+        case BH_LOGICAL_OR_REDUCE:
+        case BH_BITWISE_OR_REDUCE:
+        case BH_LOGICAL_XOR_REDUCE:
+        case BH_BITWISE_XOR_REDUCE: return true;
+        default: return false;
+    }
+}
+
+// The fold of a 1-D reduction of `n` elements: the largest divisor of n in [2, n / limit], or 1.
+int64_t reduce1d_fold(int64_t n, int64_t limit) {
+    for (int64_t i = n / limit; i > 1; --i)
+        if (n % i == 0) return i;
+    return 1;
+}
+
 } // namespace
 
 int expand(BhIR &bhir, const ExpandOptions &opt, BaseStore &created) {
@@ -87,6 +110,33 @@ int expand(BhIR &bhir, const ExpandOptions &opt, BaseStore &created) {
                 out.push_back(make(BH_SUBTRACT, {o, g, l}));
                 out.push_back(make(BH_FREE, {g}));
                 out.push_back(make(BH_FREE, {l}));
+                ++rewrites;
+                continue;
+            }
+        }
+        if (opt.reduce1d > 0 && reduce1d_opcode(instr.opcode) && instr.operand.size() == 3 &&
+            !instr.operand[1].isConstant() && instr.operand[1].ndim == 1) {
+            // out = reduce(x) over n elements -> t[n/f] = reduce over axis 0 of x viewed as [f, n/f];
+            // out = reduce(t); free t
+            const int64_t n = instr.operand[1].shape[0];
+            const int64_t fold = n * 2 < opt.reduce1d ? 1 : reduce1d_fold(n, opt.reduce1d);
+            if (fold >= 2) {
+                bh_view x = instr.operand[1];
+                const int64_t st = x.stride[0];
+                x.ndim = 2;
+                x.shape = {fold, n / fold};
+                x.stride = {st * (n / fold), st};
+                bh_view like;
+                like.ndim = 1;
+                like.shape = {n / fold};
+                const bh_view t = fresh_view(created, like, x.base->dtype());
+                bh_instruction first = make(instr.opcode, {t, x, constant_operand()});
+                first.constant = bh_constant(static_cast<int64_t>(0));
+                bh_instruction second = make(instr.opcode, {instr.operand[0], t, constant_operand()});
+                second.constant = bh_constant(static_cast<int64_t>(0));
+                out.push_back(first);
+                out.push_back(second);
+                out.push_back(make(BH_FREE, {t}));
                 ++rewrites;
                 continue;
             }

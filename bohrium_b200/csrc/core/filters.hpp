@@ -13,9 +13,15 @@
 //               a temporary freed right after its only use (exact: integers)
 //   muladd      `t1 = a*x; t2 = b*x; y = t1 +- t2` on integer arrays with t1, t2 temporaries
 //               used only there -> y = (a +- b)*x (exact: integers)
-// reduce1d (bcexp) and the reduction contraction (bccon) are off in the GPU stack and not
-// provided. Every rewrite keeps the results bit for bit except powk on floating-point data, whose
-// products may round differently from pow().
+//   reduce1d  (expand_reduce1d.cpp:31-80) with a thread limit L > 0: a reduction of a 1-D view
+//         of n >= L/2 elements -> the same reduction over axis 0 of the view reshaped to
+//         [f, n/f] into a new temporary, then over that temporary, where f is the largest divisor
+//         of n in [2, n/L]; no rewrite when there is none. Off (0) by default: the CUDA engine
+//         reduces 1-D arrays in one GRID_REDUCE kernel, and the split changes the floating-point
+//         summation order.
+// The reduction contraction (bccon) is off in the reference's configs and not provided. Every
+// rewrite keeps the results bit for bit except powk on floating-point data, whose products may
+// round differently from pow(), and reduce1d on floating-point sums and products.
 #pragma once
 
 #include <memory>
@@ -29,6 +35,7 @@ namespace filter {
 struct ExpandOptions {
     bool powk = true;
     bool sign = false;
+    int64_t reduce1d = 0; // thread limit of the 1-D reduction split; 0: off
 };
 struct ContractOptions {
     bool stupidmath = true;

@@ -1243,6 +1243,11 @@ constexpr int64_t kSplitMinChunk = 16;
 // Points from which LANE_REDUCE (C lanes of one CTA per point) fills the GPU well enough to be
 // preferred over SPLIT_REDUCE when the swept axis is contiguous.
 constexpr int64_t kLaneMinPoints = 148;
+// (point, lane) threads LANE_REDUCE aims at when it picks the lanes per point.
+#ifndef BH_LANE_TARGET
+#define BH_LANE_TARGET 600000
+#endif
+constexpr int64_t kLaneTargetThreads = BH_LANE_TARGET;
 
 // The swept sub-loop of `inner` when `inner` is [identity instructions] [swept innermost sub-loop]
 // [instructions], and the sub-loop's sweeps are reductions; nullptr otherwise.
@@ -1290,7 +1295,7 @@ int ilog2(int64_t x) {
 // Lanes per point of LANE_REDUCE: a power of two up to a CTA (256) chosen from the shapes alone.
 int64_t lane_count(int64_t points, int64_t len) {
     int64_t c = 1;
-    while (c < kThreads && points * c < kSplitTargetThreads && c * 4 <= len) c *= 2;
+    while (c < kThreads && points * c < kLaneTargetThreads && c * 4 <= len) c *= 2;
     return c;
 }
 

@@ -105,9 +105,11 @@ void *bhb_base_data(const bh_base *base);
 void *bhb_ir_bhir(bhb_ir *ir);
 /* Set the message returned by bhb_last_error() on this thread. */
 void bhb_set_last_error(const char *msg);
-/* Apply a bytecode filter of the filter components in place: "bcexp" (powk), "bcexp+sign",
- * "bccon" (stupidmath, collect, muladd). Returns the number of rewrites, -1 on error. (The filters
- * restate filter/bcexp/expander.cpp:42-87 and filter/bccon/contracter.cpp:46-52.) */
+/* Apply a bytecode filter of the filter components in place: "bcexp" (powk) with optional
+ * "+sign" and "+reduce1d=<thread limit>" (e.g. "bcexp+reduce1d=32000", the reference's GPU-stack
+ * setting), or "bccon" (stupidmath, collect, muladd). Returns the number of rewrites, -1 on error.
+ * (The filters restate filter/bcexp/expander.cpp:42-87, expand_reduce1d.cpp:31-80 and
+ * filter/bccon/contracter.cpp:46-52.) */
 int bhb_ir_filter(bhb_ir *ir, const char *name);
 /* Text listing of a decoded BhIR (opcode, operands with bases numbered by first appearance,
  * constant), valid until the next call on the same handle. */

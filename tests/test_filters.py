@@ -88,3 +88,26 @@ def test_muladd_combines_integer_products():
     counts, text = filter_text(_flush(prog), ("bccon",))
     lines = [l for l in text.splitlines() if int(l.split()[0]) != OP["FREE"]]
     assert len(lines) == 1 and lines[0].startswith(str(OP["MULTIPLY"])) and lines[0].endswith("= 5"), text
+
+
+def test_reduce1d_splits_long_1d_reductions():
+    """expand_reduce1d.cpp:31-80: with the GPU stack's thread limit 32000, a 1-D reduction of
+    2^20 elements becomes a [32, 32768] axis-0 reduction into a temporary plus the reduction of
+    the temporary (fold = largest divisor of n up to n/32000); short or prime-length ones stay."""
+    def prog(rt, n=1 << 20, name="ADD_REDUCE"):
+        x = bh.empty(rt, (n,), np.float64)
+        return [bh.reduce(name, x, 0)]
+    counts, text = filter_text(_flush(prog), ("bcexp+reduce1d=32000",))
+    assert counts == [1], text
+    lines = [line for line in text.splitlines() if line.strip()]
+    reds = [line for line in lines if int(line.split()[0]) == OP["ADD_REDUCE"]]
+    assert len(reds) == 2, text
+    assert "[0;32,32768;32768,1]" in reds[0], reds[0]
+    assert "[0;32768;1]" in reds[1], reds[1]
+    assert any(int(line.split()[0]) == OP["FREE"] for line in lines)
+    # 16000 <= n: split; below, or without a divisor in [2, n/L]: unchanged
+    for n, want in [(20_000, 0), (64_000, 1), (1_000_003, 0), (96_000, 1)]:
+        counts, _ = filter_text(_flush(lambda rt, n=n: prog(rt, n, "MAXIMUM_REDUCE")), ("bcexp+reduce1d=32000",))
+        assert counts == [want], n
+    counts, _ = filter_text(_flush(prog), ("bcexp",))
+    assert counts == [0]

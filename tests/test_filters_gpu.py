@@ -32,3 +32,20 @@ def test_filtered_stack_float_power(filtered):
     x = bh.array(rt, X)
     y = bh.binary("POWER", x, np.int64(5)).sum()
     np.testing.assert_allclose(float(y.numpy()), float(np.sum(X ** 5)), rtol=1e-12)
+
+
+def test_filtered_stack_reduce1d(monkeypatch):
+    """With the reference's GPU-stack setting reduce1d = 32000 the 1-D reductions reach the engine
+    as a [32, 32768] axis-0 reduction plus a 32768-element one: results within the float64
+    reduction tolerance of NumPy, integer and max results bit-exact."""
+    monkeypatch.setenv("BH_BCEXP_REDUCE1D", "32000")
+    ex = bh.NativeExecutor(stack="filtered_cuda")
+    rt = bh.Runtime(ex)
+    rng = np.random.default_rng(2)
+    X = rng.standard_normal(1 << 20)
+    I = rng.integers(-1000, 1000, 1 << 20).astype(np.int64)
+    x, i = bh.array(rt, X), bh.array(rt, I)
+    s, m, t = x.sum(), x.max(), i.sum()
+    np.testing.assert_allclose(float(s.numpy()), float(np.sum(X)), rtol=1e-12, atol=1e-9)
+    assert float(m.numpy()) == float(X.max())
+    assert int(t.numpy()) == int(I.sum())
