@@ -718,7 +718,26 @@ public:
 
     // Element index of view `v`: (sum of loop index x group stride) + view offset. The strided
     // part is written identically for all views of a stride group.
-    string index_expr(const bh_view &v, int hidden_axis = BH_MAXDIM, pair<int, int> axis_offset = {-1, 0}) {
+    // Views whose address is split into a pointer computed once outside the innermost loop (the
+    // schedule declares it) and that loop's term: view id -> pointer name. `hoist_axis` is the
+    // index of that loop.
+    map<int, string> hoisted;
+    int hoist_axis = -1;
+
+    // The term of loop index `axis` in the index of `v` ("0" for a broadcast axis).
+    string axis_term(const bh_view &v, int axis) {
+        const int vid = sym.view_id.at(v);
+        const int gid = sym.view_group.at(static_cast<size_t>(vid));
+        const vector<int64_t> &st = sym.stride_groups.at(static_cast<size_t>(gid));
+        if (axis >= v.ndim) return "0";
+        const int64_t stride = st.at(static_cast<size_t>(axis));
+        if (stride == 0) return "0";
+        if (stride == 1) return "i" + to_string(axis);
+        return "i" + to_string(axis) + " * p.g" + to_string(gid) + "_s" + to_string(axis);
+    }
+
+    string index_expr(const bh_view &v, int hidden_axis = BH_MAXDIM, pair<int, int> axis_offset = {-1, 0},
+                      int skip_axis = -1) {
         const int vid = sym.view_id.at(v);
         const int gid = sym.view_group.at(static_cast<size_t>(vid));
         if (v.is_scalar() || v.ndim == 0) return "(p.v" + to_string(vid) + "_o)";
@@ -732,7 +751,7 @@ public:
             int t = static_cast<int>(i);
             if (t >= hidden_axis) ++t;
             const int64_t stride = st.at(static_cast<size_t>(i));
-            if (stride == 0) continue;
+            if (stride == 0 || t == skip_axis) continue;
             if (any) ss << " + ";
             any = true;
             if (axis_offset.first == t) {
@@ -748,6 +767,10 @@ public:
     }
 
     string array_ref(const bh_view &v, int hidden_axis = BH_MAXDIM, pair<int, int> axis_offset = {-1, 0}) {
+        if (!opt.bounds_check && hidden_axis == BH_MAXDIM && axis_offset.first < 0 && !hoisted.empty()) {
+            auto it = hoisted.find(sym.view_id.at(v));
+            if (it != hoisted.end()) return it->second + "[" + axis_term(v, hoist_axis) + "]";
+        }
         const string idx = index_expr(v, hidden_axis, axis_offset);
         const int pid = sym.param_id.at(v.base);
         if (opt.bounds_check) {
@@ -1048,12 +1071,15 @@ extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME__(const __grid_c
 }
 extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME___batch(const P* __restrict__ items,
         const bh_i64* __restrict__ prefix, int nitems, bh_i64 total) {
-    // The parameters of the current item live in shared memory; consecutive work items of a CTA
-    // usually belong to the same item, which then needs neither a search nor a reload.
+    // Each CTA takes a contiguous range of the work items of all items, so consecutive work items
+    // of a CTA belong to the same item except at item boundaries. The parameters of the current
+    // item live in shared memory and are looked up and reloaded only at those boundaries.
     __shared__ P sp;
     int have = -1;
     bh_i64 have_lo = 0, have_hi = 0;
-    for (bh_i64 g = blockIdx.x; g < total; g += gridDim.x) {
+    const bh_i64 g_lo = (bh_i64)blockIdx.x * total / gridDim.x;
+    const bh_i64 g_hi = ((bh_i64)blockIdx.x + 1) * total / gridDim.x;
+    for (bh_i64 g = g_lo; g < g_hi; ++g) {
         if (g < have_lo || g >= have_hi) {
             int lo = 0, hi = nitems - 1;
             while (lo < hi) {
@@ -1151,6 +1177,34 @@ vector<bh_view> preloadable_views(const LoopB &inner, const LoopB &kernel, const
     return ret;
 }
 
+// Declare, for every array view read or written in the innermost loop `inner` (index i<axis>,
+// all higher loop indices defined), a pointer to the view's element at i<axis> = 0, and register
+// them with the emitter so that references inside the loop index the pointer by the loop term
+// only. Nothing is hoisted under bounds checking.
+void hoist_views(Emitter &em, const LoopB &inner, int axis, ostream &out, int ind) {
+    if (em.opt.bounds_check) return;
+    const string sp(static_cast<size_t>(ind), ' ');
+    for (const Block &b : inner._block_list) {
+        if (!b.isInstr()) return;
+    }
+    for (const InstrPtr &ip : jitk::all_instr(inner)) {
+        const bh_opcode op = ip->opcode;
+        if (bh_opcode_is_system(op) || op == BH_GATHER || op == BH_SCATTER || op == BH_COND_SCATTER) continue;
+        for (size_t o = 0; o < ip->operand.size(); ++o) {
+            const bh_view &v = ip->operand[o];
+            if (v.isConstant() || em.sym.temps.count(v.base) || v.ndim != axis + 1) continue;
+            if (o == 0 && bh_opcode_is_sweep(op)) continue;  // an accumulator, not an array
+            const int vid = em.sym.view_id.at(v);
+            if (em.hoisted.count(vid)) continue;
+            const string nm = "hp" + to_string(em.hoisted.size());
+            out << sp << cuda_type(v.base->dtype()) << "* __restrict__ " << nm << " = a" << em.sym.param_id.at(v.base)
+                << " + " << em.index_expr(v, BH_MAXDIM, {-1, 0}, axis) << ";\n";
+            em.hoisted[vid] = nm;
+        }
+    }
+    em.hoist_axis = axis;
+}
+
 // Emit the register arrays and the load loop of `views` for V elements per thread; element j has
 // index `idx_init(j)` (a statement defining the innermost loop index). With `guard` the loads
 // stop at the loop bound. Registers the replacements in `scope`.
@@ -1243,11 +1297,10 @@ constexpr int64_t kSplitMinChunk = 16;
 // Points from which LANE_REDUCE (C lanes of one CTA per point) fills the GPU well enough to be
 // preferred over SPLIT_REDUCE when the swept axis is contiguous.
 constexpr int64_t kLaneMinPoints = 148;
-// (point, lane) threads LANE_REDUCE aims at when it picks the lanes per point.
-#ifndef BH_LANE_TARGET
-#define BH_LANE_TARGET 600000
-#endif
-constexpr int64_t kLaneTargetThreads = BH_LANE_TARGET;
+// (point, lane) threads LANE_REDUCE aims at when it picks the lanes per point (fewer lanes per
+// point, with each CTA holding several neighbouring points, measured slower on the 4096^2 heat
+// stencil: 16-64 lanes took 1.6-2.1x the time of 256).
+constexpr int64_t kLaneTargetThreads = 600000;
 
 // The swept sub-loop of `inner` when `inner` is [identity instructions] [swept innermost sub-loop]
 // [instructions], and the sub-loop's sweeps are reductions; nullptr otherwise.
@@ -1366,6 +1419,8 @@ LaunchUnit lower_lane_reduce(const LoopB &loop, unsigned P, const CodegenOptions
     }
     const int sub_lid = sym.loop_id.at(&sub);
     const int64_t per_cta = kThreads / C;
+
+
     body << "__device__ void bh_work(const P &p, bh_i64 w) {\n";
     body << pointer_locals(sym);
     if (C > 32) {
@@ -1393,13 +1448,53 @@ LaunchUnit lower_lane_reduce(const LoopB &loop, unsigned P, const CodegenOptions
     {
         Scope scope;
         declare_chain_temps(em, sym, scope, chain, P, body, 8);
-        body << "/*@unroll@*/\n";
-        body << "        for (bh_i64 i" << P << " = lane; i" << P << " < p.n" << sub_lid << "; i" << P << " += " << C
-             << ") {\n";
-        Scope s1;
-        s1.parent = &scope;
-        em.write_body(sub, s1, 12);
-        body << "        }\n";
+        // Inputs that this kernel does not write are loaded for U strided iterations at once
+        // before any of them computes or stores: a store may alias a later load as far as the
+        // compiler can tell, so without this each iteration's loads wait for the previous one.
+        // Every lane still folds its elements in increasing order.
+        const vector<bh_view> pre = preloadable_views(sub, L, sym);
+        const int64_t U = pre.empty() ? 1 : (pre.size() <= 8 ? 4 : 2);
+        const string iv = "i" + to_string(P), nv = "p.n" + to_string(sub_lid);
+        hoist_views(em, sub, static_cast<int>(P), body, 8);
+        if (U > 1 && sub.size / C >= U) {
+            body << "/*@unroll@*/\n";
+            body << "        for (bh_i64 ib = lane; ib < " << nv << "; ib += " << C * U << ") {\n";
+            body << "            if (ib + " << C * (U - 1) << " < " << nv << ") {\n";
+            for (size_t k = 0; k < pre.size(); ++k)
+                body << "                " << cuda_type(pre[k].base->dtype()) << " pl" << k << "[" << U << "];\n";
+            body << "#pragma unroll\n";
+            body << "                for (int j = 0; j < " << U << "; ++j) {\n";
+            body << "                    const bh_i64 " << iv << " = ib + j * " << C << ";\n";
+            for (size_t k = 0; k < pre.size(); ++k)
+                body << "                    pl" << k << "[j] = " << em.array_ref(pre[k]) << ";\n";
+            body << "                }\n";
+            body << "#pragma unroll\n";
+            body << "                for (int j = 0; j < " << U << "; ++j) {\n";
+            body << "                    const bh_i64 " << iv << " = ib + j * " << C << ";\n";
+            Scope s1;
+            s1.parent = &scope;
+            for (size_t k = 0; k < pre.size(); ++k) s1.repl[ViewKey(pre[k])] = "pl" + to_string(k) + "[j]";
+            em.write_body(sub, s1, 20);
+            body << "                }\n";
+            body << "            } else {\n";
+            body << "                for (bh_i64 " << iv << " = ib; " << iv << " < " << nv << "; " << iv << " += " << C
+                 << ") {\n";
+            Scope s2;
+            s2.parent = &scope;
+            em.write_body(sub, s2, 20);
+            body << "                }\n";
+            body << "            }\n";
+            body << "        }\n";
+        } else {
+            body << "/*@unroll@*/\n";
+            body << "        for (bh_i64 " << iv << " = lane; " << iv << " < " << nv << "; " << iv << " += " << C << ") {\n";
+            Scope s1;
+            s1.parent = &scope;
+            em.write_body(sub, s1, 12);
+            body << "        }\n";
+        }
+        em.hoisted.clear();
+        em.hoist_axis = -1;
     }
     body << "    }\n";
     // Combine the C lanes of each point (every lane of the warp takes part; lanes of points past

@@ -158,3 +158,4 @@ def test_complex_programs_compile_for_every_schedule():
     _, units = plan(P.complex_chain_program(1 << 20))
     assert [u["sched"] for u in units] == ["grid_reduce"]
     assert {"flat", "grid_reduce", "split_reduce", "lane_reduce", "scan1d"} <= seen, seen
+

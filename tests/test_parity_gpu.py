@@ -271,6 +271,58 @@ def test_row_reductions_lane_schedule(gpu_rt, oracle_rt, rows, cols, dtype, op):
         assert_close(a, b, rtol, rtol, what)
 
 
+def _stencil_prog(host, rows, cols, dtype, op, offsets):
+    """dst[2:2+rows, 1:1+cols] = sum_k (k + 1) * x[2 + dr_k + i, 1 + dc_k + j]; returns the
+    reduction `op` of that sum over axis 1 and dst (the shape of the heat stencil)."""
+    def prog(rt):
+        x = bh.array(rt, host)
+        dst = bh.zeros(rt, host.shape, dtype)
+        acc = None
+        for k, (dr, dc) in enumerate(offsets):
+            term = x[2 + dr:2 + dr + rows, 1 + dc:1 + dc + cols] * dtype(k + 1)
+            acc = term if acc is None else acc + term
+        dst[2:2 + rows, 1:1 + cols] = acc
+        return [getattr(acc - x[2:2 + rows, 1:1 + cols], op)(axis=1), dst]
+    return prog
+
+
+@pytest.mark.parametrize("rows,cols,dtype,op,offsets", [
+    (1000, 1500, np.float64, "sum", [(0, 0), (-1, 0), (1, 0), (0, -1), (0, 1)]),
+    (700, 4000, np.float32, "max", [(-2, 0), (-1, 0), (0, 0), (1, 0), (2, 0)]),
+    (513, 300, np.float32, "sum", [(0, 0), (2, 0), (0, 1)]),
+    (2000, 4094, np.float32, "max", [(0, 0), (-1, 0), (1, 0), (0, -1), (0, 1)]),
+    (300, 4096, np.float64, "min", [(-1, -1), (0, 0), (1, 1), (-1, 1), (1, -1)]),
+    (160, 257, np.float64, "sum", [(1, 0), (-1, 0)]),
+])
+def test_stencil_rows_lane_schedule(gpu_rt, oracle_rt, rows, cols, dtype, op, offsets):
+    """Row reductions of stencils (shifted views of one array, the heat step's shape) on the
+    LANE_REDUCE schedule with its inputs preloaded, against the oracle."""
+    host = np.random.default_rng(rows + cols).random((rows + 4, cols + 2)).astype(dtype)
+    g, o = both(gpu_rt, oracle_rt, _stencil_prog(host, rows, cols, dtype, op, offsets))
+    rtol = reduce_tol(dtype)
+    assert_close(g[0], o[0], rtol, rtol, "reduce")
+    assert_close(g[1], o[1], *float_tol(dtype), "stencil")
+
+
+def test_stencil_rows_grouped_launch_is_bit_identical(gpu_executor):
+    """Two independent stencils in one flush share a kernel and level, so batch mode "grouped"
+    runs them as one grouped launch; results equal the plain launches' bit for bit."""
+    rt = bh.Runtime(gpu_executor)
+    offsets = [(0, 0), (-1, 0), (1, 0), (0, -1), (0, 1)]
+    hosts = [np.random.default_rng(s).random((604, 1002)).astype(np.float32) for s in (1, 2)]
+    res = {}
+    try:
+        for mode in ["off", "grouped"]:
+            gpu_executor.message(f"CUDA: batch {mode}")
+            outs = []
+            for h in hosts:
+                outs += _stencil_prog(h, 600, 1000, np.float32, "sum", offsets)(rt)
+            res[mode] = [o.numpy().tobytes() for o in outs]
+    finally:
+        gpu_executor.message("CUDA: batch off")
+    assert res["off"] == res["grouped"]
+
+
 def test_graph_replay_is_bit_identical(gpu_executor):
     """Batch mode "graph": a re-executed flush is captured into a CUDA graph (grouped launches,
     arrays created and freed inside the flush parked) and replayed; results equal the plain
