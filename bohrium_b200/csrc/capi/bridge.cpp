@@ -117,8 +117,11 @@ BhIR *decode(const int64_t *w, int64_t n, bh_base *const *syncs, int64_t nsyncs,
             j += 2;
         }
     }
+    bool builtin = true;
+    for (const bh_instruction &instr : list) builtin = builtin && instr.opcode <= BH_MAX_OPCODE_ID;
     set<bh_base *> s(syncs, syncs + nsyncs);
     BhIR *ir = new BhIR(std::move(list), std::move(s), nrepeats, cond);
+    ir->_plain = nslide == 0 && builtin;
     if (nslide == 0) {
         // The handle is immutable: fingerprint its encoding once so that an engine can recognise
         // the repeated flush (sliding views change between executions, so they get none).

@@ -1224,7 +1224,7 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
 void EngineCUDA::handleExtmethod(BhIR *bhir) {
     // Only a list that contains extension methods needs splitting (and copying).
     bool any = false;
-    if (!comp.extmethods.empty() || !comp.child_extmethods.empty()) {
+    if (!bhir->_plain && (!comp.extmethods.empty() || !comp.child_extmethods.empty())) {
         for (const bh_instruction &instr : bhir->instr_list) {
             if (comp.extmethods.count(instr.opcode) || comp.child_extmethods.count(instr.opcode)) {
                 any = true;
@@ -1317,7 +1317,7 @@ void EngineCUDA::execute(BhIR *bhir) {
             copyToHost({cond}, false);
             if (cond->getDataPtr() != nullptr && !static_cast<bool *>(cond->getDataPtr())[0]) break;
         }
-        slide_views(bhir);
+        if (!bhir->_plain) slide_views(bhir);  // a plain list has no sliding views
     }
 }
 

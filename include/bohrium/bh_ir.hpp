@@ -20,6 +20,10 @@ public:
     // the instruction list; the caller must reset it to 0 if it changes the BhIR. (Not part of the
     // reference's BhIR; callers that never set it see no difference.)
     uint64_t _fingerprint = 0;
+    // Set by a caller that knows the list has no sliding views and no extension-method opcodes
+    // (ids above BH_MAX_OPCODE_ID): an engine can then skip the per-execution walks over every
+    // instruction that look for them. False (unknown) by default; not part of the reference.
+    bool _plain = false;
 
     BhIR(std::vector<bh_instruction> instr_list, std::set<bh_base *> syncs, uint64_t nrepeats = 1,
          bh_base *repeat_condition = nullptr)
