@@ -323,6 +323,45 @@ def test_stencil_rows_grouped_launch_is_bit_identical(gpu_executor):
     assert res["off"] == res["grouped"]
 
 
+def test_matrix_full_reductions_grouped_and_graph(gpu_executor, oracle_rt):
+    """Full reductions of matrices (a row or column reduction, then a small 1-D reduction of its
+    results). Equal shapes in one flush share kernels and levels, so batch modes "grouped" and
+    "graph" run them as grouped launches. Every mode gives the same bits, on every execution,
+    within the reduction tolerance of the oracle."""
+    shapes = [(3000, 257), (4096, 300), (5000, 40), (700, 1500)]
+    hosts = [np.random.default_rng(k).random(s) for k, s in enumerate(shapes)]
+
+    keep = []  # the inputs stay alive, so the compiled flush does not free them
+
+    def prog(rt):
+        outs = []
+        for h in hosts * 2:  # pairs of equal shapes: the same kernel twice in one level
+            x = bh.array(rt, h)
+            keep.append(x)
+            outs += [(x * 2.0 + 1.0).sum(), (x - 0.5).max()]
+        return outs
+    want = run(oracle_rt, prog)
+    rt = bh.Runtime(gpu_executor)
+    res = {}
+    try:
+        for mode in ["off", "grouped", "graph"]:
+            gpu_executor.message(f"CUDA: batch {mode}")
+            outs = prog(rt)
+            ir = gpu_executor.compile(rt.take())
+            runs = []
+            for _ in range(3):
+                ir.execute()
+                runs.append([gpu_executor.peek(o.base).tobytes() for o in outs])
+            assert runs[0] == runs[1] == runs[2], mode
+            res[mode] = runs[0]
+            got = [gpu_executor.peek(o.base) for o in outs]
+            for g, w in zip(got, want):
+                assert_close(g.reshape(w.shape), w, 1e-12, 1e-12, mode)
+    finally:
+        gpu_executor.message("CUDA: batch off")
+    assert res["off"] == res["grouped"] == res["graph"]
+
+
 def test_graph_replay_is_bit_identical(gpu_executor):
     """Batch mode "graph": a re-executed flush is captured into a CUDA graph (grouped launches,
     arrays created and freed inside the flush parked) and replayed; results equal the plain
