@@ -1377,6 +1377,97 @@ bool swept_axis_contiguous(const LoopB &sub, int rank) {
 // then the C lane partials are combined by a fixed shuffle tree (xor C/2 .. 1 within a warp; for
 // C > 32 the warp sums are folded in warp order), and lane 0 runs the instructions that follow.
 // No scratch memory and no counters: one pass.
+// Stencil groups for LANE_REDUCE with one point axis and a CTA per point: read-only 2-D views of
+// one base with equal strides, unit column stride and a row stride of at least 64 elements, whose
+// starts differ by dk whole rows and dm (|dm| <= 8) columns, e.g. x[i-1, j], x[i, j-1], x[i, j],
+// x[i, j+1], x[i+1, j]. Member i reads, at point i0 and column j, element
+// s0 + (i0 + dk_i) * S0 + dm_i + j of the base, so the rows a CTA needs for consecutive points
+// overlap and can be staged once in shared memory.
+// Rows a staging CTA keeps in flight beyond the ones the current point reads (on the 4096^2
+// heat stencil, 2 and 3 took 3 % longer than 1: fewer CTAs fit in shared memory).
+constexpr int64_t kStagePrefetch = 1;
+
+struct StencilMember {
+    size_t view;  // index in the view list
+    int64_t dk, dm;
+};
+struct StencilGroup {
+    vector<StencilMember> m;
+    int64_t kmin = 0, kspan = 0, mmin = 0, mspan = 0;
+};
+
+StencilGroup stencil_group(const vector<bh_view> &views, const Symbols &sym) {
+    StencilGroup best;
+    for (size_t a = 0; a < views.size(); ++a) {
+        const bh_view &va = views[a];
+        if (va.ndim != 2 || va.stride[1] != 1 || va.stride[0] < 64 || va.hasSlide()) continue;
+        const int ga = sym.view_group.at(static_cast<size_t>(sym.view_id.at(va)));
+        const int64_t S0 = va.stride[0];
+        StencilGroup g;
+        for (size_t b = 0; b < views.size(); ++b) {
+            const bh_view &vb = views[b];
+            if (vb.base != va.base || vb.ndim != 2 || vb.hasSlide() ||
+                sym.view_group.at(static_cast<size_t>(sym.view_id.at(vb))) != ga)
+                continue;
+            const int64_t d = vb.start - va.start;
+            const int64_t dk = d >= 0 ? (d + S0 / 2) / S0 : -((-d + S0 / 2) / S0);
+            const int64_t dm = d - dk * S0;
+            if (dm < -8 || dm > 8) continue;
+            g.m.push_back({b, dk, dm});
+        }
+        int64_t kmax = g.m[0].dk, mmax = g.m[0].dm;
+        g.kmin = kmax;
+        g.mmin = mmax;
+        for (const StencilMember &x : g.m) {
+            g.kmin = min(g.kmin, x.dk);
+            kmax = max(kmax, x.dk);
+            g.mmin = min(g.mmin, x.dm);
+            mmax = max(mmax, x.dm);
+        }
+        g.kspan = kmax - g.kmin;
+        g.mspan = mmax - g.mmin;
+        if (g.kspan < 1 || g.kspan > 4) continue;  // no row shared between points, or too many rows
+        if (g.m.size() > best.m.size()) best = g;
+    }
+    return best;
+}
+
+// Asynchronous global -> shared copies (cp.async, completed in commit groups) for staged rows.
+const char *kStagePrelude = R"CUDA(
+__device__ __forceinline__ void bh_cp16(void *s, const void *g) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"((unsigned)__cvta_generic_to_shared(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void bh_cp8(void *s, const void *g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"((unsigned)__cvta_generic_to_shared(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void bh_cp4(void *s, const void *g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"((unsigned)__cvta_generic_to_shared(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void bh_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void bh_cp_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
+__device__ __forceinline__ void bh_cp_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// Stage `nelem` elements starting at `src` into dst[pre ...] (dst 16-byte aligned, src - pre a
+// 16-byte boundary): whole 16-byte chunks in one copy, the partial chunks at either end element
+// by element. Nothing outside [src, src + nelem) is read.
+template <typename T> __device__ __forceinline__ void bh_stage_row(T *dst, const T *src, bh_i64 nelem, int pre) {
+    const char *g = (const char *)src - pre * (int)sizeof(T);
+    char *d = (char *)dst;
+    const bh_i64 b_lo = (bh_i64)pre * (bh_i64)sizeof(T), b_hi = b_lo + nelem * (bh_i64)sizeof(T);
+    const bh_i64 nchunks = (b_hi + 15) / 16;
+    for (bh_i64 c = threadIdx.x; c < nchunks; c += blockDim.x) {
+        const bh_i64 b0 = c * 16;
+        if (b0 >= b_lo && b0 + 16 <= b_hi) {
+            bh_cp16(d + b0, g + b0);
+        } else {
+            for (bh_i64 b = b0 > b_lo ? b0 : b_lo; b < b0 + 16 && b < b_hi; b += (bh_i64)sizeof(T)) {
+                if (sizeof(T) == 4) bh_cp4(d + b, g + b);
+                else bh_cp8(d + b, g + b);
+            }
+        }
+    }
+}
+)CUDA";
+
 LaunchUnit lower_lane_reduce(const LoopB &loop, unsigned P, const CodegenOptions &opt) {
     LaunchUnit u;
     u.sched = Sched::LANE_REDUCE;
@@ -1544,7 +1635,156 @@ LaunchUnit lower_lane_reduce(const LoopB &loop, unsigned P, const CodegenOptions
             body << "    " << em.array_ref(reds[k]->operand[0], reds[k]->sweep_axis()) << " = pacc" << k << ";\n";
         }
     }
-    body << "}\n" << kWrappers;
+    body << "}\n";
+
+    // Staged rows: with one point axis, a CTA per point and a stencil group among the read-only
+    // views, each CTA walks a contiguous range of points (rows) and keeps the group's rows in a
+    // ring of shared-memory buffers filled by asynchronous copies one row ahead, so every base
+    // row is read once per CTA and the copies overlap the computation. The lanes fold the same
+    // elements in the same order as bh_work. A kernel-side check (layout, view offsets, bounds)
+    // falls back to bh_work for launches the staging does not fit.
+    bool staged = false;
+    if (P == 1 && C == kThreads && !opt.bounds_check) {
+        const vector<bh_view> pre = preloadable_views(sub, L, sym);
+        const StencilGroup g = stencil_group(pre, sym);
+        const bh_view *v0 = g.m.empty() ? nullptr : &pre[g.m[0].view];
+        const int64_t es = v0 ? bh_type_size(v0->base->dtype()) : 0;
+        const int64_t n = sub.size, U = (n + C - 1) / C, F = n / C;
+        const int64_t nrow = n + g.mspan, CE = es > 0 ? 16 / es : 1, NB = g.kspan + 1 + kStagePrefetch;
+        const int64_t RS = (nrow + CE - 1 + CE - 1) / CE * CE;
+        const int64_t smem = NB * RS * es;
+        if (v0 != nullptr && (es == 4 || es == 8) && U <= 16 && smem <= 160 * 1024) {
+            staged = true;
+            const string T = cuda_type(v0->base->dtype());
+            const int gid = sym.view_group.at(static_cast<size_t>(sym.view_id.at(*v0)));
+            const int vid0 = sym.view_id.at(*v0);
+            const int pid = sym.param_id.at(v0->base);
+            const string nv = "p.n" + to_string(sub_lid), S0 = "p.g" + to_string(gid) + "_s0";
+            ParamField fe{ParamField::I64};
+            fe.i64 = v0->base->nelem();
+            pl.add(fe, "bh_i64", "stage_nelem");
+            body << "// bh_dynamic_shared_bytes: " << smem << "\n";
+            body << kStagePrelude;
+            // Launch-time check: the layout the staging assumes holds for these parameters, and
+            // every staged row lies inside the base.
+            body << "__device__ __forceinline__ bool bh_stage_ok(const P &p, bh_i64 lo, bh_i64 hi) {\n";
+            body << "    const bh_i64 S0 = " << S0 << ";\n";
+            body << "    if (S0 < " << nrow << " || (S0 * " << es << ") % 16 != 0 || " << nv << " != " << n
+                 << ") return false;\n";
+            for (const StencilMember &x : g.m) {
+                const int vid = sym.view_id.at(pre[x.view]);
+                body << "    if (p.v" << vid << "_o - p.v" << vid0 << "_o != " << x.dk << "LL * S0 + (" << x.dm
+                     << "LL)) return false;\n";
+            }
+            body << "    const bh_i64 first = p.v" << vid0 << "_o + (lo + (" << g.kmin << "LL)) * S0 + (" << g.mmin
+                 << "LL);\n";
+            body << "    const bh_i64 last = p.v" << vid0 << "_o + (hi - 1 + (" << g.kmin + g.kspan << "LL)) * S0 + ("
+                 << g.mmin << "LL) + " << nrow << ";\n";
+            body << "    return first >= 0 && last <= p.stage_nelem;\n";
+            body << "}\n";
+            body << "__device__ void bh_work_staged(const P &p, bh_i64 lo, bh_i64 hi) {\n";
+            body << "    extern __shared__ __align__(16) unsigned char bh_dyn[];\n";
+            body << "    " << T << "* ring = (" << T << "*)bh_dyn;\n";
+            body << pointer_locals(sym);
+            for (size_t k = 0; k < reds.size(); ++k)
+                body << "    __shared__ " << ctypes[k] << " wsum" << k << "[2][" << kThreads / 32 << "];\n";
+            body << "    const int lane = threadIdx.x;\n";
+            body << "    const bh_i64 S0 = " << S0 << ";\n";
+            body << "    const " << T << "* rows0 = a" << pid << " + (p.v" << vid0 << "_o + (" << g.kmin << "LL) * S0 + ("
+                 << g.mmin << "LL));\n";
+            body << "    const int pre = (int)(((unsigned long long)(rows0 + lo * S0) & 15ULL) / " << es << ");\n";
+            body << "    const bh_i64 rend = hi + " << g.kspan << ";\n";
+            body << "    for (int b = 0; b < " << NB << "; ++b) {\n";
+            body << "        const bh_i64 r = lo + b;\n";
+            body << "        if (r < rend) bh_stage_row(ring + (r % " << NB << ") * " << RS << ", rows0 + r * S0, (bh_i64)"
+                 << nrow << ", pre);\n";
+            body << "        bh_cp_commit();\n";
+            body << "    }\n";
+            body << "    for (bh_i64 pt = lo; pt < hi; ++pt) {\n";
+            body << "        bh_cp_wait<" << kStagePrefetch << ">();  // all but the newest prefetched rows have landed\n";
+            body << "        __syncthreads();\n";
+            body << "        const bh_i64 i0 = pt;\n";
+            for (size_t k = 0; k < reds.size(); ++k)
+                body << "        " << ctypes[k] << " pacc" << k << " = " << idents[k] << ";\n";
+            for (size_t k = 0; k < g.m.size(); ++k)
+                body << "        const " << T << "* sr" << k << " = ring + ((pt + " << g.m[k].dk - g.kmin << ") % " << NB
+                     << ") * " << RS << " + pre + " << g.m[k].dm - g.mmin << ";\n";
+            {
+                Scope scope;
+                declare_chain_temps(em, sym, scope, chain, P, body, 8);
+                body << (U <= 16 ? "#pragma unroll\n" : "#pragma unroll 4\n");
+                body << "        for (int j = 0; j < " << U << "; ++j) {\n";
+                body << "            const bh_i64 i1 = lane + j * " << C << ";\n";
+                body << "            if (j < " << F << " || i1 < " << nv << ") {\n";
+                Scope s1;
+                s1.parent = &scope;
+                for (size_t k = 0; k < g.m.size(); ++k) s1.repl[ViewKey(pre[g.m[k].view])] = "sr" + to_string(k) + "[i1]";
+                em.write_body(sub, s1, 16);
+                body << "            }\n";
+                body << "        }\n";
+            }
+            for (size_t k = 0; k < reds.size(); ++k) {
+                body << "#pragma unroll\n";
+                body << "        for (int m = 16; m >= 1; m >>= 1) { const " << ctypes[k] << " o = bh_shfl_xor(pacc" << k
+                     << ", m); pacc" << k << " = " << reduce_expr(reds[k]->opcode, "pacc" + to_string(k), "o") << "; }\n";
+                body << "        if ((threadIdx.x & 31) == 0) wsum" << k << "[pt & 1][threadIdx.x >> 5] = pacc" << k << ";\n";
+            }
+            body << "        __syncthreads();  // also: every thread is done with the oldest row's buffer\n";
+            body << "        const bh_i64 rnext = pt + " << NB << ";\n";
+            body << "        if (rnext < rend) bh_stage_row(ring + (rnext % " << NB << ") * " << RS
+                 << ", rows0 + rnext * S0, (bh_i64)" << nrow << ", pre);\n";
+            body << "        bh_cp_commit();\n";
+            body << "        if (lane == 0) {\n";
+            for (size_t k = 0; k < reds.size(); ++k) {
+                body << "            pacc" << k << " = wsum" << k << "[pt & 1][0];\n";
+                body << "            for (int j = 1; j < " << kThreads / 32 << "; ++j) pacc" << k << " = "
+                     << reduce_expr(reds[k]->opcode, "pacc" + to_string(k), "wsum" + to_string(k) + "[pt & 1][j]")
+                     << ";\n";
+            }
+            {
+                Scope scope;
+                declare_chain_temps(em, sym, scope, chain, P - 1, body, 12);
+                for (const bh_base *b : em.sorted_temps(inner)) {
+                    if (sym.temps.count(b) && !scope.is_tmp(b)) {
+                        scope.tmps.insert(b);
+                        body << "            " << cuda_type(b->dtype()) << " t" << sym.base_index(b) << ";\n";
+                    }
+                }
+                bool after = false;
+                for (const Block &b : inner._block_list) {
+                    if (!b.isInstr()) {
+                        after = true;
+                        continue;
+                    }
+                    if (after) em.write_instr(*b.getInstr(), scope, 12);
+                }
+                for (size_t k = 0; k < reds.size(); ++k) {
+                    if (sym.temps.count(reds[k]->operand[0].base)) continue;
+                    body << "            " << em.array_ref(reds[k]->operand[0], reds[k]->sweep_axis()) << " = pacc" << k
+                         << ";\n";
+                }
+            }
+            body << "        }\n";
+            body << "    }\n";
+            body << "    bh_cp_wait0();  // no copy in flight when the CTA leaves\n";
+            body << "}\n";
+            string wrappers = kWrappers;
+            const string loop = "    for (bh_i64 w = blockIdx.x; w < p.work; w += gridDim.x) bh_work(p, w);\n";
+            const size_t at = wrappers.find(loop);
+            if (at == string::npos) throw runtime_error("lower_lane_reduce(): wrapper template changed");
+            wrappers.replace(at, loop.size(),
+                             "    // a contiguous range of points (rows) per CTA\n"
+                             "    const bh_i64 lo = (bh_i64)blockIdx.x * p.work / gridDim.x;\n"
+                             "    const bh_i64 hi = ((bh_i64)blockIdx.x + 1) * p.work / gridDim.x;\n"
+                             "    if (lo < hi && bh_stage_ok(p, lo, hi)) {\n"
+                             "        bh_work_staged(p, lo, hi);\n"
+                             "    } else {\n"
+                             "        for (bh_i64 w = lo; w < hi; ++w) bh_work(p, w);\n"
+                             "    }\n");
+            body << wrappers;
+        }
+    }
+    if (!staged) body << kWrappers;
     u.fields = pl.fields;
     u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
     u.elements = points * sub.size;

@@ -64,6 +64,7 @@ struct DeviceApi {
     CUresult (*cuOccupancyMaxActiveBlocksPerMultiprocessor)(int *, CUfunction, int, size_t) = nullptr;
     CUresult (*cuGetErrorString)(CUresult, const char **) = nullptr;
     CUresult (*cuFuncGetAttribute)(int *, CUfunction_attribute, CUfunction) = nullptr;
+    CUresult (*cuFuncSetAttribute)(CUfunction, CUfunction_attribute, int) = nullptr;
 
     template <typename F>
     void get(const char *name, F &fp) {
@@ -80,6 +81,7 @@ struct DeviceApi {
         get("cuOccupancyMaxActiveBlocksPerMultiprocessor", cuOccupancyMaxActiveBlocksPerMultiprocessor);
         get("cuGetErrorString", cuGetErrorString);
         get("cuFuncGetAttribute", cuFuncGetAttribute);
+        get("cuFuncSetAttribute", cuFuncSetAttribute);
     }
     void ck(CUresult r, const char *what) const {
         if (r != CUDA_SUCCESS) {
@@ -481,7 +483,21 @@ vector<char> EngineCUDA::cubin_for(const string &name, const string &source, int
     return cubin;
 }
 
-EngineCUDA::Compiled::Variant EngineCUDA::load_variant(const vector<char> &cubin, const string &name, int maxrreg) {
+// Dynamic shared memory a kernel source asks for: the value of its "// bh_dynamic_shared_bytes: N"
+// line (0 without one). Only the plain kernel uses it; the grouped-launch wrapper does not.
+int EngineCUDA::dynamic_shared_bytes(const string &source) {
+    const string key = "// bh_dynamic_shared_bytes: ";
+    const size_t at = source.find(key);
+    return at == string::npos ? 0 : atoi(source.c_str() + at + key.size());
+}
+
+unsigned EngineCUDA::shared_bytes_of(void *fn) const {
+    auto it = fn_shared.find(fn);
+    return it == fn_shared.end() ? 0u : it->second;
+}
+
+EngineCUDA::Compiled::Variant EngineCUDA::load_variant(const vector<char> &cubin, const string &name, int maxrreg,
+                                                       int dyn_smem) {
     CUmodule mod;
     api->ck(api->cuModuleLoadData(&mod, cubin.data()), "cuModuleLoadData");
     Compiled::Variant v;
@@ -490,7 +506,13 @@ EngineCUDA::Compiled::Variant EngineCUDA::load_variant(const vector<char> &cubin
     api->ck(api->cuModuleGetFunction(&fb, mod, (name + "_batch").c_str()), "cuModuleGetFunction(batch)");
     v.fn = reinterpret_cast<void *>(f);
     v.fn_batch = reinterpret_cast<void *>(fb);
-    api->ck(api->cuOccupancyMaxActiveBlocksPerMultiprocessor(&v.occ, f, kThreads, 0), "cuOccupancy");
+    if (dyn_smem > 0) {
+        api->ck(api->cuFuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, dyn_smem),
+                "cuFuncSetAttribute(dynamic shared memory)");
+        fn_shared[v.fn] = static_cast<unsigned>(dyn_smem);
+    }
+    api->ck(api->cuOccupancyMaxActiveBlocksPerMultiprocessor(&v.occ, f, kThreads, static_cast<size_t>(dyn_smem)),
+            "cuOccupancy");
     api->ck(api->cuOccupancyMaxActiveBlocksPerMultiprocessor(&v.occ_batch, fb, kThreads, 0), "cuOccupancy");
     api->ck(api->cuFuncGetAttribute(&v.regs, CU_FUNC_ATTRIBUTE_NUM_REGS, f), "cuFuncGetAttribute");
     v.occ = max(v.occ, 1);
@@ -527,7 +549,7 @@ EngineCUDA::Compiled *EngineCUDA::compiled_for(const LaunchUnit &u) {
     Compiled c;
     c.name = u.name;
     c.source = u.source;
-    c.variants.push_back(load_variant(cubin, u.name, 0));
+    c.variants.push_back(load_variant(cubin, u.name, 0, dynamic_shared_bytes(u.source)));
     // A register cap chosen by an earlier tuning run of this source.
     auto tc = tune_choices.find(h);
     if (tc != tune_choices.end()) {
@@ -676,7 +698,8 @@ void EngineCUDA::launch_plain(const PlanUnit &pu, const vector<bh_base *> &bases
     record_begin(rec, e0);
     busy_begin();
     api->ck(api->cuLaunchKernel(reinterpret_cast<CUfunction>(pu.compiled->fn), static_cast<unsigned>(grid), 1, 1,
-                                kThreads, 1, 1, 0, static_cast<CUstream>(_stream), args, nullptr),
+                                kThreads, 1, 1, shared_bytes_of(pu.compiled->fn), static_cast<CUstream>(_stream), args,
+                                nullptr),
             "cuLaunchKernel");
     busy_end();
     record_end(rec, e0);
@@ -686,7 +709,8 @@ void EngineCUDA::launch_plain(const PlanUnit &pu, const vector<bh_base *> &bases
 
 int EngineCUDA::launch_raw(void *fn, int64_t grid, void **args) {
     return static_cast<int>(api->cuLaunchKernel(reinterpret_cast<CUfunction>(fn), static_cast<unsigned>(grid), 1, 1,
-                                                kThreads, 1, 1, 0, static_cast<CUstream>(_stream), args, nullptr));
+                                                kThreads, 1, 1, shared_bytes_of(fn), static_cast<CUstream>(_stream),
+                                                args, nullptr));
 }
 
 void EngineCUDA::launch_batched(const vector<const PlanUnit *> &group, const vector<bh_base *> &bases,

@@ -174,7 +174,12 @@ private:
     std::unordered_map<uint64_t, Compiled> functions;
     std::unordered_map<uint64_t, std::vector<char>> ahead;
     std::string disk_cache_path(const std::string &source, int maxrreg = 0) const; // "" without a cache dir
-    Compiled::Variant load_variant(const std::vector<char> &cubin, const std::string &name, int maxrreg);
+    Compiled::Variant load_variant(const std::vector<char> &cubin, const std::string &name, int maxrreg,
+                                   int dyn_smem = 0);
+    // Dynamic shared memory of the plain kernels that need it (by CUfunction), used by every launch.
+    std::unordered_map<void *, unsigned> fn_shared;
+    unsigned shared_bytes_of(void *fn) const;
+    static int dynamic_shared_bytes(const std::string &source);
     std::vector<char> cubin_for(const std::string &name, const std::string &source, int maxrreg);
     // Autotuning of plain launches (tune.cpp)
     bool tune_launch(Compiled &c, const LaunchUnit &u, int64_t work, void **args);

@@ -62,7 +62,7 @@ EngineCUDA::Compiled::Variant EngineCUDA::make_variant(const Compiled &c, int ma
         for (size_t pos = src.find(kUnrollMarker); pos != string::npos; pos = src.find(kUnrollMarker, pos))
             src.replace(pos, sizeof(kUnrollMarker) - 1, pragma);
     }
-    Compiled::Variant v = load_variant(cubin_for(c.name, src, maxrreg), c.name, maxrreg);
+    Compiled::Variant v = load_variant(cubin_for(c.name, src, maxrreg), c.name, maxrreg, dynamic_shared_bytes(c.source));
     v.unroll = unroll;
     return v;
 }

@@ -159,3 +159,20 @@ def test_complex_programs_compile_for_every_schedule():
     assert [u["sched"] for u in units] == ["grid_reduce"]
     assert {"flat", "grid_reduce", "split_reduce", "lane_reduce", "scan1d"} <= seen, seen
 
+
+
+def test_heat_step_stages_stencil_rows_in_shared_memory():
+    """The heat step's five shifted views of one grid form a stencil group: the lane kernel stages
+    grid rows in a ring of shared-memory buffers with asynchronous copies (one row ahead) and asks
+    for the ring as dynamic shared memory, with a launch-time check that falls back to the plain
+    lane code."""
+    def prog(rt):
+        a, b = bh.empty(rt, (4096, 4096), np.float32), bh.empty(rt, (4096, 4096), np.float32)
+        return [W.heat_step(a, b)]
+    res, units = plan(prog)
+    lane = [u for u in units if u["sched"] == "lane_reduce"]
+    assert len(lane) == 1
+    src = lane[0]["source"]
+    assert "bh_work_staged(p, lo, hi)" in src and "bh_stage_ok(p, lo, hi)" in src
+    assert "// bh_dynamic_shared_bytes: 65600" in src  # 4 rows of 4,100 floats
+    assert "cp.async.cg.shared.global" in src
