@@ -35,6 +35,11 @@ sys.path.insert(0, ROOT)
 METRIC = "flush wall-time & HBM GB/s (%peak): batched+learned vs plain ve/cuda; vs ve/openmp"
 BS_OPTIONS = 10_000_000
 BS_ITERS = 10
+# DRAM bytes (read + written) per option of one Black-Scholes kernel launch, from an ncu capture
+# of a 6,000,000-option launch (dram__bytes_read.sum 144.08 MB + dram__bytes_write.sum 3.48 MB;
+# inputs of 144 MB, larger than L2): one pass over the three inputs plus the tile partials, so
+# the traffic grows in proportion to the options and is scaled to the launch's option count.
+BS_TRAFFIC_PER_OPTION = (144_082_176 + 3_477_504) / 6_000_000
 
 
 def peaks():
@@ -229,7 +234,9 @@ def run_ours(args, world, rank, local):
     avg_kernel_ms = statistics.mean(kernel_ms) if kernel_ms else dev_ms / args.steps / BS_ITERS
     achieved = bs_bytes(n) / (avg_kernel_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                "frac": round(achieved / peak, 4), "traffic": round(BS_TRAFFIC_PER_OPTION * n),
+                "traffic_source": "ncu DRAM bytes of a 6e6-option launch, scaled to the launch's options",
+                "peak_kind": peak_kind,
                 "kernel": "bh_grid_reduce (Black-Scholes flush)", "kernel_ms": round(avg_kernel_ms, 5),
                 "algorithmic_bytes_per_launch": bs_bytes(n)}
     del irs, outs, inputs
