@@ -1966,6 +1966,50 @@ string block_reduce_fn(const string &ctype, const string &fname, bh_opcode op, c
     return ss.str();
 }
 
+// Block reduction of K values per thread for several reductions at once: every reduction gets
+// the tree of bh_block_reduce_k, but all share one pair of barriers (each has its own region of
+// `sm`, at `offsets` bytes).
+string block_reduce_all_fn(const vector<string> &ctypes, const vector<bh_opcode> &ops, const vector<string> &idents,
+                           const vector<int64_t> &offsets, int K) {
+    stringstream ss;
+    ss << "__device__ __forceinline__ void bh_block_reduce_all(";
+    for (size_t r = 0; r < ctypes.size(); ++r) ss << ctypes[r] << " (&v" << r << ")[" << K << "], ";
+    ss << "unsigned char *sm) {\n";
+    for (size_t r = 0; r < ctypes.size(); ++r)
+        ss << "    " << ctypes[r] << " *s" << r << " = (" << ctypes[r] << " *)(sm + " << offsets[r] << ");\n";
+    ss << "#pragma unroll\n";
+    ss << "    for (int k = 0; k < " << K << "; ++k) {\n";
+    for (size_t r = 0; r < ctypes.size(); ++r) {
+        ss << "#pragma unroll\n";
+        ss << "        for (int m = 16; m >= 1; m >>= 1) { const " << ctypes[r] << " o = bh_shfl_xor(v" << r << "[k], m); v"
+           << r << "[k] = " << reduce_expr(ops[r], "v" + to_string(r) + "[k]", "o") << "; }\n";
+    }
+    ss << "    }\n";
+    ss << "    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n";
+    ss << "    __syncthreads();\n";
+    ss << "    if (lane == 0) {\n";
+    ss << "#pragma unroll\n";
+    ss << "        for (int k = 0; k < " << K << "; ++k) {\n";
+    for (size_t r = 0; r < ctypes.size(); ++r) ss << "            s" << r << "[warp * " << K << " + k] = v" << r << "[k];\n";
+    ss << "        }\n";
+    ss << "    }\n";
+    ss << "    __syncthreads();\n";
+    ss << "    if (warp == 0) {\n";
+    ss << "#pragma unroll\n";
+    ss << "        for (int k = 0; k < " << K << "; ++k) {\n";
+    for (size_t r = 0; r < ctypes.size(); ++r) {
+        ss << "            v" << r << "[k] = lane < " << (kThreads / 32) << " ? s" << r << "[lane * " << K << " + k] : "
+           << idents[r] << ";\n";
+        ss << "#pragma unroll\n";
+        ss << "            for (int m = 16; m >= 1; m >>= 1) { const " << ctypes[r] << " o = bh_shfl_xor(v" << r
+           << "[k], m); v" << r << "[k] = " << reduce_expr(ops[r], "v" + to_string(r) + "[k]", "o") << "; }\n";
+    }
+    ss << "        }\n";
+    ss << "    }\n";
+    ss << "}\n";
+    return ss.str();
+}
+
 // GRID_REDUCE: `loop` is a 1-D innermost loop whose rank-0 sweeps are reductions to scalars.
 // `identities` are the kernel-level identity instructions of those reductions (folded). Work item
 // = one tile of kReduceTile elements; the CTA that completes the last tile of a unit folds the
@@ -2064,10 +2108,24 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
     u.slot_bytes = red_slot_bytes(reds);
     u.scratch_bytes_per_tile = u.slot_bytes * static_cast<int64_t>(reds.size());
     for (const InstrPtr &r : reds) u.red_orders.emplace_back(r->origin_id, "tree:" + to_string(L.size));
+    // Several reductions share the tile's block-reduction barriers (each keeps its own tree).
+    int64_t sm_bytes = (kThreads / 32) * K * u.slot_bytes;
+    if (reds.size() > 1) {
+        vector<int64_t> offsets;
+        vector<bh_opcode> ops;
+        int64_t off = 0;
+        for (const InstrPtr &r : reds) {
+            offsets.push_back(off);
+            ops.push_back(r->opcode);
+            off += ((kThreads / 32) * K * bh_type_size(r->operand[0].base->dtype()) + 15) / 16 * 16;
+        }
+        sm_bytes = max(sm_bytes, off);
+        helpers << block_reduce_all_fn(ctypes, ops, idents, offsets, K);
+    }
     body << helpers.str();
     body << "__device__ void bh_work(const P &p, bh_i64 w) {\n";
     body << pointer_locals(sym);
-    body << "    __shared__ alignas(16) unsigned long long sm_raw[" << (kThreads / 32) * K * (u.slot_bytes / 8) << "];\n";
+    body << "    __shared__ alignas(16) unsigned long long sm_raw[" << (sm_bytes + 7) / 8 << "];\n";
     body << "    __shared__ bool am_last;\n";
     for (size_t k = 0; k < reds.size(); ++k)
         body << "    " << ctypes[k] << "* part" << k << " = (" << ctypes[k] << "*)(p.scratch + p.ntiles * "
@@ -2122,8 +2180,14 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
         body << "        }\n";
     }
     body << "    }\n";
+    if (reds.size() > 1) {
+        body << "    bh_block_reduce_all(";
+        for (size_t k = 0; k < reds.size(); ++k) body << accs[k] << ", ";
+        body << "(unsigned char*)sm_raw);\n";
+    } else {
+        body << "    bh_block_reduce_k0(" << accs[0] << ", (" << ctypes[0] << "*)sm_raw);\n";
+    }
     for (size_t k = 0; k < reds.size(); ++k) {
-        body << "    bh_block_reduce_k" << k << "(" << accs[k] << ", (" << ctypes[k] << "*)sm_raw);\n";
         body << "    if (threadIdx.x == 0) {\n";
         body << "#pragma unroll\n";
         body << "        for (int k = 0; k < " << K << "; ++k)\n";
