@@ -21,7 +21,10 @@
 //   LANE_REDUCE   the SPLIT_REDUCE structure when the swept axis is contiguous and there are
 //                 enough points: C (power of two <= 256, from the shapes) lanes of one CTA share a
 //                 point, lane c folds elements c, c+C, ... (coalesced), and a fixed shuffle tree
-//                 combines the lanes; one pass, no scratch.
+//                 combines the lanes; one pass, no scratch. With one point axis, a CTA per point
+//                 and a stencil group among its read-only views (views of one base that differ by
+//                 whole rows and a few columns), each CTA walks a range of rows and stages the
+//                 group's rows in a shared-memory ring with cp.async, one row ahead.
 //   OUTER_REDUCE  a nest that reduces its outermost axis into an array: threads own the output
 //                 elements (the inner parallel ranks) and loop over the reduced axis.
 //   SCAN1D        a 1-D nest with one accumulate (cumulative sum/product) among elementwise
@@ -29,9 +32,10 @@
 //                 re-scan with the carry -- each with a fixed block scan (order set by the length).
 //   SERIAL        anything else: one thread runs the nest in program order (always correct).
 //
-// All loop sizes, view offsets/strides and constants are kernel parameters, so one compiled
-// kernel serves every array size and sliding offset; the generated source depends only on the
-// block structure and element types.
+// Loop sizes, view offsets/strides and constants are kernel parameters. The source also fixes a
+// few choices derived from the sizes (lanes per point, tiles per work item, iterations per lane,
+// the stencil ring), so arrays of different sizes may get different kernels; code whose fast path
+// assumes a layout (the stencil staging) checks it at launch and falls back otherwise.
 #pragma once
 
 #include <cstdint>
