@@ -65,9 +65,10 @@ int64_t LaunchUnit::scratch_bytes() const {
 }
 
 int64_t LaunchUnit::counters_needed() const {
-    if (sched == Sched::GRID_REDUCE) return 1;
-    if (sched == Sched::SPLIT_REDUCE) return (rows * cols + kThreads - 1) / kThreads;
-    return 0;
+    int64_t own = 0;
+    if (sched == Sched::GRID_REDUCE) own = 1;
+    if (sched == Sched::SPLIT_REDUCE) own = (rows * cols + kThreads - 1) / kThreads;
+    return tail ? own + 1 : own;  // the tail's completion counter follows
 }
 
 string cuda_type(bh_type t) {
@@ -993,7 +994,56 @@ uint64_t fnv1a(const string &s) {
     return h;
 }
 
+// The wrappers of every unit: bh_main (what one CTA of a plain launch does; the stencil staging
+// replaces its loop) and the two kernels. The kernels' text (kKernels) is the same for every unit.
+const char *kKernels = R"CUDA(
+extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME__(const __grid_constant__ P p) {
+    bh_main(p);
+}
+extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME___batch(const P* __restrict__ items,
+        const bh_i64* __restrict__ prefix, int nitems, bh_i64 total) {
+    // Each CTA takes a contiguous range of the work items of all items, so consecutive work items
+    // of a CTA belong to the same item except at item boundaries. The parameters of the current
+    // item live in shared memory and are looked up and reloaded only at those boundaries.
+    __shared__ P sp;
+    int have = -1;
+    bh_i64 have_lo = 0, have_hi = 0;
+    const bh_i64 g_lo = (bh_i64)blockIdx.x * total / gridDim.x;
+    const bh_i64 g_hi = ((bh_i64)blockIdx.x + 1) * total / gridDim.x;
+    for (bh_i64 g = g_lo; g < g_hi; ++g) {
+        if (g < have_lo || g >= have_hi) {
+            int lo = 0, hi = nitems - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (prefix[mid] <= g) lo = mid; else hi = mid - 1;
+            }
+            __syncthreads();
+            for (int k = threadIdx.x; k < (int)(sizeof(P) / 8); k += blockDim.x)
+                ((unsigned long long*)&sp)[k] = ((const unsigned long long*)(items + lo))[k];
+            __syncthreads();
+            have = lo;
+            have_lo = prefix[lo];
+            have_hi = prefix[lo + 1];
+        }
+        bh_work(sp, g - have_lo);
+    }
+    (void)have;
+}
+)CUDA";
+const string kWrappers = string(R"CUDA(
+__device__ __forceinline__ void bh_main(const P &p) {
+    for (bh_i64 w = blockIdx.x; w < p.work; w += gridDim.x) bh_work(p, w);
+}
+)CUDA") + kKernels;
+
 void finish_source(LaunchUnit &u, const string &params_decl, const string &body, const CodegenOptions &opt) {
+    u.params_decl = params_decl;
+    u.body_core = body;
+    const string kk = kKernels;
+    if (u.body_core.size() >= kk.size() && u.body_core.compare(u.body_core.size() - kk.size(), kk.size(), kk) == 0)
+        u.body_core.resize(u.body_core.size() - kk.size());
+    else
+        u.body_core.clear();  // wrappers of its own: not combinable with another unit
     stringstream src;
     src << kPrelude;
     auto uses = [&](const char *name) { return params_decl.find(name) != string::npos || body.find(name) != string::npos; };
@@ -1065,40 +1115,7 @@ int64_t unit_bytes(const Symbols &sym, const vector<const Block *> &items) {
 // the work items of many units of the same kernel in one persistent grid (item lookup by binary
 // search over the prefix sums of their work counts). Both call the same device code on the same
 // work items, so batched results equal plain results bit for bit.
-const char *kWrappers = R"CUDA(
-extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME__(const __grid_constant__ P p) {
-    for (bh_i64 w = blockIdx.x; w < p.work; w += gridDim.x) bh_work(p, w);
-}
-extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME___batch(const P* __restrict__ items,
-        const bh_i64* __restrict__ prefix, int nitems, bh_i64 total) {
-    // Each CTA takes a contiguous range of the work items of all items, so consecutive work items
-    // of a CTA belong to the same item except at item boundaries. The parameters of the current
-    // item live in shared memory and are looked up and reloaded only at those boundaries.
-    __shared__ P sp;
-    int have = -1;
-    bh_i64 have_lo = 0, have_hi = 0;
-    const bh_i64 g_lo = (bh_i64)blockIdx.x * total / gridDim.x;
-    const bh_i64 g_hi = ((bh_i64)blockIdx.x + 1) * total / gridDim.x;
-    for (bh_i64 g = g_lo; g < g_hi; ++g) {
-        if (g < have_lo || g >= have_hi) {
-            int lo = 0, hi = nitems - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (prefix[mid] <= g) lo = mid; else hi = mid - 1;
-            }
-            __syncthreads();
-            for (int k = threadIdx.x; k < (int)(sizeof(P) / 8); k += blockDim.x)
-                ((unsigned long long*)&sp)[k] = ((const unsigned long long*)(items + lo))[k];
-            __syncthreads();
-            have = lo;
-            have_lo = prefix[lo];
-            have_hi = prefix[lo + 1];
-        }
-        bh_work(sp, g - have_lo);
-    }
-    (void)have;
-}
-)CUDA";
+
 
 ParamField work_field(int64_t work) {
     ParamField f{ParamField::I64};
@@ -2215,7 +2232,47 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
         body << "    }\n";
     }
     body << "    if (threadIdx.x == 0) *p.counter = 0u;\n";
-    body << "}\n" << kWrappers;
+    body << "}\n";
+    // The whole reduction in one CTA, for another kernel's tail (fuse_tails): only for small
+    // arrays and order-free reductions, where the fold order does not change the result.
+    bool order_free = !opt.bounds_check && ntiles <= 4;
+    for (const InstrPtr &r : reds) {
+        const bh_type t = r->operand[0].base->dtype();
+        const bool exact_arith = (r->opcode == BH_ADD_REDUCE || r->opcode == BH_MULTIPLY_REDUCE) &&
+                                 (bh_type_is_integer(t) || t == bh_type::BOOL);
+        const bool cmp_or_bits = r->opcode == BH_MAXIMUM_REDUCE || r->opcode == BH_MINIMUM_REDUCE ||
+                                 r->opcode == BH_LOGICAL_AND_REDUCE || r->opcode == BH_LOGICAL_OR_REDUCE ||
+                                 r->opcode == BH_LOGICAL_XOR_REDUCE || r->opcode == BH_BITWISE_AND_REDUCE ||
+                                 r->opcode == BH_BITWISE_OR_REDUCE || r->opcode == BH_BITWISE_XOR_REDUCE;
+        if (!(exact_arith || (cmp_or_bits && !bh_type_is_complex(t)))) order_free = false;
+    }
+    if (order_free) {
+        u.tail_capable = true;
+        body << "__device__ void bh_tail(const P &p) {\n";
+        body << pointer_locals(sym);
+        body << "    __shared__ alignas(16) unsigned long long tail_sm[" << (kThreads / 32) * 2 << "];\n";
+        map<ViewKey, string> acc1;
+        for (size_t k = 0; k < reds.size(); ++k) {
+            body << "    " << ctypes[k] << " tacc" << k << " = " << idents[k] << ";\n";
+            acc1[ViewKey(reds[k]->operand[0])] = "tacc" + to_string(k);
+        }
+        body << "#pragma unroll 4\n";
+        body << "    for (bh_i64 i0 = threadIdx.x; i0 < " << n0 << "; i0 += " << kThreads << ") {\n";
+        {
+            Scope scope;
+            Emitter et(sym, body, opt);
+            et.external_acc = acc1;
+            et.write_body(L, scope, 8);
+        }
+        body << "    }\n";
+        for (size_t k = 0; k < reds.size(); ++k) {
+            body << "    tacc" << k << " = bh_block_reduce" << k << "(tacc" << k << ", (" << ctypes[k] << "*)tail_sm);\n";
+            if (!sym.temps.count(reds[k]->operand[0].base))
+                body << "    if (threadIdx.x == 0) " << em.array_ref(reds[k]->operand[0]) << " = tacc" << k << ";\n";
+        }
+        body << "}\n";
+    }
+    body << kWrappers;
     u.fields = pl.fields;
     u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
     u.elements = L.size;
@@ -2544,6 +2601,96 @@ bool identity_loop(const Block &b) {
     return instrs.size() == 1 && instrs[0]->opcode == BH_IDENTITY && instrs[0]->operand[1].isConstant();
 }
 
+// The wrappers of a unit with a folded tail (see fuse_tails): the CTA that arrives last on the
+// completion counter runs the tail -- per launch, or per item of a grouped launch.
+const char *kTailWrappers = R"CUDA(
+struct P {
+    bh_u1::P a;
+    bh_u2::P b;
+    alignas(8) unsigned int* tail_counter;
+};
+// Every thread's writes are made visible device-wide, thread 0 arrives with an acquire-release
+// atomic, and the tail's threads acquire before reading.
+__device__ __forceinline__ bool bh_tail_gate(unsigned int *counter, unsigned int arrivals) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = bh_arrive(counter) == arrivals - 1u;
+    __syncthreads();
+    const bool l = last;
+    if (l) {
+        bh_acquire();
+        if (threadIdx.x == 0) *counter = 0u;
+    }
+    return l;
+}
+extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME__(const __grid_constant__ P p) {
+    bh_u1::bh_main(p.a);
+    if (bh_tail_gate(p.tail_counter, gridDim.x)) bh_u2::bh_tail(p.b);
+}
+extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME___batch(const P* __restrict__ items,
+        const bh_i64* __restrict__ prefix, int nitems, bh_i64 total) {
+    // As the plain grouped wrapper; each item's tail runs after the item's last work item.
+    __shared__ P sp;
+    bh_i64 have_lo = 0, have_hi = 0;
+    const bh_i64 g_lo = (bh_i64)blockIdx.x * total / gridDim.x;
+    const bh_i64 g_hi = ((bh_i64)blockIdx.x + 1) * total / gridDim.x;
+    for (bh_i64 g = g_lo; g < g_hi; ++g) {
+        if (g < have_lo || g >= have_hi) {
+            int lo = 0, hi = nitems - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (prefix[mid] <= g) lo = mid; else hi = mid - 1;
+            }
+            __syncthreads();
+            for (int k = threadIdx.x; k < (int)(sizeof(P) / 8); k += blockDim.x)
+                ((unsigned long long*)&sp)[k] = ((const unsigned long long*)(items + lo))[k];
+            __syncthreads();
+            have_lo = prefix[lo];
+            have_hi = prefix[lo + 1];
+        }
+        bh_u1::bh_work(sp.a, g - have_lo);
+        if (bh_tail_gate(sp.tail_counter, (unsigned int)(have_hi - have_lo))) bh_u2::bh_tail(sp.b);
+    }
+}
+)CUDA";
+
+LaunchUnit fuse_tail(const LaunchUnit &u1, const LaunchUnit &u2) {
+    LaunchUnit u = u1;
+    u.tail = true;
+    for (const ParamField &f : u2.fields) u.fields.push_back(f);  // its counter and scratch stay unused
+    ParamField gate{ParamField::COUNTER};
+    gate.off = u1.counters_needed();
+    u.fields.push_back(gate);
+    u.algorithmic_bytes = u1.algorithmic_bytes + u2.algorithmic_bytes;
+    u.elements = u1.elements + u2.elements;
+    u.red_orders.insert(u.red_orders.end(), u2.red_orders.begin(), u2.red_orders.end());
+    stringstream src;
+    src << kPrelude;
+    auto uses = [&](const char *name) {
+        for (const LaunchUnit *x : {&u1, &u2})
+            if (x->params_decl.find(name) != string::npos || x->body_core.find(name) != string::npos) return true;
+        return false;
+    };
+    if (uses("bh_c64") || uses("bh_c128")) src << kComplexPrelude;
+    src << "namespace bh_u1 {\nstruct P {\n" << u1.params_decl << "};\n" << u1.body_core << "} // namespace bh_u1\n";
+    src << "namespace bh_u2 {\nstruct P {\n" << u2.params_decl << "};\n" << u2.body_core << "} // namespace bh_u2\n";
+    src << kTailWrappers;
+    const string without_name = src.str();
+    stringstream nm;
+    nm << "bh_" << sched_name(u1.sched) << "_tail_" << hex << fnv1a(without_name);
+    u.name = nm.str();
+    string text = without_name;
+    const string placeholder = "__KERNEL_NAME__";
+    for (size_t pos = text.find(placeholder); pos != string::npos; pos = text.find(placeholder))
+        text.replace(pos, placeholder.size(), u.name);
+    u.source = text;
+    u.params_decl.clear();
+    u.body_core.clear();
+    u.tail_capable = false;
+    return u;
+}
+
 } // namespace
 
 vector<LaunchUnit> lower_kernel(const LoopB &kernel, const CodegenOptions &opt) {
@@ -2640,6 +2787,48 @@ vector<LaunchUnit> lower_kernel(const LoopB &kernel, const CodegenOptions &opt) 
     if (!serial && (!pending_identities.empty() || !pending_id_loops.empty())) serial = true;
     if (serial) return {lower_serial(items, opt)};
     return units;
+}
+
+vector<int> fuse_tails(const vector<LoopB> &kernels, vector<vector<LaunchUnit>> &lowered, const CodegenOptions &opt) {
+    vector<int> into(lowered.size(), -1);
+    if (opt.bounds_check) return into;
+    // Bases each kernel reads and writes (frees count as writes).
+    const size_t n = kernels.size();
+    vector<set<const bh_base *>> reads(n), writes(n);
+    for (size_t k = 0; k < n; ++k) {
+        for (const InstrPtr &ip : jitk::all_instr(kernels[k]))
+            for (size_t o = 0; o < ip->operand.size(); ++o)
+                if (!ip->operand[o].isConstant()) (o == 0 ? writes[k] : reads[k]).insert(ip->operand[o].base);
+        for (bh_base *f : kernels[k].getAllFrees()) writes[k].insert(f);
+    }
+    auto meets = [](const set<const bh_base *> &a, const set<const bh_base *> &b) {
+        for (const bh_base *x : a)
+            if (b.count(x)) return true;
+        return false;
+    };
+    for (size_t j = 1; j < n; ++j) {
+        if (lowered[j].size() != 1 || !lowered[j][0].tail_capable || lowered[j][0].body_core.empty()) continue;
+        // The producer: the last earlier kernel that writes an array this reduction reads. The
+        // reduction moves up to the end of the producer's kernel, which keeps the program's
+        // meaning when it commutes with every kernel in between (no array one writes and the other
+        // reads or writes).
+        size_t k = j;
+        while (k > 0 && !meets(writes[k - 1], reads[j])) --k;
+        if (k == 0) continue;
+        --k;
+        bool commutes = true;
+        for (size_t m = k + 1; m < j && commutes; ++m)
+            commutes = !meets(writes[m], reads[j]) && !meets(writes[m], writes[j]) && !meets(reads[m], writes[j]);
+        if (!commutes || lowered[k].empty() || into[k] >= 0) continue;
+        LaunchUnit &u1 = lowered[k].back();
+        if (u1.tail || u1.sched == Sched::SCAN1D || u1.sched == Sched::SERIAL || u1.body_core.empty()) continue;
+        u1 = fuse_tail(u1, lowered[j][0]);
+        lowered[j].clear();
+        into[j] = static_cast<int>(k);
+        writes[k].insert(writes[j].begin(), writes[j].end());
+        reads[k].insert(reads[j].begin(), reads[j].end());
+    }
+    return into;
 }
 
 } // namespace cuda

@@ -62,6 +62,7 @@ struct ParamField {
     bh_constant c{};         // CONST / R123_*
     int64_t origin = -1;     // CONST / R123_*: origin id of the instruction holding the constant
     int part = 0;            // CONST: which 8 bytes of the constant (1: the imaginary part of a complex128)
+    int64_t off = 0;         // COUNTER: index offset in the unit's counters
 };
 
 struct LaunchUnit {
@@ -79,6 +80,16 @@ struct LaunchUnit {
                                 // GRID_REDUCE: tiles per work item; SCAN1D: work items of the phase
     int64_t scan_chunks = 0;    // SCAN1D: chunks of 2048 elements
     int64_t scan_offset = 0;    // SCAN1D: offset of its totals/carries in the scan arena (set by the plan)
+    // The parameter members and the device code (without the kernel wrappers) of the source;
+    // body_core is empty for sources with wrappers of their own.
+    std::string params_decl, body_core;
+    // GRID_REDUCE of a small array with order-free reductions only: body_core also defines
+    // bh_tail(p), the whole reduction run by one CTA (threads fold strided elements, then one
+    // block tree), which another unit's kernel can run in its tail (see fuse_tails).
+    bool tail_capable = false;
+    // This unit's kernel runs a folded reduction's bh_tail in the CTA that finishes last; the
+    // completion counter follows the unit's own counters.
+    bool tail = false;
     int64_t work_items() const;
     int64_t scratch_bytes() const;   // partials in the scratch arena
     int64_t counters_needed() const; // completion counters
@@ -100,6 +111,18 @@ struct CodegenOptions {
 
 // Lower one kernel (as produced by jitk::get_kernel_list) into launch units executed in order.
 std::vector<LaunchUnit> lower_kernel(const jitk::LoopB &kernel, const CodegenOptions &opt);
+
+// Tail fusion over a flush's lowered kernels (`lowered[k]`: the units of kernel k, empty for
+// system-only kernels). A kernel j that is one tail-capable GRID_REDUCE (a small array, order-
+// free reductions: max, min, logical, bitwise, integer sums and products -- typically the second
+// level of a 2-D max) is folded into its producer k, the last earlier kernel that writes an array
+// j reads, when j commutes with every kernel between them and k's last unit is a FLAT /
+// GRID_REDUCE / SPLIT_REDUCE / LANE_REDUCE / OUTER_REDUCE unit: every CTA runs the first unit's
+// work, and the CTA that arrives last on an acquire-release completion counter runs the
+// reduction. Kernel j's unit list is emptied. Returns, per kernel, the kernel it was folded into
+// (-1: none).
+std::vector<int> fuse_tails(const std::vector<jitk::LoopB> &kernels, std::vector<std::vector<LaunchUnit>> &lowered,
+                            const CodegenOptions &opt);
 
 // CUDA element type name (the "long long" family is used for 64-bit integers).
 std::string cuda_type(bh_type t);

@@ -92,20 +92,25 @@ extern "C" const char *bh_ve_cuda_dry_run(bhb_ir *handle, int compile, const cha
         cfg.avoid_mixed_sweeps = true;
         const vector<jitk::LoopB> kernels = jitk::get_kernel_list(instr_list, cfg);
         cuda::CodegenOptions opt;
+        vector<vector<cuda::LaunchUnit>> lowered(kernels.size());
+        for (size_t k = 0; k < kernels.size(); ++k)
+            if (!kernels[k].isSystemOnly()) lowered[k] = cuda::lower_kernel(kernels[k], opt);
+        const vector<int> folded = cuda::fuse_tails(kernels, lowered, opt);
         stringstream ss;
         ss << "{\"kernels\": [";
         for (size_t k = 0; k < kernels.size(); ++k) {
             if (k) ss << ", ";
-            ss << "{\"block\": \"" << json_escape(kernels[k].pprint()) << "\", \"units\": [";
-            const vector<cuda::LaunchUnit> units =
-                kernels[k].isSystemOnly() ? vector<cuda::LaunchUnit>{} : cuda::lower_kernel(kernels[k], opt);
+            ss << "{\"block\": \"" << json_escape(kernels[k].pprint()) << "\", \"folded_into\": " << folded[k]
+               << ", \"units\": [";
+            const vector<cuda::LaunchUnit> &units = lowered[k];
             for (size_t u = 0; u < units.size(); ++u) {
                 if (u) ss << ", ";
                 string err;
                 if (compile) err = nvrtc_compile(units[u].source, units[u].name, false);
                 ss << "{\"name\": \"" << units[u].name << "\", \"sched\": \"" << cuda::sched_name(units[u].sched)
                    << "\", \"fields\": " << units[u].fields.size() << ", \"work\": " << units[u].work_items()
-                   << ", \"bytes\": " << units[u].algorithmic_bytes << ", \"compile_error\": \"" << json_escape(err)
+                   << ", \"bytes\": " << units[u].algorithmic_bytes << ", \"tail\": " << (units[u].tail ? "true" : "false")
+                   << ", \"compile_error\": \"" << json_escape(err)
                    << "\", \"source\": \"" << json_escape(units[u].source) << "\"}";
             }
             ss << "]}";

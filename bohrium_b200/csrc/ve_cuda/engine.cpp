@@ -615,7 +615,7 @@ void EngineCUDA::pack_params(const PlanUnit &pu, const vector<bh_base *> &bases,
                 break;
             }
             case ParamField::COUNTER: {
-                void *p = counters + counter_idx;
+                void *p = counters + counter_idx + f.off;
                 memcpy(slot, &p, 8);
                 break;
             }
@@ -1020,19 +1020,29 @@ EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const
     vector<int> last_write_level(base_ids.size(), -1), last_read_level(base_ids.size(), -1);
     // Lower every kernel first so that all new sources compile in parallel.
     vector<vector<LaunchUnit>> lowered(kernels.size());
+    vector<int> folded_into(kernels.size(), -1);
     {
         const auto tc = chrono::steady_clock::now();
         vector<const LaunchUnit *> all;
         for (size_t k = 0; k < kernels.size(); ++k) {
             if (kernels[k].isSystemOnly()) continue;
             lowered[k] = lower_kernel(kernels[k], cg_opt);
-            for (const LaunchUnit &u : lowered[k]) all.push_back(&u);
         }
+        // Small dependent order-free reductions run in the tail of the kernel before them. Not
+        // while recording per-kernel timings, whose features describe one kernel each.
+        if (!record) folded_into = fuse_tails(kernels, lowered, cg_opt);
+        for (size_t k = 0; k < kernels.size(); ++k)
+            for (const LaunchUnit &u : lowered[k]) all.push_back(&u);
         _stats.time_codegen += seconds_since(tc);
         precompile(all);
     }
     for (size_t kidx = 0; kidx < kernels.size(); ++kidx) {
+        if (folded_into[kidx] >= 0) continue;  // runs in the tail of an earlier kernel
         const LoopB &kernel = kernels[kidx];
+        // The kernels this plan kernel runs: itself and any folded into its tail.
+        vector<const LoopB *> parts{&kernel};
+        for (size_t j = kidx + 1; j < kernels.size(); ++j)
+            if (folded_into[j] == static_cast<int>(kidx)) parts.push_back(&kernels[j]);
         PlanKernel pk;
         if (!kernel.isSystemOnly()) {
             vector<LaunchUnit> &units = lowered[kidx];
@@ -1054,31 +1064,34 @@ EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const
             }
         }
         set<int> reads, writes;
-        for (const InstrPtr &instr : all_instr(kernel)) {
-            for (size_t o = 0; o < instr->operand.size(); ++o) {
-                const bh_view &v = instr->operand[o];
-                if (v.isConstant()) continue;
-                const int b = idx(v.base);
-                if (b < 0) continue;
-                if (o == 0) {
-                    writes.insert(b);
-                } else {
-                    reads.insert(b);
+        for (const LoopB *part : parts) {
+            for (const InstrPtr &instr : all_instr(*part)) {
+                for (size_t o = 0; o < instr->operand.size(); ++o) {
+                    const bh_view &v = instr->operand[o];
+                    if (v.isConstant()) continue;
+                    const int b = idx(v.base);
+                    if (b < 0) continue;
+                    if (o == 0) {
+                        writes.insert(b);
+                    } else {
+                        reads.insert(b);
+                    }
                 }
             }
-        }
-        for (bh_base *f : kernel.getAllFrees()) {
-            const int b = idx(f);
-            if (b >= 0) {
-                pk.frees.push_back(b);
-                writes.insert(b);
+            for (bh_base *f : part->getAllFrees()) {
+                const int b = idx(f);
+                if (b >= 0) {
+                    pk.frees.push_back(b);
+                    writes.insert(b);
+                }
             }
         }
         pk.writes.assign(writes.begin(), writes.end());
         if ((record || learned_on) && !pk.units.empty()) pk.feat = jitk::block_features(kernel);
         // Summation order of the floating-point sums and products: "seq" (one thread folds in
         // index order) unless a unit reduces the sweep across threads.
-        for (const InstrPtr &instr : all_instr(kernel)) {
+        for (const LoopB *part : parts)
+        for (const InstrPtr &instr : all_instr(*part)) {
             if (!bh_opcode_is_sweep(instr->opcode)) continue;
             const bh_opcode op = instr->opcode;
             if (op != BH_ADD_REDUCE && op != BH_MULTIPLY_REDUCE && op != BH_ADD_ACCUMULATE &&

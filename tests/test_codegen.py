@@ -46,7 +46,25 @@ def test_heat_step_fuses_stencil_write_and_split_partial_max():
         return [W.heat_step(a, b), b]
     res, units = plan(prog)
     scheds = [u["sched"] for u in units]
-    assert scheds == ["split_reduce", "grid_reduce"], scheds
+    # the max over the 62 row maxima runs in the tail of the stencil kernel
+    assert scheds == ["split_reduce"] and units[0]["tail"], scheds
+    assert [k["folded_into"] for k in res["kernels"] if k["folded_into"] >= 0] == [0]
+
+
+def test_small_order_free_second_level_reduction_runs_in_the_tail():
+    """A 2-D max (or integer sum) is a row reduction followed by a small reduction of the row
+    results: at most four tiles of those run in the first kernel's tail. Floating-point sums keep
+    their own kernel (a different fold order would change the result), and so do larger arrays."""
+    cases = [((4096, 300), np.float64, "max", True), ((8192, 300), np.float32, "min", True),
+             ((4096, 300), np.int64, "sum", True), ((4096, 300), np.float64, "sum", False),
+             ((8193, 300), np.float64, "max", False)]
+    for shape, dt, op, folded in cases:
+        def prog(rt, shape=shape, dt=dt, op=op):
+            x = bh.empty(rt, shape, dt)
+            return [getattr(getattr(x + dt(1), op)(axis=1), op)()]
+        res, units = plan(prog)
+        tails = [u["tail"] for u in units]
+        assert any(tails) == folded, (shape, dt, op, [u["sched"] for u in units], tails)
 
 
 def test_batching_systems_lower_to_one_unit_each():
