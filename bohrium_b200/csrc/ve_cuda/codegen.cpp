@@ -1401,7 +1401,8 @@ bool swept_axis_contiguous(const LoopB &sub, int rank) {
 // s0 + (i0 + dk_i) * S0 + dm_i + j of the base, so the rows a CTA needs for consecutive points
 // overlap and can be staged once in shared memory.
 // Rows a staging CTA keeps in flight beyond the ones the current point reads (on the 4096^2
-// heat stencil, 2 and 3 took 3 % longer than 1: fewer CTAs fit in shared memory).
+// heat stencil, 2 and 3 took 3 % longer than 1 -- fewer CTAs fit in shared memory -- and 0 took
+// 8 % longer although four CTAs fit).
 constexpr int64_t kStagePrefetch = 1;
 
 struct StencilMember {
