@@ -304,6 +304,24 @@ def test_stencil_rows_lane_schedule(gpu_rt, oracle_rt, rows, cols, dtype, op, of
     assert_close(g[1], o[1], *float_tol(dtype), "stencil")
 
 
+@pytest.mark.parametrize("dtype,op", [(np.int32, "sum"), (np.int64, "max"), (np.complex64, "sum"),
+                                      (np.complex128, "sum")])
+def test_stencil_rows_other_element_types(gpu_rt, oracle_rt, dtype, op):
+    """The staged stencil rows with integer and complex elements (4, 8 and 16-byte elements: the
+    16-byte ones take the plain lane code), against the oracle."""
+    rng = np.random.default_rng(5)
+    shape = (604, 1004)  # a row of 1004 elements: 16-byte multiples for 4 and 8-byte elements
+    if np.dtype(dtype).kind == "c":
+        host = (rng.random(shape) + 1j * rng.random(shape)).astype(dtype)
+    else:
+        host = rng.integers(-1000, 1000, shape).astype(dtype)
+    offsets = [(0, 0), (-1, 0), (1, 0), (0, -1), (0, 1)]
+    g, o = both(gpu_rt, oracle_rt, _stencil_prog(host, 600, 1002, dtype, op, offsets))
+    tol = 0 if np.dtype(dtype).kind == "i" else (1e-5 if np.dtype(dtype) == np.complex64 else 1e-12)
+    assert_close(g[0], o[0], tol, tol, "reduce")
+    assert_close(g[1], o[1], tol, tol, "stencil")
+
+
 def test_stencil_rows_grouped_launch_is_bit_identical(gpu_executor):
     """Two independent stencils in one flush share a kernel and level, so batch mode "grouped"
     runs them as one grouped launch; results equal the plain launches' bit for bit."""
