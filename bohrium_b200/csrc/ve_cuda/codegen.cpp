@@ -2284,14 +2284,15 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
 // ------------------------------------------------------------------------------------- SCAN1D
 // A 1-D innermost loop with one accumulate (cumulative sum/product) among elementwise
 // instructions. Three launch units, in a fixed order that depends on the length only:
-//   A  per chunk of 2048 elements: thread t folds elements 8t..8t+7 of the chunk in order (the
-//      instructions before the accumulate are computed on the fly), a fixed block scan of the 256
-//      thread totals gives the chunk total;
+//   A  per chunk of 2048 elements: the accumulate's inputs are computed on the fly at coalesced
+//      positions and staged in shared memory; thread t folds elements 8t..8t+7 of the chunk in
+//      order from there, and a fixed block scan of the 256 thread totals gives the chunk total;
 //   B  one CTA: exclusive scan of the chunk totals (groups of 2048, the same block scan, a running
 //      carry) -> the carry into every chunk;
-//   C  per chunk: the same per-thread fold and block scan; element value = carry op (exclusive
-//      thread prefix op running thread prefix); written out, then the instructions after the
-//      accumulate run on it.
+//   C  per chunk: the same staging, per-thread fold and block scan; element value = carry op
+//      (exclusive thread prefix op running thread prefix), staged again and written out at
+//      coalesced positions, where the instructions after the accumulate run on it.
+// The fold order is the same whatever the staging, so results depend on the length only.
 constexpr int kScanPerThread = 8;
 constexpr int64_t kScanTile = kThreads * kScanPerThread;
 
@@ -2437,41 +2438,31 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
             body << "    }\n";
             body << "}\n" << kWrappers;
         } else {
-            // Thread fold over its 8 elements (inputs computed on the fly).
-            body << "    " << T << " s = " << ident << ";\n";
-            body << "    " << T << " xs[" << kScanPerThread << "];\n";
-            {
+            // Pass 1: the accumulate's inputs, computed at coalesced positions (element k*256 + t
+            // of the chunk in thread t) and staged in shared memory; stage slot of element q is
+            // q + q/8, so the per-thread reads of 8 consecutive elements below hit distinct banks.
+            body << "    __shared__ " << T << " stage[" << kScanTile + kScanTile / kScanPerThread << "];\n";
+            body << "    const bh_i64 cbase = c * " << kScanTile << ";\n";
+            auto stage_pass = [&](bool with_inputs, const string &what) {
                 Scope scope;
                 body << "#pragma unroll\n";
                 body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
-                body << "        const bh_i64 i0 = c * " << kScanTile << " + threadIdx.x * " << kScanPerThread << " + k;\n";
-                body << "        xs[k] = " << ident << ";\n";
+                body << "        const int q = k * " << kThreads << " + (int)threadIdx.x;\n";
+                body << "        const bh_i64 i0 = cbase + q;\n";
+                if (what == "in") body << "        " << T << " x = " << ident << ";\n";
                 body << "        if (i0 < " << n0 << ") {\n";
                 declare_temps(scope, 12);
-                emit_inputs(scope, 12);
-                body << "            xs[k] = " << em.name(acc->operand[1], scope) << ";\n";
-                body << "            s = " << reduce_expr(rop, "s", "xs[k]") << ";\n";
-                body << "        }\n";
-                body << "    }\n";
-            }
-            body << "    " << T << " total;\n";
-            body << "    const " << T << " e = bh_block_scan(s, total, sm);\n";
-            if (phase == 0) {
-                body << "    if (threadIdx.x == 0) totals[c] = total;\n";
-                body << "}\n" << kWrappers;
-            } else {
-                body << "    const " << T << " carry = carries[c];\n";
-                body << "    " << T << " r = " << ident << ";\n";
-                Scope scope;
-                body << "#pragma unroll\n";
-                body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
-                body << "        const bh_i64 i0 = c * " << kScanTile << " + threadIdx.x * " << kScanPerThread << " + k;\n";
-                body << "        if (i0 < " << n0 << ") {\n";
-                declare_temps(scope, 12);
-                emit_inputs(scope, 12);  // recomputed: instructions after the accumulate may read them
-                body << "            r = " << reduce_expr(rop, "r", "xs[k]") << ";\n";
-                body << "            const " << T << " inner = " << reduce_expr(rop, "e", "r") << ";\n";
-                body << "            const " << T << " out = " << reduce_expr(rop, "carry", "inner") << ";\n";
+                if (with_inputs) emit_inputs(scope, 12);
+                if (what == "in") {
+                    body << "            x = " << em.name(acc->operand[1], scope) << ";\n";
+                    body << "        }\n";
+                    body << "        stage[q + (q >> 3)] = x;\n";
+                    body << "    }\n";
+                    return;
+                }
+                // Pass 2: the scanned values back at coalesced positions, then the instructions
+                // after the accumulate.
+                body << "            const " << T << " out = stage[q + (q >> 3)];\n";
                 if (sym.temps.count(acc->operand[0].base)) {
                     body << "            t" << sym.base_index(acc->operand[0].base) << " = out;\n";
                 } else {
@@ -2489,6 +2480,55 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
                 }
                 body << "        }\n";
                 body << "    }\n";
+            };
+            stage_pass(true, "in");
+            body << "    __syncthreads();\n";
+            // Thread t folds elements 8t..8t+7 of the chunk in order.
+            body << "    " << T << " s = " << ident << ";\n";
+            body << "    " << T << " xs[" << kScanPerThread << "];\n";
+            body << "#pragma unroll\n";
+            body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+            body << "        const int q = (int)threadIdx.x * " << kScanPerThread << " + k;\n";
+            body << "        xs[k] = stage[q + (q >> 3)];\n";
+            body << "        if (cbase + q < " << n0 << ") s = " << reduce_expr(rop, "s", "xs[k]") << ";\n";
+            body << "    }\n";
+            // The block scan's first barrier orders these stage reads before any later stage write.
+            body << "    " << T << " total;\n";
+            body << "    const " << T << " e = bh_block_scan(s, total, sm);\n";
+            if (phase == 0) {
+                body << "    if (threadIdx.x == 0) totals[c] = total;\n";
+                body << "}\n" << kWrappers;
+            } else {
+                body << "    const " << T << " carry = carries[c];\n";
+                body << "    " << T << " r = " << ident << ";\n";
+                body << "#pragma unroll\n";
+                body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+                body << "        const int j = (int)threadIdx.x * " << kScanPerThread << " + k;\n";
+                body << "        if (cbase + j < " << n0 << ") {\n";
+                body << "            r = " << reduce_expr(rop, "r", "xs[k]") << ";\n";
+                body << "            const " << T << " inner = " << reduce_expr(rop, "e", "r") << ";\n";
+                body << "            stage[j + (j >> 3)] = " << reduce_expr(rop, "carry", "inner") << ";\n";
+                body << "        }\n";
+                body << "    }\n";
+                body << "    __syncthreads();\n";
+                // Instructions after the accumulate that read values computed before it get them
+                // recomputed (same thread and element as in pass 1, so stores repeat their values).
+                bool reread = false, after = false;
+                for (const Block &b : L._block_list) {
+                    const InstrPtr &i = b.getInstr();
+                    if (i == acc) {
+                        after = true;
+                        continue;
+                    }
+                    if (!after || bh_opcode_is_system(i->opcode)) continue;
+                    for (size_t o = 1; o < i->operand.size(); ++o) {
+                        const bh_view &v = i->operand[o];
+                        if (!v.isConstant() && v.base != acc->operand[0].base) reread = true;
+                    }
+                }
+                stage_pass(reread, "out");
+                // Stage reads of this work item before the next item's pass 1 writes.
+                body << "    __syncthreads();\n";
                 body << "}\n" << kWrappers;
             }
         }

@@ -81,3 +81,70 @@ def grid_reduce_sum(x: np.ndarray) -> np.ndarray:
         chunk[:c.size] = c
         fold = np.where(np.arange(256) < c.size, fold + chunk, fold)
     return cta_tree(fold[None, :])[0]
+
+
+def _block_scan(s: np.ndarray):
+    """The engine's block scan of the 256 thread values of each row of `s` (rows, 256): an
+    inclusive shuffle-up scan in each warp (x = y + x for lanes >= d, d = 1..16), shifted by one
+    lane, plus the warp offsets from a serial scan of the 8 warp totals. Returns the exclusive
+    prefixes (rows, 256) and the row totals."""
+    dt = s.dtype
+    zero = dt.type(0)
+    w = s.reshape(s.shape[0], 8, 32).copy()
+    lane = np.arange(32)
+    for d in (1, 2, 4, 8, 16):
+        y = w.copy()
+        y[:, :, d:] = w[:, :, :-d]
+        w = np.where(lane >= d, y + w, w)
+    ex = np.full_like(w, zero)
+    ex[:, :, 1:] = w[:, :, :-1]
+    run = np.full(s.shape[0], zero, dtype=dt)
+    wo = np.empty((s.shape[0], 8), dtype=dt)
+    for k in range(8):
+        wo[:, k] = run
+        run = run + w[:, k, 31]
+    return (wo[:, :, None] + ex).reshape(s.shape[0], 256), run
+
+
+def scan1d_cumsum(x: np.ndarray) -> np.ndarray:
+    """Exact model of the addition order of the engine's SCAN1D schedule for an ADD_ACCUMULATE of
+    a contiguous 1-D array. Chunks of 2048 elements; thread t of a chunk folds elements 8t..8t+7
+    in order from 0, a block scan of the 256 thread sums gives each thread's exclusive prefix e and
+    the chunk total. One CTA scans the chunk totals the same way, 2048 at a time with a running
+    carry, into the carry of every chunk. Element 8t+k of a chunk is then
+    carry + (e + (x[8t] + ... + x[8t+k])). Vectorised NumPy in the array's own dtype, so the
+    result is bit-exact."""
+    dt = x.dtype
+    zero = dt.type(0)
+    n = x.size
+    nch = -(-n // 2048)
+    pad = np.zeros(nch * 2048, dtype=dt)
+    pad[:n] = x
+    xs = pad.reshape(nch, 256, 8)
+    valid = (np.arange(nch * 2048) < n).reshape(nch, 256, 8)
+    s = np.full((nch, 256), zero, dtype=dt)
+    for k in range(8):
+        s = np.where(valid[:, :, k], s + xs[:, :, k], s)
+    e, totals = _block_scan(s)
+    carries = np.empty(nch, dtype=dt)
+    run = zero
+    for base in range(0, nch, 2048):
+        cnt = min(2048, nch - base)
+        g = np.zeros(2048, dtype=dt)
+        g[:cnt] = totals[base:base + cnt]
+        gv = g.reshape(256, 8)
+        ok = (np.arange(2048) < cnt).reshape(256, 8)
+        v = np.empty((256, 8), dtype=dt)
+        acc = np.full(256, zero, dtype=dt)
+        for k in range(8):
+            v[:, k] = acc
+            acc = np.where(ok[:, k], acc + gv[:, k], acc)
+        ge, gt = _block_scan(acc[None, :])
+        carries[base:base + cnt] = (run + (ge[0][:, None] + v)).reshape(-1)[:cnt]
+        run = run + gt[0]
+    out = np.empty((nch, 256, 8), dtype=dt)
+    r = np.full((nch, 256), zero, dtype=dt)
+    for k in range(8):
+        r = np.where(valid[:, :, k], r + xs[:, :, k], r)
+        out[:, :, k] = carries[:, None] + (e + r)
+    return out.reshape(-1)[:n]

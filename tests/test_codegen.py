@@ -158,6 +158,33 @@ def test_one_dimensional_accumulate_lowers_to_three_scan_units():
     assert [u["sched"] for u in units] == ["scan1d", "scan1d", "scan1d"], [u["sched"] for u in units]
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.int8, np.complex128])
+def test_scan_units_stage_elements_at_coalesced_positions(dtype):
+    """The chunk-total and re-scan units compute the accumulate's input at element k*256 + t of the
+    chunk in thread t and stage it in shared memory, from which thread t folds elements
+    8t..8t+7; instructions after the accumulate run at the coalesced positions again. Kept arrays
+    and the input array read after the accumulate compile for 1-, 8- and 16-byte elements."""
+    def kept(rt):
+        x = bh.empty(rt, (1_000_003,), dtype)
+        t = x * dtype(2) + dtype(1)
+        c = bh.accumulate("ADD_ACCUMULATE", t, 0)
+        return [t, c, c - t]
+
+    def recomputed(rt):
+        x = bh.empty(rt, (1_000_003,), dtype)
+        c = bh.accumulate("ADD_ACCUMULATE", x * dtype(2) + dtype(1), 0)
+        return [c, c - x * dtype(3)]
+
+    for prog in (kept, recomputed):
+        _, units = plan(prog)
+        assert [u["sched"] for u in units] == ["scan1d"] * 3
+        for phase in (0, 2):
+            src = units[phase]["source"]
+            assert "const int q = k * 256 + (int)threadIdx.x;" in src
+            assert "stage[q + (q >> 3)] = x;" in src
+        assert "= stage[q + (q >> 3)];" in units[2]["source"]
+
+
 def test_complex_programs_compile_for_every_schedule():
     """Complex64/complex128 kernels compile with NVRTC: every elementwise opcode of the complex
     type signatures, and reductions/accumulates on the GRID_REDUCE, SPLIT_REDUCE, LANE_REDUCE and

@@ -480,6 +480,58 @@ def test_scan1d(gpu_rt, oracle_rt, n, dtype, name):
         assert_close(a, b, tol, tol, what)
 
 
+@pytest.mark.parametrize("n,dtype", [(5, np.float64), (2049, np.float32), (1_000_003, np.float64),
+                                     (4_500_001, np.float32)])
+def test_scan1d_order_is_canonical(gpu_rt, n, dtype):
+    """SCAN1D adds in one fixed order (per-thread runs of 8, block scans, carries over the chunk
+    totals, more than one group of 2048 totals at 4.5M elements): the GPU cumulative sum of a
+    fused input equals the exact order model bit for bit."""
+    from tests.harness import scan1d_cumsum
+    x = np.random.default_rng(n).standard_normal(n).astype(dtype)
+
+    def prog(rt):
+        return [bh.accumulate("ADD_ACCUMULATE", bh.array(rt, x) * dtype(1) + dtype(0), 0)]
+    (got,) = run(gpu_rt, prog)
+    want = scan1d_cumsum(x)
+    assert np.asarray(got).tobytes() == want.tobytes()
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.int64])
+def test_scan1d_reads_values_from_before_the_accumulate(gpu_rt, oracle_rt, dtype):
+    """Instructions after the accumulate that read a kept array computed before it, or the
+    accumulate's own input array, against the oracle; float64 also bit for bit against the order
+    model."""
+    from tests.harness import scan1d_cumsum
+    n = 1_000_003
+    rng = np.random.default_rng(7)
+    host = rng.standard_normal(n) if dtype == np.float64 else rng.integers(-50, 50, n)
+    host = host.astype(dtype)
+
+    def kept(rt):
+        x = bh.array(rt, host)
+        t = x * dtype(2) + dtype(1)
+        c = bh.accumulate("ADD_ACCUMULATE", t, 0)
+        return [t, c, c - t]
+
+    def recomputed(rt):
+        x = bh.array(rt, host)
+        c = bh.accumulate("ADD_ACCUMULATE", x * dtype(2) + dtype(1), 0)
+        return [c, c - x * dtype(3)]
+
+    tol = 0 if dtype == np.int64 else 1e-11
+    g, o = both(gpu_rt, oracle_rt, kept)
+    for a, b, what in zip(g, o, ["kept", "scan", "after kept"]):
+        assert_close(a, b, tol, tol, what)
+    g2, o2 = both(gpu_rt, oracle_rt, recomputed)
+    for a, b, what in zip(g2, o2, ["scan", "after recomputed"]):
+        assert_close(a, b, tol, tol, what)
+    if dtype == np.float64:
+        t = host * 2.0 + 1.0
+        c = scan1d_cumsum(t)
+        assert g[1].tobytes() == c.tobytes() and g[2].tobytes() == (c - t).tobytes()
+        assert g2[0].tobytes() == c.tobytes() and g2[1].tobytes() == (c - host * 3.0).tobytes()
+
+
 @pytest.mark.parametrize("m,k,n,dtype,trans", [(64, 48, 80, np.float64, False), (300, 200, 100, np.float32, False),
                                                (128, 256, 64, np.float64, True)])
 def test_blas_extmethods_on_cublas(gpu_rt, m, k, n, dtype, trans):
