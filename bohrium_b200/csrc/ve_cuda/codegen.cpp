@@ -68,6 +68,7 @@ int64_t LaunchUnit::counters_needed() const {
     int64_t own = 0;
     if (sched == Sched::GRID_REDUCE) own = 1;
     if (sched == Sched::SPLIT_REDUCE) own = (rows * cols + kThreads - 1) / kThreads;
+    if (sched == Sched::SCAN1D && scan_gate) own = 1;
     return tail ? own + 1 : own;  // the tail's completion counter follows
 }
 
@@ -2287,8 +2288,10 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
 //   A  per chunk of 2048 elements: the accumulate's inputs are computed on the fly at coalesced
 //      positions and staged in shared memory; thread t folds elements 8t..8t+7 of the chunk in
 //      order from there, and a fixed block scan of the 256 thread totals gives the chunk total;
-//   B  one CTA: exclusive scan of the chunk totals (groups of 2048, the same block scan, a running
-//      carry) -> the carry into every chunk;
+//   B  per group of 2048 chunk totals: the same per-thread fold and block scan -> each chunk's
+//      exclusive prefix within its group, and the group total; the CTA that finishes last folds
+//      the group totals in order -> the carry into every group. A chunk's carry is its group's
+//      carry op its prefix within the group;
 //   C  per chunk: the same staging, per-thread fold and block scan; element value = carry op
 //      (exclusive thread prefix op running thread prefix), staged again and written out at
 //      coalesced positions, where the instructions after the accumulate run on it.
@@ -2368,6 +2371,7 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
     const LoopB &L = holder.getLoop();
     const int64_t n = L.size;
     const int64_t nchunks = (n + kScanTile - 1) / kScanTile;
+    const int64_t ngroups = (nchunks + kScanTile - 1) / kScanTile;  // groups of chunk totals
     const bh_type t = acc->operand[0].base->dtype();
     const string T = cuda_type(t);
     const bh_opcode rop = scan_reduce_op(acc->opcode);
@@ -2377,14 +2381,19 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
         LaunchUnit u;
         u.sched = Sched::SCAN1D;
         u.cols = n;
-        u.chunks = phase == 1 ? 1 : nchunks;  // work items
+        u.chunks = phase == 1 ? ngroups : nchunks;  // work items
         Symbols sym = build_symbols({&holder}, {});
         ParamLayout pl;
         add_common_fields(sym, pl, opt);
         pl.add(work_field(nchunks), "bh_i64", "nchunks");
-        pl.add(work_field(phase == 1 ? 1 : nchunks), "bh_i64", "work");
+        pl.add(work_field(phase == 1 ? ngroups : nchunks), "bh_i64", "work");
         ParamField fs{ParamField::SCRATCH};
         pl.add(fs, "unsigned char*", "scratch");
+        if (phase == 1) {
+            ParamField fc{ParamField::COUNTER};
+            pl.add(fc, "unsigned int*", "counter");
+            u.scan_gate = true;
+        }
         stringstream body;
         Emitter em(sym, body, opt);
         body << block_scan_fn(T, "bh_block_scan", rop, ident);
@@ -2413,28 +2422,44 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
             }
         };
         if (phase == 1) {
-            body << "    if (c != 0) return;\n";
-            body << "    " << T << " run = " << ident << ";\n";
-            body << "    for (bh_i64 base = 0; base < p.nchunks; base += " << kScanTile << ") {\n";
-            body << "        " << T << " v[" << kScanPerThread << "];\n";
-            body << "        " << T << " s = " << ident << ";\n";
+            // Work item g scans chunk totals 2048g..2048g+2047 into carries local to the group
+            // and stores the group total; the CTA that finishes last folds the group totals in
+            // group order into the carry of every group.
+            body << "    " << T << "* gtot = carries + p.nchunks;\n";
+            body << "    " << T << "* grun = gtot + p.work;\n";
+            body << "    __shared__ bool am_last;\n";
+            body << "    const bh_i64 base = c * " << kScanTile << ";\n";
+            body << "    " << T << " v[" << kScanPerThread << "];\n";
+            body << "    " << T << " s = " << ident << ";\n";
             body << "#pragma unroll\n";
-            body << "        for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
-            body << "            const bh_i64 j = base + threadIdx.x * " << kScanPerThread << " + k;\n";
-            body << "            v[k] = s;\n";  // exclusive running prefix
-            body << "            if (j < p.nchunks) { const " << T << " x = totals[j]; s = " << reduce_expr(rop, "s", "x")
+            body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+            body << "        const bh_i64 j = base + threadIdx.x * " << kScanPerThread << " + k;\n";
+            body << "        v[k] = s;\n";  // exclusive running prefix
+            body << "        if (j < p.nchunks) { const " << T << " x = totals[j]; s = " << reduce_expr(rop, "s", "x")
                  << "; }\n";
-            body << "        }\n";
-            body << "        " << T << " total;\n";
-            body << "        const " << T << " e = bh_block_scan(s, total, sm);\n";
+            body << "    }\n";
+            body << "    " << T << " total;\n";
+            body << "    const " << T << " e = bh_block_scan(s, total, sm);\n";
             body << "#pragma unroll\n";
-            body << "        for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
-            body << "            const bh_i64 j = base + threadIdx.x * " << kScanPerThread << " + k;\n";
-            body << "            const " << T << " inner = " << reduce_expr(rop, "e", "v[k]") << ";\n";
-            body << "            if (j < p.nchunks) carries[j] = " << reduce_expr(rop, "run", "inner") << ";\n";
+            body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+            body << "        const bh_i64 j = base + threadIdx.x * " << kScanPerThread << " + k;\n";
+            body << "        if (j < p.nchunks) carries[j] = " << reduce_expr(rop, "e", "v[k]") << ";\n";
+            body << "    }\n";
+            body << "    if (threadIdx.x == 0) {\n";
+            body << "        gtot[c] = total;\n";
+            body << "        am_last = bh_arrive(p.counter) == (unsigned)(p.work - 1);\n";
+            body << "    }\n";
+            body << "    __syncthreads();\n";
+            body << "    if (!am_last) return;\n";
+            body << "    bh_acquire();\n";
+            body << "    if (threadIdx.x == 0) {\n";
+            body << "        " << T << " run = " << ident << ";\n";
+            body << "        for (bh_i64 g = 0; g < p.work; ++g) {\n";
+            body << "            grun[g] = run;\n";
+            body << "            const " << T << " t = bh_ldcg(gtot + g);\n";
+            body << "            run = " << reduce_expr(rop, "run", "t") << ";\n";
             body << "        }\n";
-            body << "        run = " << reduce_expr(rop, "run", "total") << ";\n";
-            body << "        __syncthreads();\n";
+            body << "        *p.counter = 0u;\n";
             body << "    }\n";
             body << "}\n" << kWrappers;
         } else {
@@ -2499,7 +2524,10 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
                 body << "    if (threadIdx.x == 0) totals[c] = total;\n";
                 body << "}\n" << kWrappers;
             } else {
-                body << "    const " << T << " carry = carries[c];\n";
+                body << "    const " << T << "* grun = carries + p.nchunks + (p.nchunks + " << kScanTile - 1 << ") / "
+                     << kScanTile << ";\n";
+                body << "    const " << T << " carry = " << reduce_expr(rop, "grun[c / " + to_string(kScanTile) + "]", "carries[c]")
+                     << ";\n";
                 body << "    " << T << " r = " << ident << ";\n";
                 body << "#pragma unroll\n";
                 body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
@@ -2534,12 +2562,12 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
         }
         u.fields = pl.fields;
         u.scratch_bytes_per_tile = 0;
-        u.scan_bytes_per_chunk = 2 * static_cast<int64_t>(bh_type_size(t));
+        // chunk totals, chunk carries, group totals, group carries
+        u.scan_bytes = 2 * (nchunks + ngroups) * static_cast<int64_t>(bh_type_size(t));
         u.algorithmic_bytes = phase == 2 ? unit_bytes(sym, vector<const Block *>{&holder}) : 0;
         u.elements = phase == 1 ? nchunks : n;
         if (phase == 2) u.red_orders.emplace_back(acc->origin_id, "scan:" + to_string(kScanTile) + ":" + to_string(n));
         finish_source(u, pl.decl.str(), body.str(), opt);
-        u.scan_chunks = nchunks;
         units.push_back(std::move(u));
     }
     return units;

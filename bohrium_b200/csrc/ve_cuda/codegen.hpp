@@ -75,11 +75,11 @@ struct LaunchUnit {
     int nred = 0;               // GRID_REDUCE / SPLIT_REDUCE: number of reductions
     int64_t scratch_bytes_per_tile = 0; // GRID_REDUCE: bytes of partials per tile (all reductions)
     int slot_bytes = 8;         // GRID_REDUCE / SPLIT_REDUCE: bytes of one partial (16 with complex128)
-    int64_t scan_bytes_per_chunk = 16; // SCAN1D: total + carry of one chunk in the scan arena
     int64_t chunks = 1;         // SPLIT_REDUCE: chunks of the swept axis; LANE_REDUCE: lanes per point;
                                 // GRID_REDUCE: tiles per work item; SCAN1D: work items of the phase
-    int64_t scan_chunks = 0;    // SCAN1D: chunks of 2048 elements
-    int64_t scan_offset = 0;    // SCAN1D: offset of its totals/carries in the scan arena (set by the plan)
+    int64_t scan_bytes = 0;     // SCAN1D: its chunk totals and carries and group totals and carries
+    int64_t scan_offset = 0;    // SCAN1D: offset of scan_bytes in the scan arena (set by the plan)
+    bool scan_gate = false;     // SCAN1D carry unit: one completion counter
     // The parameter members and the device code (without the kernel wrappers) of the source;
     // body_core is empty for sources with wrappers of their own.
     std::string params_decl, body_core;

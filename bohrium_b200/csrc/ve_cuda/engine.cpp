@@ -1050,7 +1050,7 @@ EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const
             for (LaunchUnit &u : units) {
                 if (u.sched != Sched::SCAN1D) continue;
                 u.scan_offset = plan.scan_bytes;
-                scan_need = max<int64_t>(scan_need, (u.scan_bytes_per_chunk * u.scan_chunks + 255) / 256 * 256);
+                scan_need = max<int64_t>(scan_need, (u.scan_bytes + 255) / 256 * 256);
             }
             plan.scan_bytes += scan_need;
             for (LaunchUnit &u : units) {
