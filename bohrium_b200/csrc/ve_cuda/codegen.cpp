@@ -2510,11 +2510,12 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
             body << "    __syncthreads();\n";
             // Thread t folds elements 8t..8t+7 of the chunk in order.
             body << "    " << T << " s = " << ident << ";\n";
+            body << "    " << T << " xs[" << kScanPerThread << "];\n";
             body << "#pragma unroll\n";
             body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
             body << "        const int q = (int)threadIdx.x * " << kScanPerThread << " + k;\n";
-            body << "        if (cbase + q < " << n0 << ") { const " << T << " x = stage[q + (q >> 3)]; s = "
-                 << reduce_expr(rop, "s", "x") << "; }\n";
+            body << "        xs[k] = stage[q + (q >> 3)];\n";
+            body << "        if (cbase + q < " << n0 << ") s = " << reduce_expr(rop, "s", "xs[k]") << ";\n";
             body << "    }\n";
             // The block scan's first barrier orders these stage reads before any later stage write.
             body << "    " << T << " total;\n";
@@ -2531,11 +2532,8 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
                 body << "#pragma unroll\n";
                 body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
                 body << "        const int j = (int)threadIdx.x * " << kScanPerThread << " + k;\n";
-                // The inputs are read from the stage again rather than kept in registers across
-                // the block scan: thread t alone reads and rewrites slots 8t..8t+7 here.
                 body << "        if (cbase + j < " << n0 << ") {\n";
-                body << "            const " << T << " x = stage[j + (j >> 3)];\n";
-                body << "            r = " << reduce_expr(rop, "r", "x") << ";\n";
+                body << "            r = " << reduce_expr(rop, "r", "xs[k]") << ";\n";
                 body << "            const " << T << " inner = " << reduce_expr(rop, "e", "r") << ";\n";
                 body << "            stage[j + (j >> 3)] = " << reduce_expr(rop, "carry", "inner") << ";\n";
                 body << "        }\n";
