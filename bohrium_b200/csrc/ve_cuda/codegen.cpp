@@ -2508,7 +2508,9 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
             };
             stage_pass(true, "in");
             body << "    __syncthreads();\n";
-            // Thread t folds elements 8t..8t+7 of the chunk in order.
+            // Thread t folds elements 8t..8t+7 of the chunk in order. The re-scan keeps them in
+            // registers across the block scan: reading them back from the stage instead cut the
+            // float64 re-scan from 64 to 48 registers but measured 4 % slower per flush.
             body << "    " << T << " s = " << ident << ";\n";
             body << "    " << T << " xs[" << kScanPerThread << "];\n";
             body << "#pragma unroll\n";
