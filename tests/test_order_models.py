@@ -1,0 +1,100 @@
+"""The exact order models of tests/harness.py on the CPU: integer inputs, where every order gives
+the same result, pin their structure (tiles, chunks, groups of chunk totals, carries); float
+inputs stay within the rounding error of a long sum; and a scalar transcription of the SCAN1D
+unit steps (thread folds, shuffle scan, warp offsets, carries) agrees bit for bit on small cases.
+The GPU tests compare the engine with the same models bit for bit."""
+import numpy as np
+import pytest
+
+from tests.harness import grid_reduce_sum, scan1d_cumsum
+
+
+def _scalar_block_scan(vals, zero):
+    """One CTA's block scan written out per thread: returns (exclusive prefixes, total)."""
+    x = list(vals)
+    for d in (1, 2, 4, 8, 16):
+        prev = list(x)
+        for t in range(256):
+            if t % 32 >= d:
+                x[t] = prev[t - d] + prev[t]
+    ex = [zero if t % 32 == 0 else x[t - 1] for t in range(256)]
+    run, wo = zero, []
+    for w in range(8):
+        wo.append(run)
+        run = run + x[32 * w + 31]
+    return [wo[t // 32] + ex[t] for t in range(256)], run
+
+
+def _scalar_scan1d(x):
+    dt = x.dtype.type
+    zero = dt(0)
+    n = x.size
+    nch = -(-n // 2048)
+    totals, prefixes = [], []
+    for c in range(nch):
+        sums = []
+        for t in range(256):
+            s = zero
+            for k in range(8):
+                i = 2048 * c + 8 * t + k
+                if i < n:
+                    s = s + x[i]
+            sums.append(s)
+        e, tot = _scalar_block_scan(sums, zero)
+        totals.append(tot)
+        prefixes.append(e)
+    carries = [zero] * nch
+    run = zero
+    for base in range(0, nch, 2048):
+        v = [[zero] * 8 for _ in range(256)]
+        sums = []
+        for t in range(256):
+            s = zero
+            for k in range(8):
+                j = base + 8 * t + k
+                v[t][k] = s
+                if j < nch:
+                    s = s + totals[j]
+            sums.append(s)
+        e, tot = _scalar_block_scan(sums, zero)
+        for t in range(256):
+            for k in range(8):
+                j = base + 8 * t + k
+                if j < nch:
+                    carries[j] = run + (e[t] + v[t][k])
+        run = run + tot
+    out = np.empty(n, dtype=x.dtype)
+    for c in range(nch):
+        for t in range(256):
+            r = zero
+            for k in range(8):
+                i = 2048 * c + 8 * t + k
+                if i < n:
+                    r = r + x[i]
+                    out[i] = carries[c] + (prefixes[c][t] + r)
+    return out
+
+
+@pytest.mark.parametrize("n", [1, 7, 2047, 2048, 2049, 6000])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_scan_model_matches_scalar_transcription(n, dtype):
+    x = np.random.default_rng(n).standard_normal(n).astype(dtype)
+    assert scan1d_cumsum(x).tobytes() == _scalar_scan1d(x).tobytes()
+
+
+@pytest.mark.parametrize("n", [1, 2049, 300_001, 4_194_304, 4_194_305, 9_000_001])
+def test_scan_model_is_a_cumulative_sum(n):
+    """Integers: exact at every length, across one and several groups of 2048 chunk totals."""
+    x = np.random.default_rng(n).integers(-1000, 1000, n).astype(np.int64)
+    assert np.array_equal(scan1d_cumsum(x), np.cumsum(x))
+    f = np.random.default_rng(n).random(n)
+    want = np.cumsum(f.astype(np.longdouble))
+    assert np.max(np.abs(scan1d_cumsum(f) - want)) <= 1e-12 * max(1.0, float(want[-1]))
+
+
+@pytest.mark.parametrize("n", [1, 2048, 2049, 1_000_003, 3_000_017])
+def test_grid_reduce_model_is_a_sum(n):
+    x = np.random.default_rng(n).integers(-1000, 1000, n).astype(np.int64)
+    assert grid_reduce_sum(x) == x.sum()
+    f = np.random.default_rng(n).random(n)
+    assert abs(float(grid_reduce_sum(f)) - float(np.sum(f.astype(np.longdouble)))) <= 1e-12 * n
