@@ -10,11 +10,11 @@ from .runtime import NativeExecutor, Runtime, load_library
 from .array import (BhArray, empty, full, zeros, ones, array, arange, random123, random_sample, binary, unary,
                     reduce, accumulate, gather, scatter, sqrt, exp, log, sin, cos, tanh, absolute, floor, sign,
                     maximum, minimum, where, true_divide, matmul, extmethod_opcode, tan, sinh, cosh, log10, real,
-                    imag, conj)
+                    imag, conj, user_kernel, make_behaving, is_behaving)
 from .inspect import DryRunExecutor, dry_run
 
 __all__ = ["ir", "NativeExecutor", "Runtime", "load_library", "BhArray", "empty", "full", "zeros", "ones", "array",
            "arange", "random123", "random_sample", "binary", "unary", "reduce", "accumulate", "gather", "scatter",
            "sqrt", "exp", "log", "sin", "cos", "tanh", "absolute", "floor", "sign", "maximum", "minimum", "where",
            "true_divide", "matmul", "extmethod_opcode", "tan", "sinh", "cosh", "log10", "real", "imag", "conj",
-           "DryRunExecutor", "dry_run"]
+           "user_kernel", "make_behaving", "is_behaving", "DryRunExecutor", "dry_run"]

@@ -485,3 +485,56 @@ def matmul(a: BhArray, b: BhArray, trans_a: bool = False) -> BhArray:
     op = extmethod_opcode(a.rt, "blas_gemmt" if trans_a else "blas_gemm")
     a.rt.enqueue(ir.Instr(op, [out.view(), a.view(), b.view()]))
     return out
+
+
+def is_behaving(a: BhArray) -> bool:
+    """A behaving array is C-contiguous, starts at the first element of its base and covers all
+    of it, so a user kernel can index it without offsets or strides (the reference's
+    `_bh.is_array_behaving`, used by bridge/npbackend/bohrium/user_kernel.py:62-71)."""
+    return a.start == 0 and a.is_contiguous() and a.size == a.base.nelem
+
+
+def make_behaving(a: BhArray, dtype=None) -> BhArray:
+    """`a` (converted to `dtype`), copied if it is not behaving
+    (bridge/npbackend/bohrium/user_kernel.py:120-150)."""
+    if dtype is not None:
+        a = a.astype(dtype)
+    return a if is_behaving(a) else a.copy()
+
+
+def _param_string(param) -> str:
+    """{"global_work_size": (20, 5), ...} -> "global_work_size: 20 5; ..." (as the reference's
+    front end builds it, bridge/npbackend/bohrium/user_kernel.py:76-83)."""
+    parts = []
+    for key, value in (param or {}).items():
+        if isinstance(value, (list, tuple)):
+            value = " ".join(str(v) for v in value)
+        parts.append(f"{key}: {value}")
+    return "; ".join(parts)
+
+
+def user_kernel(kernel_source: str, operand_list: Sequence[BhArray], compiler_command: Optional[str] = None,
+                tag: str = "openmp", param=None, only_behaving_operands: bool = True) -> None:
+    """Compile and run the function `execute` of `kernel_source` with the arrays of `operand_list`
+    as its arguments (bohrium.user_kernel.execute, bridge/npbackend/bohrium/user_kernel.py:21-89).
+
+    Pending bytecode is flushed first. With tag "cuda" the stack's CUDA engine compiles the source
+    with NVRTC: `execute` must be an `extern "C" __global__` function taking one pointer per
+    operand, and `param` gives "global_work_size" and "local_work_size" (up to three dimensions,
+    the global size a multiple of the local size). Raises RuntimeError with the engine's message
+    when compilation or the launch fails, and TypeError for an operand that is not behaving
+    unless `only_behaving_operands` is False."""
+    ops = list(operand_list)
+    if not ops:
+        raise ValueError("user_kernel: operand_list is empty")
+    for op in ops:
+        if not isinstance(op, BhArray):
+            raise TypeError("All operands in `operand_list` must be Bohrium arrays")
+        if only_behaving_operands and not is_behaving(op):
+            raise TypeError("Operand is not behaving set `only_behaving_operands=False` or use `make_behaving()`")
+    rt = ops[0].rt
+    rt.flush()
+    msg = rt.ex.user_kernel(kernel_source, [op.base for op in ops], compiler_command or "", tag,
+                            _param_string(param))
+    if msg:
+        raise RuntimeError(msg)

@@ -251,6 +251,21 @@ int bhb_extmethod(bhb_runtime *rt, const char *name, int64_t opcode) {
     });
 }
 
+const char *bhb_user_kernel(bhb_runtime *rt, const char *kernel, int64_t nop, bh_base *const *operands,
+                            const char *compile_cmd, const char *tag, const char *param) {
+    const int r = guarded([&] {
+        if (kernel == nullptr || tag == nullptr) throw runtime_error("bhb_user_kernel: kernel and tag are required");
+        if (nop < 0 || (nop > 0 && operands == nullptr)) throw runtime_error("bhb_user_kernel: bad operand list");
+        vector<bh_view> ops;
+        for (int64_t i = 0; i < nop; ++i) {
+            if (operands[i] == nullptr) throw runtime_error("bhb_user_kernel: null operand");
+            ops.emplace_back(operands[i]);
+        }
+        rt->message = rt->child.userKernel(kernel, ops, compile_cmd ? compile_cmd : "", tag, param ? param : "");
+    });
+    return r == 0 ? rt->message.c_str() : nullptr;
+}
+
 void *bhb_get_device_context(bhb_runtime *rt) {
     void *r = nullptr;
     guarded([&] { r = rt->child.getDeviceContext(); });

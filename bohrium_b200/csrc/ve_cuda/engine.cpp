@@ -1344,6 +1344,108 @@ void slide_views(BhIR *bhir) {
 }
 } // namespace
 
+// ------------------------------------------------------------------------------------- user kernels
+namespace {
+// The integers after "<option>:" in a user-kernel parameter string such as
+// "global_work_size: 20 5; local_work_size: 1 1": digits separated by spaces, tabs, newlines or
+// commas, up to the first other character. Empty when the option is absent or a number does not
+// fit. The same reading as the reference's OpenCL engine (ve/opencl/engine_opencl.cpp:588-608).
+vector<int64_t> param_integers(const string &option, const string &param) {
+    const size_t at = param.find(option + ":");
+    if (at == string::npos) return {};
+    vector<int64_t> out;
+    string tok;
+    auto flush_tok = [&]() {
+        if (tok.empty()) return true;
+        if (tok.size() > 18) return false;
+        out.push_back(stoll(tok));
+        tok.clear();
+        return true;
+    };
+    for (size_t i = at + option.size() + 1; i < param.size(); ++i) {
+        const char ch = param[i];
+        if (ch >= '0' && ch <= '9') {
+            tok += ch;
+        } else if (ch == ' ' || ch == '\t' || ch == '\n' || ch == '\r' || ch == ',') {
+            if (!flush_tok()) return {};
+        } else {
+            break;
+        }
+    }
+    if (!flush_tok()) return {};
+    return out;
+}
+} // namespace
+
+string EngineCUDA::userKernel(const string &kernel, vector<bh_view> &operands, const string &param) {
+    for (const bh_view &op : operands)
+        if (op.isConstant()) return "[UserKernel] fatal error - operands cannot be constants";
+    const vector<int64_t> global = param_integers("global_work_size", param);
+    const vector<int64_t> local = param_integers("local_work_size", param);
+    if (global.size() != local.size())
+        return "[CUDA] userKernel-param dimension of global_work_size and local_work_size must be the same";
+    if (global.empty() || global.size() > 3) return "[CUDA] userKernel-param maximum of three dimensions!";
+    // Dimension d of the work sizes is CUDA's x, y, z: a block of local_work_size threads, and
+    // global_work_size / local_work_size blocks (a whole number, as OpenCL 1.x requires).
+    unsigned grid[3] = {1, 1, 1}, block[3] = {1, 1, 1};
+    const int64_t max_block[3] = {1024, 1024, 64}, max_grid[3] = {2147483647, 65535, 65535};
+    int64_t threads = 1;
+    for (size_t d = 0; d < global.size(); ++d) {
+        if (local[d] <= 0 || global[d] <= 0 || global[d] % local[d] != 0)
+            return "[CUDA] userKernel-param global_work_size must be a positive multiple of local_work_size";
+        if (local[d] > max_block[d] || global[d] / local[d] > max_grid[d])
+            return "[CUDA] userKernel-param work size beyond the device's block or grid limits";
+        block[d] = static_cast<unsigned>(local[d]);
+        grid[d] = static_cast<unsigned>(global[d] / local[d]);
+        threads *= local[d];
+    }
+    if (threads > 1024) return "[CUDA] userKernel-param local_work_size has more than 1024 threads";
+
+    const uint64_t h = fnv1a(kernel.data(), kernel.size());
+    void *fn = nullptr;
+    auto it = user_functions.find(h);
+    if (it != user_functions.end()) {
+        fn = it->second;
+    } else {
+        const auto t0 = chrono::steady_clock::now();
+        vector<char> cubin;
+        try {
+            cubin = cubin_for("bh_user_kernel", kernel, 0);
+        } catch (const exception &e) {
+            return string("[CUDA] userKernel compilation failed: ") + e.what();
+        }
+        CUmodule mod;
+        CUfunction f;
+        if (api->cuModuleLoadData(&mod, cubin.data()) != CUDA_SUCCESS) return "[CUDA] userKernel: cuModuleLoadData failed";
+        if (api->cuModuleGetFunction(&f, mod, "execute") != CUDA_SUCCESS)
+            return "[CUDA] userKernel: the source defines no extern \"C\" __global__ function named execute";
+        fn = reinterpret_cast<void *>(f);
+        user_functions[h] = fn;
+        _stats.time_compile += seconds_since(t0);
+    }
+    // One device pointer per operand: the start of its base array, as the reference's engines
+    // pass whole buffers (ve/opencl/engine_opencl.cpp:628-630, ve/openmp/engine_openmp.cpp:503-506).
+    vector<void *> ptrs(operands.size()), args(operands.size());
+    for (size_t i = 0; i < operands.size(); ++i) {
+        ptrs[i] = getBuffer(operands[i].base);
+        args[i] = &ptrs[i];
+    }
+    const auto t0 = chrono::steady_clock::now();
+    const CUresult r = api->cuLaunchKernel(reinterpret_cast<CUfunction>(fn), grid[0], grid[1], grid[2], block[0], block[1],
+                                           block[2], 0, reinterpret_cast<CUstream>(_stream),
+                                           args.empty() ? nullptr : args.data(), nullptr);
+    if (r != CUDA_SUCCESS) {
+        const char *msg = "?";
+        api->cuGetErrorString(r, &msg);
+        return string("[CUDA] userKernel launch failed: ") + msg;
+    }
+    ++_stats.launches;
+    synchronize();
+    _stats.time_exec_host += seconds_since(t0);
+    for (const bh_view &op : operands) mark_device_written(op.base);
+    return "";
+}
+
 void EngineCUDA::execute(BhIR *bhir) {
     ++_stats.flushes;
     bh_base *cond = bhir->getRepeatCondition();

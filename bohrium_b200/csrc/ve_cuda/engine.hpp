@@ -68,6 +68,11 @@ public:
     void execute(BhIR *bhir);                  // the repeat loop of one flush
     void handleExecution(BhIR *bhir);          // one pass over the instruction list
     void handleExtmethod(BhIR *bhir);          // split around extension methods
+    // ComponentImpl::userKernel with tag "cuda": compile `kernel` with NVRTC, run its
+    // `extern "C" __global__ void execute(...)` with one device pointer per operand base, on a grid
+    // given by `param` ("global_work_size: ...; local_work_size: ..."), and wait for it. Returns ""
+    // on success, else the error text.
+    std::string userKernel(const std::string &kernel, std::vector<bh_view> &operands, const std::string &param);
 
     // Memory interface (ComponentImpl methods are thin wrappers).
     void *getMemoryPointer(bh_base &base, bool copy2host, bool force_alloc, bool nullify);
@@ -173,6 +178,7 @@ private:
     // Kernel cache: source hash -> compiled kernels; cubins compiled ahead of loading
     std::unordered_map<uint64_t, Compiled> functions;
     std::unordered_map<uint64_t, std::vector<char>> ahead;
+    std::unordered_map<uint64_t, void *> user_functions; // user-kernel source hash -> its execute()
     std::string disk_cache_path(const std::string &source, int maxrreg = 0) const; // "" without a cache dir
     Compiled::Variant load_variant(const std::vector<char> &cubin, const std::string &name, int maxrreg,
                                    int dyn_smem = 0);

@@ -120,7 +120,9 @@ public:
 
     string userKernel(const string &kernel, vector<bh_view> &operand_list, const string &compile_cmd,
                       const string &tag, const string &param) override {
-        if (tag == "cuda") throw runtime_error("[CUDA] userKernel not implemented, set tag \"openmp\"");
+        // The reference's ve/cuda throws for tag "cuda" (ve/cuda/main.cpp:111-121); this engine
+        // compiles and runs the kernel on the device, as its OpenCL engine does for "opencl".
+        if (tag == "cuda") return engine.userKernel(kernel, operand_list, param);
         for (const bh_view &op : operand_list) engine.copyToHost({op.base}, true);
         return child.userKernel(kernel, operand_list, compile_cmd, tag, param);
     }

@@ -56,6 +56,8 @@ def load_library():
         "bhb_get_device_context": (P, [P]),
         "bhb_set_device_context": (I, [P, P]),
         "bhb_last_execute_ms": (ctypes.c_double, [P]),
+        "bhb_user_kernel": (ctypes.c_char_p, [P, ctypes.c_char_p, I64, P, ctypes.c_char_p, ctypes.c_char_p,
+                                              ctypes.c_char_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -170,6 +172,16 @@ class NativeExecutor:
 
     def last_execute_ms(self) -> float:
         return float(self.lib.bhb_last_execute_ms(self.rt))
+
+    def user_kernel(self, kernel: str, bases, compile_cmd: str, tag: str, param: str) -> str:
+        """ComponentImpl::userKernel through bhb_user_kernel: the component's message ("" on
+        success, else the error text)."""
+        handles = (ctypes.c_void_p * max(len(bases), 1))(*[b.handle for b in bases])
+        r = self.lib.bhb_user_kernel(self.rt, kernel.encode(), len(bases), handles, compile_cmd.encode(),
+                                     tag.encode(), param.encode())
+        if r is None:
+            raise RuntimeError("bhb_user_kernel: " + _err(self.lib))
+        return r.decode()
 
 
 class NativeIR:

@@ -88,6 +88,19 @@ const char *bhb_message(bhb_runtime *rt, const char *msg);
 /* ComponentImpl::extmethod (bhc_extmethod): register extension method `name` as `opcode`
  * (> BH_MAX_OPCODE_ID). */
 int bhb_extmethod(bhb_runtime *rt, const char *name, int64_t opcode);
+/* ComponentImpl::userKernel (replaces bhc_user_kernel, bridge/c/gen_specials.py:287-304, and
+ * bhxx::Runtime::userKernel, bridge/cxx/src/Runtime.cpp:131-138): compile `kernel` and run its
+ * function `execute` with one argument per operand, the start of that base's data, in order. The
+ * caller flushes pending bytecode first, as the reference's front end does. Tag "cuda" runs on
+ * this engine: `execute` is an `extern "C" __global__` function compiled with NVRTC for sm_100a,
+ * launched with blocks of local_work_size threads and global_work_size / local_work_size blocks,
+ * both taken from `param` ("global_work_size: 1024; local_work_size: 128", up to three numbers
+ * each); `compile_cmd` is not used. Other tags go down the stack. Returns the component's message:
+ * "" on success, else the error text (which the reference's front end raises); NULL when the call
+ * itself failed (bhb_last_error). The string stays valid until the next call on the same
+ * runtime. */
+const char *bhb_user_kernel(bhb_runtime *rt, const char *kernel, int64_t nop, bh_base *const *operands,
+                            const char *compile_cmd, const char *tag, const char *param);
 /* ComponentImpl::getDeviceContext / setDeviceContext. */
 void *bhb_get_device_context(bhb_runtime *rt);
 int bhb_set_device_context(bhb_runtime *rt, void *ctx);
