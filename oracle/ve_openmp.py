@@ -415,6 +415,29 @@ def _compile(source: str):
     return fn
 
 
+def _compile_user(source: str):
+    """A user kernel's source with its launcher, compiled like the oracle's own kernels; returns
+    the launcher `_bh_launcher(void *data_list[])`."""
+    global _workdir
+    h = "u" + hashlib.sha1((" ".join(CFLAGS) + source).encode()).hexdigest()[:20]
+    if h in _compiled:
+        return _compiled[h]
+    if _workdir is None:
+        _workdir = tempfile.mkdtemp(prefix="bh_oracle_")
+    src = os.path.join(_workdir, h + ".c")
+    so = os.path.join(_workdir, h + ".so")
+    with open(src, "w") as f:
+        f.write(source)
+    r = subprocess.run([CC] + CFLAGS + [src, "-o", so, "-lm"], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("[UserKernel] compilation failed:\n" + r.stderr)
+    fn = ctypes.CDLL(so)._bh_launcher
+    fn.restype = None
+    fn.argtypes = [ctypes.c_void_p]
+    _compiled[h] = fn
+    return fn
+
+
 def set_threads(n: int) -> None:
     try:
         lib = ctypes.CDLL("libgomp.so.1")
@@ -461,6 +484,27 @@ class OracleExecutor:
             a = np.zeros(max(base.nelem, 1), dtype=base.dtype)
             self.store[base.id] = a
         return a
+
+    def user_kernel(self, kernel: str, bases, compile_cmd: str, tag: str, param: str) -> str:
+        """ComponentImpl::userKernel of ve/openmp (ve/openmp/engine_openmp.cpp:484-530): the
+        source plus a launcher that casts each operand's data to its C type and calls
+        `execute(a0, a1, ...)`, compiled and run on the host. Only tag "openmp"; the oracle's own
+        compiler flags replace `compile_cmd`. Returns "" or the error text."""
+        if tag != "openmp":
+            return f'[UserKernel] the oracle runs tag "openmp" only, not "{tag}"'
+        lines = [kernel, "void _bh_launcher(void *data_list[]) {"]
+        for i, b in enumerate(bases):
+            lines.append(f"    {ctype(b.dtype)} *a{i} = data_list[{i}];")
+        lines.append("    execute(" + ", ".join(f"a{i}" for i in range(len(bases))) + ");")
+        lines.append("}")
+        try:
+            fn = _compile_user("\n".join(lines) + "\n")
+        except RuntimeError as e:
+            return str(e)
+        arrays = [self._array(b) for b in bases]
+        ptrs = (ctypes.c_void_p * max(len(arrays), 1))(*[a.ctypes.data for a in arrays])
+        fn(ptrs)
+        return ""
 
     # execution ---------------------------------------------------------------------------
     def execute(self, flush: ir.Flush) -> None:

@@ -1,6 +1,6 @@
-"""User kernels: the front end's checks and parameter string, with no GPU (the reference's
-bridge/npbackend/bohrium/user_kernel.py:21-150). The kernels themselves run in
-tests/test_user_kernel_gpu.py."""
+"""User kernels with no GPU: the front end's checks and parameter string (the reference's
+bridge/npbackend/bohrium/user_kernel.py:21-150), and the reference's openmp user-kernel test on
+the oracle. The CUDA kernels run in tests/test_user_kernel_gpu.py."""
 import numpy as np
 import pytest
 
@@ -42,3 +42,23 @@ def test_param_string_matches_the_reference_front_end():
     assert _param_string({"global_work_size": 1024, "local_work_size": [128]}) == \
         "global_work_size: 1024; local_work_size: 128"
     assert _param_string(None) == ""
+
+
+def test_openmp_user_kernel_on_the_oracle(oracle_rt):
+    """The reference's own openmp user-kernel test (test/python/tests/test_user_kernel.py) on the
+    oracle's restatement of ve/openmp's userKernel."""
+    kernel = r"""
+#include <stdint.h>
+void execute(double *a, double *b, double *c) {
+    for (uint64_t i = 0; i < 100; ++i) {
+        c[i] = a[i] + b[i] + i;
+    }
+}
+"""
+    a = bh.ones(oracle_rt, (100,), np.float64)
+    b = bh.make_behaving(bh.ones(oracle_rt, (110,), np.float64)[10:])
+    res = bh.empty(oracle_rt, (100,), np.float64)
+    bh.user_kernel(kernel, [a, b, res])
+    np.testing.assert_array_equal(res.numpy(), 2.0 + np.arange(100))
+    with pytest.raises(RuntimeError, match="compilation failed"):
+        bh.user_kernel("void execute(double *a) { a[0] = ; }", [a])
