@@ -14,7 +14,7 @@ against it. Nothing in bohrium_b200/ imports it, and the product never runs it.
                  header) to pin kernel_deps.h
 
 Parity pins: the Philox restatement is checked against oracle/_ref (the reference's own header,
-compiled from /root/reference) and against the known-answer vector (counter 0, key 42) ->
+compiled in place by oracle/Makefile) and against the known-answer vector (counter 0, key 42) ->
 (624017136, 4231775638); operation semantics are checked against NumPy, the witness the
 reference's own test-suite uses (test/python/run.py:42-59), in tests/test_oracle.py; golden
 vectors generated with the reference header live in tests/golden/.
