@@ -1,5 +1,6 @@
-"""The reference's hot-path reduce and accumulate cases (test/python/tests/test_reduce.py and
-test_accumulate.py: primitives per type, reductions of views along every axis, cumsum/cumprod)
+"""The reference's hot-path reduce and accumulate cases (test/python/tests/test_reduce.py,
+test_accumulate.py and test_summations.py: primitives per type, reductions of views along every
+axis, cumsum/cumprod, sum/prod/all/any/mean)
 run on the oracle, with NumPy as the witness as in the reference's harness
 (test/python/run.py:42-59). CPU only. Integer, bitwise and boolean results must be exact;
 float sums and products are held to 1e-5 (float32) and 1e-12 (float64) relative, since the oracle's
@@ -108,3 +109,22 @@ def test_accumulate_primitives(oracle_rt, op, dtype):
     host = random_of_dtype((10,), dtype)
     got = bh.accumulate(op + "_ACCUMULATE", bh.array(oracle_rt, host), 0).numpy()
     _check(got, NUMPY_UFUNC[op].accumulate(host, dtype=host.dtype), dtype)
+
+
+@pytest.mark.parametrize("op", ["sum", "prod", "all", "any", "mean"])
+def test_summations(oracle_rt, op):
+    """test_summations.py test_sums: sum, prod, all, any and mean of 3-D float32 arrays and views,
+    over the whole array and along every axis (prod of values near 1, so it stays finite)."""
+    host = (random_of_dtype((5, 4, 6), np.float32) * np.float32(0.2) + np.float32(0.9)).astype(np.float32)
+    if op in ("all", "any"):
+        host[1, 2, :] = 0
+    a = bh.array(oracle_rt, host)
+    views = [(a, host), (a[::-1, 1:, ::2], host[::-1, 1:, ::2]), (a.transpose((2, 0, 1)), host.transpose((2, 0, 1)))]
+    for view, ref in views:
+        for axis in [None, 0, 1, 2]:
+            got = getattr(view, op)(axis).numpy()
+            want = getattr(ref, op)(axis=axis)
+            if op in ("all", "any"):
+                assert np.array_equal(np.asarray(got).astype(bool), want), (op, axis)
+            else:
+                _check(got, want, np.float32)
