@@ -63,21 +63,28 @@ TRANSCENDENTAL = {"COS", "SIN", "TAN", "COSH", "SINH", "TANH", "ARCSIN", "ARCCOS
                   "ARCTANH", "EXP", "EXP2", "EXPM1", "LOG", "LOG2", "LOG10", "LOG1P", "ARCTAN2", "POWER"}
 
 
+def binary_inputs(name, dtype, n=1000, seed=0):
+    """The two operand arrays of binary_program (its constant operand is B[3])."""
+    dt = np.dtype(dtype)
+    lo = 0 if name in ("LEFT_SHIFT", "RIGHT_SHIFT", "POWER") or dt.kind == "u" else None
+    hi_b = 5 if name in ("LEFT_SHIFT", "RIGHT_SHIFT", "POWER") else None
+    nz = name in ("DIVIDE", "MOD", "REMAINDER")
+    if dt.kind == "f":
+        A = data(n, dt, seed, 0.05, 4.0)
+        B = data(n, dt, seed + 1, 0.05 if nz or name == "POWER" else -2.0, 3.0)
+    else:
+        # POWER stays inside the type's range: the reference converts pow()'s double result,
+        # which is undefined behaviour in C on overflow.
+        A = data(n, dt, seed, lo, 20 if name == "POWER" else (None if hi_b is None else 100))
+        B = data(n, dt, seed + 1, lo if lo is not None else None, hi_b, nonzero=nz)
+    return A, B
+
+
 def binary_program(name, dtype, n=1000, seed=0):
     dt = np.dtype(dtype)
 
     def prog(rt):
-        lo = 0 if name in ("LEFT_SHIFT", "RIGHT_SHIFT", "POWER") or dt.kind == "u" else None
-        hi_b = 5 if name in ("LEFT_SHIFT", "RIGHT_SHIFT", "POWER") else None
-        nz = name in ("DIVIDE", "MOD", "REMAINDER")
-        if dt.kind == "f":
-            A = data(n, dt, seed, 0.05, 4.0)
-            B = data(n, dt, seed + 1, 0.05 if nz or name == "POWER" else -2.0, 3.0)
-        else:
-            # POWER stays inside the type's range: the reference converts pow()'s double result,
-            # which is undefined behaviour in C on overflow.
-            A = data(n, dt, seed, lo, 20 if name == "POWER" else (None if hi_b is None else 100))
-            B = data(n, dt, seed + 1, lo if lo is not None else None, hi_b, nonzero=nz)
+        A, B = binary_inputs(name, dt, n, seed)
         a = bh.array(rt, A)
         b = bh.array(rt, B)
         out = bh.empty(rt, (n,), dt)
@@ -90,11 +97,17 @@ def binary_program(name, dtype, n=1000, seed=0):
     return prog
 
 
+def compare_inputs(dtype, n=1000, seed=0):
+    """The operands of compare_program: every third element equal."""
+    A = data(n, dtype, seed)
+    B = data(n, dtype, seed + 1)
+    B[::3] = A[::3]
+    return A, B
+
+
 def compare_program(name, dtype, n=1000, seed=0):
     def prog(rt):
-        A = data(n, dtype, seed)
-        B = data(n, dtype, seed + 1)
-        B[::3] = A[::3]
+        A, B = compare_inputs(dtype, n, seed)
         a, b = bh.array(rt, A), bh.array(rt, B)
         out = bh.empty(rt, (n,), np.bool_)
         rt.enqueue(ir.Instr(ir.OPCODES[name], [out.view(), a.view(), b.view()]))
@@ -111,22 +124,29 @@ def logical_program(name, n=1000, seed=0):
     return prog
 
 
+def unary_inputs(name, dtype, n=1000, seed=0):
+    """The operand of unary_program: inside each function's domain, with NaNs and infinities for
+    the predicates."""
+    dt = np.dtype(dtype)
+    if dt.kind == "f":
+        lo, hi = {"ARCCOSH": (1.0, 5.0), "ARCTANH": (-0.9, 0.9), "ARCSIN": (-1, 1), "ARCCOS": (-1, 1),
+                  "LOG": (0.01, 9), "LOG2": (0.01, 9), "LOG10": (0.01, 9), "SQRT": (0, 9),
+                  "LOG1P": (-0.5, 9)}.get(name, (-3.0, 3.0))
+        A = data(n, dt, seed, lo, hi)
+        if name in ("ISNAN", "ISINF", "ISFINITE"):
+            A[::7] = np.nan
+            A[1::11] = np.inf
+    else:
+        A = data(n, dt, seed)
+    return A
+
+
 def unary_program(name, dtype, n=1000, seed=0):
     dt = np.dtype(dtype)
     out_dt = np.bool_ if name in ("ISNAN", "ISINF", "ISFINITE") else dt
 
     def prog(rt):
-        if dt.kind == "f":
-            lo, hi = {"ARCCOSH": (1.0, 5.0), "ARCTANH": (-0.9, 0.9), "ARCSIN": (-1, 1), "ARCCOS": (-1, 1),
-                      "LOG": (0.01, 9), "LOG2": (0.01, 9), "LOG10": (0.01, 9), "SQRT": (0, 9),
-                      "LOG1P": (-0.5, 9)}.get(name, (-3.0, 3.0))
-            A = data(n, dt, seed, lo, hi)
-            if name in ("ISNAN", "ISINF", "ISFINITE"):
-                A[::7] = np.nan
-                A[1::11] = np.inf
-        else:
-            A = data(n, dt, seed)
-        a = bh.array(rt, A)
+        a = bh.array(rt, unary_inputs(name, dt, n, seed))
         out = bh.empty(rt, (n,), out_dt)
         rt.enqueue(ir.Instr(ir.OPCODES[name], [out.view(), a.view()]))
         return [out]
