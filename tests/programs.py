@@ -153,14 +153,18 @@ def unary_program(name, dtype, n=1000, seed=0):
     return prog
 
 
+def identity_inputs(src_dt, dst_dt, n=500, seed=0):
+    """The source array of identity_program: values every destination type holds (no negative
+    values for unsigned destinations, floats within +-100)."""
+    s = np.dtype(src_dt)
+    if s.kind == "f":
+        return data(n, s, seed, -100.0 if np.dtype(dst_dt).kind in "if" else 0.0, 100.0)
+    return data(n, s, seed, 0 if np.dtype(dst_dt).kind == "u" else None)
+
+
 def identity_program(src_dt, dst_dt, n=500, seed=0):
     def prog(rt):
-        s = np.dtype(src_dt)
-        if s.kind == "f":
-            A = data(n, s, seed, -100.0 if np.dtype(dst_dt).kind in "if" else 0.0, 100.0)
-        else:
-            A = data(n, s, seed, 0 if np.dtype(dst_dt).kind == "u" else None)
-        a = bh.array(rt, A)
+        a = bh.array(rt, identity_inputs(src_dt, dst_dt, n, seed))
         return [a.astype(dst_dt)]
     return prog
 

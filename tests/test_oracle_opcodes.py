@@ -89,3 +89,16 @@ def test_unary_any_vs_numpy(oracle_rt, name):
         with np.errstate(all="ignore"):
             want = UNARY_NUMPY[name](A)
         assert_close(got, want.astype(got.dtype), 0, 0, f"{name} {np.dtype(dt)}")
+
+
+def test_type_conversions_vs_numpy(oracle_rt):
+    """BH_IDENTITY between every pair of the GPU suite's types (test_typecast.py of the
+    reference), against NumPy's astype on values every destination type holds."""
+    types = [np.bool_, np.int8, np.int32, np.int64, np.uint8, np.uint64, np.float32, np.float64]
+    for s in types:
+        for d in types:
+            if s == d:
+                continue
+            A = P.identity_inputs(s, d)
+            (got,) = run(oracle_rt, P.identity_program(s, d))
+            assert_close(got, A.astype(d), 0, 0, f"{np.dtype(s)}->{np.dtype(d)}")
