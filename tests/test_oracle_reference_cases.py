@@ -1,6 +1,7 @@
-"""The reference's hot-path reduce and accumulate cases (test/python/tests/test_reduce.py,
-test_accumulate.py and test_summations.py: primitives per type, reductions of views along every
-axis, cumsum/cumprod, sum/prod/all/any/mean)
+"""The reference's hot-path test cases (test/python/tests/test_reduce.py, test_accumulate.py,
+test_summations.py, test_negatives.py and test_emptiness.py: reduce primitives per type,
+reductions of views along every axis, cumsum/cumprod, sum/prod/all/any/mean, division and
+remainders of negative integers, empty arrays)
 run on the oracle, with NumPy as the witness as in the reference's harness
 (test/python/run.py:42-59). CPU only. Integer, bitwise and boolean results must be exact;
 float sums and products are held to 1e-5 (float32) and 1e-12 (float64) relative, since the oracle's
@@ -128,3 +129,24 @@ def test_summations(oracle_rt, op):
                 assert np.array_equal(np.asarray(got).astype(bool), want), (op, axis)
             else:
                 _check(got, want, np.float32)
+
+
+@pytest.mark.parametrize("dtype", [np.int8, np.int16, np.int32, np.int64])
+@pytest.mark.parametrize("swap", [False, True])
+def test_negative_operands(oracle_rt, dtype, swap):
+    """test_negatives.py: a = arange(-11, -1), b = arange(1, 11) and the other way round, through
+    true division, floor division, % / remainder (the divisor's sign) and fmod (the dividend's)."""
+    x, y = np.arange(-11, -1, dtype=dtype), np.arange(1, 11, dtype=dtype)
+    A, B = (y, x) if swap else (x, y)
+    a, b = bh.array(oracle_rt, A), bh.array(oracle_rt, B)
+    np.testing.assert_array_equal((a / b).numpy(), A / B)
+    np.testing.assert_array_equal((a // b).numpy(), A // B)
+    np.testing.assert_array_equal((a % b).numpy(), np.remainder(A, B))
+    np.testing.assert_array_equal(bh.binary("MOD", a, b).numpy(), np.fmod(A, B))
+
+
+def test_empty_arrays(oracle_rt):
+    """test_emptiness.py: a + a of empty arrays is an empty array."""
+    a = bh.array(oracle_rt, np.array([], dtype=np.float64))
+    res = (a + a).numpy()
+    assert res.shape == (0,) and res.dtype == np.float64
