@@ -1,7 +1,7 @@
 """The reference's hot-path test cases (test/python/tests/test_reduce.py, test_accumulate.py,
-test_summations.py, test_negatives.py and test_emptiness.py: reduce primitives per type,
-reductions of views along every axis, cumsum/cumprod, sum/prod/all/any/mean, division and
-remainders of negative integers, empty arrays)
+test_summations.py, test_negatives.py, test_emptiness.py and test_loop.py: reduce primitives per
+type, reductions of views along every axis, cumsum/cumprod, sum/prod/all/any/mean, division and
+remainders of negative integers, empty arrays, flush-and-repeat with sliding views)
 run on the oracle, with NumPy as the witness as in the reference's harness
 (test/python/run.py:42-59). CPU only. Integer, bitwise and boolean results must be exact;
 float sums and products are held to 1e-5 (float32) and 1e-12 (float64) relative, since the oracle's
@@ -150,3 +150,51 @@ def test_empty_arrays(oracle_rt):
     a = bh.array(oracle_rt, np.array([], dtype=np.float64))
     res = (a + a).numpy()
     assert res.shape == (0,) and res.dtype == np.float64
+
+
+def test_loop_sliding_views_triangular_numbers():
+    """test_loop.py test_loop_faculty_function_using_sliding_views: a[i+1] += a[i] for 10
+    iterations of one flush, both views sliding by one element per iteration."""
+    from bohrium_b200 import ir
+    from oracle.ve_openmp import OracleExecutor
+    rt = bh.Runtime(OracleExecutor(threads=2))
+    niter = 10
+    host = np.arange(1, niter + 2, dtype=np.int64)
+    a = bh.array(rt, host)
+    rt.flush()
+    nxt = ir.View(a.base, 1, (1,), (1,))
+    cur = ir.View(a.base, 0, (1,), (1,))
+    ins = ir.Instr(ir.OPCODES["ADD"], [nxt, ir.View(a.base, 1, (1,), (1,)), cur])
+    for k in range(3):
+        ins.slides[k] = ([ir.Slide(0, 1, 0, 1, niter + 1)], {})
+    rt.ex.execute(ir.Flush([ins], nrepeats=niter))
+    want = host.copy()
+    for i in range(niter):
+        want[i + 1] += want[i]
+    np.testing.assert_array_equal(a.numpy(), want)
+
+
+def test_loop_one_and_two_dimensional_sliding_views():
+    """test_loop.py test_loop_one_and_two_dimensional_sliding_views: res[i] += b[i, i], the
+    element of b sliding along both axes at once."""
+    from bohrium_b200 import ir
+    from oracle.ve_openmp import OracleExecutor
+    rt = bh.Runtime(OracleExecutor(threads=2))
+    niter = 5
+    B = np.ones((20, niter))
+    B[::2, ::2] += 1
+    B[1::2, 1::2] += 1
+    b = bh.array(rt, B)
+    res = bh.zeros(rt, (niter, 1), np.float64)
+    rt.flush()
+    r = ir.View(res.base, 0, (1, 1), (1, 1))
+    e = ir.View(b.base, 0, (1, 1), (niter, 1))
+    ins = ir.Instr(ir.OPCODES["ADD"], [r, ir.View(res.base, 0, (1, 1), (1, 1)), e])
+    for k in range(2):
+        ins.slides[k] = ([ir.Slide(0, 1, 0, 1, niter)], {})
+    ins.slides[2] = ([ir.Slide(0, 1, 0, niter, 20), ir.Slide(1, 1, 0, 1, niter)], {})
+    rt.ex.execute(ir.Flush([ins], nrepeats=niter))
+    want = np.zeros((niter, 1))
+    for i in range(niter):
+        want[i] += B[i, i]
+    np.testing.assert_array_equal(res.numpy(), want)
