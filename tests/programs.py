@@ -398,3 +398,43 @@ def complex_chain_program(n, dtype=np.complex128, seed=0):
         p = bh.real(z) * bh.real(z) + bh.imag(z) * bh.imag(z)
         return [z, z.sum(), p, p.sum(), bh.absolute(z)]
     return prog
+
+
+def loop_triangular_numbers(rt, niter=10):
+    """a[i+1] += a[i] for niter iterations of one flush-and-repeat, the three views sliding by one
+    element per iteration (the reference's test_loop_faculty_function_using_sliding_views).
+    Returns the result and NumPy's loop."""
+    host = np.arange(1, niter + 2, dtype=np.int64)
+    a = bh.array(rt, host)
+    rt.flush()
+    ins = ir.Instr(ir.OPCODES["ADD"], [ir.View(a.base, 1, (1,), (1,)), ir.View(a.base, 1, (1,), (1,)),
+                                       ir.View(a.base, 0, (1,), (1,))])
+    for k in range(3):
+        ins.slides[k] = ([ir.Slide(0, 1, 0, 1, niter + 1)], {})
+    rt.ex.execute(ir.Flush([ins], nrepeats=niter))
+    want = host.copy()
+    for i in range(niter):
+        want[i + 1] += want[i]
+    return a.numpy(), want
+
+
+def loop_diagonal(rt, niter=5):
+    """res[i] += b[i, i] for niter iterations, the (1, 1) view of b sliding along both axes (the
+    reference's test_loop_one_and_two_dimensional_sliding_views). Returns the result and NumPy's
+    loop."""
+    B = np.ones((20, niter))
+    B[::2, ::2] += 1
+    B[1::2, 1::2] += 1
+    b = bh.array(rt, B)
+    res = bh.zeros(rt, (niter, 1), np.float64)
+    rt.flush()
+    ins = ir.Instr(ir.OPCODES["ADD"], [ir.View(res.base, 0, (1, 1), (1, 1)), ir.View(res.base, 0, (1, 1), (1, 1)),
+                                       ir.View(b.base, 0, (1, 1), (niter, 1))])
+    for k in range(2):
+        ins.slides[k] = ([ir.Slide(0, 1, 0, 1, niter)], {})
+    ins.slides[2] = ([ir.Slide(0, 1, 0, niter, 20), ir.Slide(1, 1, 0, 1, niter)], {})
+    rt.ex.execute(ir.Flush([ins], nrepeats=niter))
+    want = np.zeros((niter, 1))
+    for i in range(niter):
+        want[i] += B[i, i]
+    return res.numpy(), want

@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import bohrium_b200 as bh
+from tests import programs as P
 
 NORMAL = [np.int32, np.int64, np.uint32, np.uint64, np.float32, np.float64]
 
@@ -152,49 +153,15 @@ def test_empty_arrays(oracle_rt):
     assert res.shape == (0,) and res.dtype == np.float64
 
 
-def test_loop_sliding_views_triangular_numbers():
+def test_loop_sliding_views_triangular_numbers(oracle_rt):
     """test_loop.py test_loop_faculty_function_using_sliding_views: a[i+1] += a[i] for 10
     iterations of one flush, both views sliding by one element per iteration."""
-    from bohrium_b200 import ir
-    from oracle.ve_openmp import OracleExecutor
-    rt = bh.Runtime(OracleExecutor(threads=2))
-    niter = 10
-    host = np.arange(1, niter + 2, dtype=np.int64)
-    a = bh.array(rt, host)
-    rt.flush()
-    nxt = ir.View(a.base, 1, (1,), (1,))
-    cur = ir.View(a.base, 0, (1,), (1,))
-    ins = ir.Instr(ir.OPCODES["ADD"], [nxt, ir.View(a.base, 1, (1,), (1,)), cur])
-    for k in range(3):
-        ins.slides[k] = ([ir.Slide(0, 1, 0, 1, niter + 1)], {})
-    rt.ex.execute(ir.Flush([ins], nrepeats=niter))
-    want = host.copy()
-    for i in range(niter):
-        want[i + 1] += want[i]
-    np.testing.assert_array_equal(a.numpy(), want)
+    got, want = P.loop_triangular_numbers(oracle_rt)
+    np.testing.assert_array_equal(got, want)
 
 
-def test_loop_one_and_two_dimensional_sliding_views():
+def test_loop_one_and_two_dimensional_sliding_views(oracle_rt):
     """test_loop.py test_loop_one_and_two_dimensional_sliding_views: res[i] += b[i, i], the
     element of b sliding along both axes at once."""
-    from bohrium_b200 import ir
-    from oracle.ve_openmp import OracleExecutor
-    rt = bh.Runtime(OracleExecutor(threads=2))
-    niter = 5
-    B = np.ones((20, niter))
-    B[::2, ::2] += 1
-    B[1::2, 1::2] += 1
-    b = bh.array(rt, B)
-    res = bh.zeros(rt, (niter, 1), np.float64)
-    rt.flush()
-    r = ir.View(res.base, 0, (1, 1), (1, 1))
-    e = ir.View(b.base, 0, (1, 1), (niter, 1))
-    ins = ir.Instr(ir.OPCODES["ADD"], [r, ir.View(res.base, 0, (1, 1), (1, 1)), e])
-    for k in range(2):
-        ins.slides[k] = ([ir.Slide(0, 1, 0, 1, niter)], {})
-    ins.slides[2] = ([ir.Slide(0, 1, 0, niter, 20), ir.Slide(1, 1, 0, 1, niter)], {})
-    rt.ex.execute(ir.Flush([ins], nrepeats=niter))
-    want = np.zeros((niter, 1))
-    for i in range(niter):
-        want[i] += B[i, i]
-    np.testing.assert_array_equal(res.numpy(), want)
+    got, want = P.loop_diagonal(oracle_rt)
+    np.testing.assert_array_equal(got, want)
