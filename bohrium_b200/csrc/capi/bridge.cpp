@@ -1,4 +1,5 @@
 // The flat C bridge declared in include/bh_b200.h.
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -40,12 +41,54 @@ struct bhb_runtime {
 };
 
 struct bhb_ir {
+    ~bhb_ir() {
+        if (ir) bh_ir_hints_clear(ir.get());
+    }
     unique_ptr<BhIR> ir;
     bohrium::filter::BaseStore created;  // temporaries made by bhb_ir_filter
     string text;                          // last bhb_ir_text result
 };
 
 namespace {
+// Content fingerprint of a decoded list without sliding views: every instruction's opcode,
+// constant and operand views, with each base's address, element type and size (an address can be
+// reused for another base), plus the syncs and repeat settings. Never 0.
+uint64_t fingerprint(const BhIR &ir) {
+    uint64_t h = 0xcbf29ce484222325ULL ^ static_cast<uint64_t>(ir.instr_list.size());
+    auto mix = [&h](uint64_t v) {
+        v *= 0x9E3779B97F4A7C15ULL;
+        h = (h ^ (v ^ (v >> 29))) * 0x100000001B3ULL;
+    };
+    for (const bh_instruction &instr : ir.instr_list) {
+        mix(static_cast<uint64_t>(instr.opcode));
+        mix(static_cast<uint64_t>(instr.constant.type));
+        uint64_t cw[2] = {0, 0};
+        memcpy(cw, &instr.constant.value, min(sizeof(cw), sizeof(instr.constant.value)));
+        mix(cw[0]);
+        mix(cw[1]);
+        mix(instr.operand.size());
+        for (const bh_view &v : instr.operand) {
+            if (v.isConstant()) {
+                mix(~0ULL);
+                continue;
+            }
+            mix(reinterpret_cast<uint64_t>(v.base));
+            mix(static_cast<uint64_t>(v.base->dtype()));
+            mix(static_cast<uint64_t>(v.base->nelem()));
+            mix(static_cast<uint64_t>(v.start));
+            mix(static_cast<uint64_t>(v.ndim));
+            for (int64_t d = 0; d < v.ndim; ++d) {
+                mix(static_cast<uint64_t>(v.shape[d]));
+                mix(static_cast<uint64_t>(v.stride[d]));
+            }
+        }
+    }
+    for (const bh_base *b : ir._syncs) mix(reinterpret_cast<uint64_t>(b));
+    mix(ir._nrepeats);
+    mix(reinterpret_cast<uint64_t>(ir._repeat_condition));
+    return h | 1ULL;
+}
+
 BhIR *decode(const int64_t *w, int64_t n, bh_base *const *syncs, int64_t nsyncs, uint64_t nrepeats, bh_base *cond,
              const int64_t *slides, int64_t nslide) {
     vector<bh_instruction> list;
@@ -121,28 +164,11 @@ BhIR *decode(const int64_t *w, int64_t n, bh_base *const *syncs, int64_t nsyncs,
     for (const bh_instruction &instr : list) builtin = builtin && instr.opcode <= BH_MAX_OPCODE_ID;
     set<bh_base *> s(syncs, syncs + nsyncs);
     BhIR *ir = new BhIR(std::move(list), std::move(s), nrepeats, cond);
-    ir->_plain = nslide == 0 && builtin;
-    if (nslide == 0) {
-        // The handle is immutable: fingerprint its encoding once so that an engine can recognise
-        // the repeated flush (sliding views change between executions, so they get none).
-        uint64_t h = 0xcbf29ce484222325ULL ^ static_cast<uint64_t>(n);
-        auto mix = [&h](uint64_t v) {
-            v *= 0x9E3779B97F4A7C15ULL;
-            h = (h ^ (v ^ (v >> 29))) * 0x100000001B3ULL;
-        };
-        for (int64_t k = 0; k < n; ++k) mix(static_cast<uint64_t>(w[k]));
-        // Base identity includes element type and size (a base address can be reused).
-        for (const bh_instruction &instr : ir->instr_list)
-            for (const bh_view &v : instr.operand)
-                if (!v.isConstant()) {
-                    mix(static_cast<uint64_t>(v.base->dtype()));
-                    mix(static_cast<uint64_t>(v.base->nelem()));
-                }
-        for (int64_t k = 0; k < nsyncs; ++k) mix(reinterpret_cast<uint64_t>(syncs[k]));
-        mix(nrepeats);
-        mix(reinterpret_cast<uint64_t>(cond));
-        ir->_fingerprint = h | 1ULL;
-    }
+    BhIRHints hints;
+    hints.plain = nslide == 0 && builtin;
+    // Sliding views change between executions, so such a list gets no fingerprint.
+    if (nslide == 0) hints.fingerprint = fingerprint(*ir);
+    bh_ir_hints_set(ir, hints);
     return ir;
 }
 } // namespace
@@ -235,6 +261,10 @@ int bhb_execute(bhb_runtime *rt, const int64_t *words, int64_t nwords, bh_base *
                 uint64_t nrepeats, bh_base *repeat_condition, const int64_t *slides, int64_t nslide_words) {
     return guarded([&] {
         unique_ptr<BhIR> ir(decode(words, nwords, syncs, nsyncs, nrepeats, repeat_condition, slides, nslide_words));
+        struct Clear {
+            const BhIR *p;
+            ~Clear() { bh_ir_hints_clear(p); }
+        } clear{ir.get()};
         rt->child.execute(ir.get());
     });
 }
@@ -323,6 +353,10 @@ extern "C" int bhb_ir_filter(bhb_ir *ir, const char *name) {
         } else {
             throw runtime_error("bhb_ir_filter: unknown filter " + f);
         }
+        // The list changed: a fingerprint must describe the filtered list.
+        BhIRHints hints = bh_ir_hints_get(ir->ir.get());
+        if (hints.fingerprint != 0) hints.fingerprint = fingerprint(*ir->ir);
+        bh_ir_hints_set(ir->ir.get(), hints);
     });
     return n;
 }

@@ -58,6 +58,7 @@ struct Hasher {
 // (the machine that builds it has no GPU driver).
 struct DeviceApi {
     CUresult (*cuModuleLoadData)(CUmodule *, const void *) = nullptr;
+    CUresult (*cuModuleUnload)(CUmodule) = nullptr;
     CUresult (*cuModuleGetFunction)(CUfunction *, CUmodule, const char *) = nullptr;
     CUresult (*cuLaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
                                CUstream, void **, void **) = nullptr;
@@ -76,6 +77,7 @@ struct DeviceApi {
     }
     DeviceApi() {
         get("cuModuleLoadData", cuModuleLoadData);
+        get("cuModuleUnload", cuModuleUnload);
         get("cuModuleGetFunction", cuModuleGetFunction);
         get("cuLaunchKernel", cuLaunchKernel);
         get("cuOccupancyMaxActiveBlocksPerMultiprocessor", cuOccupancyMaxActiveBlocksPerMultiprocessor);
@@ -175,7 +177,8 @@ void EngineCUDA::copyToDevice(bh_base *base) {
     DevBuf b;
     b.nbytes = base->nbytes();
     if (b.nbytes > 0) {
-        check(cudaMallocAsync(&b.ptr, static_cast<size_t>(b.nbytes), static_cast<cudaStream_t>(_stream)),
+        check(inject_alloc_failures > 0 ? (--inject_alloc_failures, cudaErrorMemoryAllocation)
+                                        : cudaMallocAsync(&b.ptr, static_cast<size_t>(b.nbytes), static_cast<cudaStream_t>(_stream)),
               "cudaMallocAsync");
         if (base->getDataPtr() != nullptr) {
             check(cudaMemcpyAsync(b.ptr, base->getDataPtr(), static_cast<size_t>(b.nbytes), cudaMemcpyHostToDevice,
@@ -434,10 +437,10 @@ void EngineCUDA::precompile(const vector<const LaunchUnit *> &units) {
         const uint64_t h = fnv1a(u->source.data(), u->source.size());
         if (functions.count(h) || ahead.count(h) || !seen.insert(h).second) continue;
         const string path = disk_cache_path(u->source);
-        if (!path.empty() && access(path.c_str(), R_OK) == 0) continue;
+        if (!path.empty() && access(path.c_str(), R_OK) == 0) continue;  // checked when it is loaded
         todo.push_back(u);
     }
-    if (todo.size() < 2) return;
+    if (todo.size() < 2 || inject_nvrtc_failures > 0) return;  // an injected failure hits the serial path
     const auto t0 = chrono::steady_clock::now();
     const vector<string> opts = nvrtc_options(fmad);
     vector<vector<char>> cubins(todo.size());
@@ -460,26 +463,73 @@ void EngineCUDA::precompile(const vector<const LaunchUnit *> &units) {
     _stats.parallel_compiles += todo.size();
 }
 
+// Kernel cache files: an 8-byte tag, the cubin's size and its FNV-1a hash, then the cubin. A file
+// that is short, has another tag or fails the hash (a truncated write, a stale format, a damaged
+// disk) is deleted and the kernel recompiled: its bytes never reach the driver.
+namespace {
+const char kCacheTag[8] = {'B', 'H', 'C', 'U', 'B', 'I', 'N', '1'};
+}
+
+bool EngineCUDA::read_cache_file(const string &path, vector<char> &cubin) {
+    ifstream in(path, ios::binary);
+    if (!in) return false;
+    vector<char> all((istreambuf_iterator<char>(in)), istreambuf_iterator<char>());
+    cubin.clear();
+    uint64_t n = 0, h = 0;
+    bool ok = all.size() >= 24 && memcmp(all.data(), kCacheTag, 8) == 0;
+    if (ok) {
+        memcpy(&n, all.data() + 8, 8);
+        memcpy(&h, all.data() + 16, 8);
+        ok = n > 0 && all.size() == 24 + n && fnv1a(all.data() + 24, n) == h;
+    }
+    if (!ok) {
+        ++_stats.disk_cache_rejected;
+        unlink(path.c_str());
+        return false;
+    }
+    cubin.assign(all.begin() + 24, all.end());
+    return true;
+}
+
+void EngineCUDA::write_cache_file(const string &path, const vector<char> &cubin) {
+    if (path.empty()) return;
+    const string tmp = path + ".tmp" + to_string(getpid());
+    {
+        ofstream out(tmp, ios::binary);
+        const uint64_t n = cubin.size(), h = fnv1a(cubin.data(), cubin.size());
+        out.write(kCacheTag, 8);
+        out.write(reinterpret_cast<const char *>(&n), 8);
+        out.write(reinterpret_cast<const char *>(&h), 8);
+        out.write(cubin.data(), static_cast<streamsize>(cubin.size()));
+        if (!out) {
+            out.close();
+            unlink(tmp.c_str());
+            return;
+        }
+    }
+    rename(tmp.c_str(), path.c_str());
+}
+
+bool EngineCUDA::compile_cubin(const string &name, const string &source, const vector<string> &opts,
+                               vector<char> &cubin, string &error) {
+    if (inject_nvrtc_failures > 0) {
+        --inject_nvrtc_failures;
+        error = "NVRTC compilation of " + name + " failed: injected failure";
+        return false;
+    }
+    return nvrtc_cubin(name, source, opts, cubin, error);
+}
+
 vector<char> EngineCUDA::cubin_for(const string &name, const string &source, int maxrreg) {
     vector<char> cubin;
     const string path = disk_cache_path(source, maxrreg);
-    if (!path.empty()) {
-        ifstream in(path, ios::binary);
-        if (in) cubin.assign(istreambuf_iterator<char>(in), istreambuf_iterator<char>());
-        if (!cubin.empty()) {
-            ++_stats.disk_cache_hits;
-            return cubin;
-        }
+    if (!path.empty() && read_cache_file(path, cubin)) {
+        ++_stats.disk_cache_hits;
+        return cubin;
     }
     string error;
-    if (!nvrtc_cubin(name, source, nvrtc_options(fmad, maxrreg), cubin, error)) throw runtime_error(error);
-    if (!path.empty()) {
-        const string tmp = path + ".tmp" + to_string(getpid());
-        ofstream out(tmp, ios::binary);
-        out.write(cubin.data(), static_cast<streamsize>(cubin.size()));
-        out.close();
-        rename(tmp.c_str(), path.c_str());
-    }
+    if (!compile_cubin(name, source, nvrtc_options(fmad, maxrreg), cubin, error)) throw runtime_error(error);
+    write_cache_file(path, cubin);
     return cubin;
 }
 
@@ -535,14 +585,7 @@ EngineCUDA::Compiled *EngineCUDA::compiled_for(const LaunchUnit &u) {
     if (pre != ahead.end()) {
         cubin = std::move(pre->second);
         ahead.erase(pre);
-        const string path = disk_cache_path(u.source);
-        if (!path.empty()) {
-            const string tmp = path + ".tmp" + to_string(getpid());
-            ofstream out(tmp, ios::binary);
-            out.write(cubin.data(), static_cast<streamsize>(cubin.size()));
-            out.close();
-            rename(tmp.c_str(), path.c_str());
-        }
+        write_cache_file(disk_cache_path(u.source), cubin);
     } else {
         cubin = cubin_for(u.name, u.source, 0);
     }
@@ -1166,8 +1209,9 @@ void EngineCUDA::run_plan(const FlushPlan &plan, const vector<bh_base *> &bases,
 void EngineCUDA::handleExecution(BhIR *bhir) {
     const auto t0 = chrono::steady_clock::now();
     // A repeated, unmodified BhIR replays its plan without scanning the instruction list.
-    if (bhir->_fingerprint != 0) {
-        auto rit = replays.find(bhir->_fingerprint);
+    const uint64_t fingerprint = bhir == cur_ir ? cur_hints.fingerprint : 0;
+    if (fingerprint != 0) {
+        auto rit = replays.find(fingerprint);
         // A graph replay whose arrays and host copies are untouched since its last launch needs
         // no checks at all.
         const bool graph_mode = batch_mode == "graph" && !prof && !record;
@@ -1211,7 +1255,7 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
     vector<bh_base *> base_ids;
     bool sliding = false;
     Replay replay;
-    const uint64_t key = prepare(bhir->instr_list, instr_list, base_ids, sliding, bhir->_fingerprint ? &replay : nullptr);
+    const uint64_t key = prepare(bhir->instr_list, instr_list, base_ids, sliding, fingerprint ? &replay : nullptr);
     const auto t1 = chrono::steady_clock::now();
     _stats.time_prepare += chrono::duration<double>(t1 - t0).count();
     if (staging_used > 0 && staging_event) {
@@ -1240,7 +1284,7 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
             if (!sliding) plans[key] = std::move(plan);
         }
     }
-    if (bhir->_fingerprint != 0 && !sliding) {
+    if (fingerprint != 0 && !sliding) {
         auto pit = plans.find(key);
         if (pit != plans.end()) {
             replay.plan = &pit->second;
@@ -1248,7 +1292,7 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
             replay.instr_copy.reserve(instr_list.size());
             for (const bh_instruction *i : instr_list) replay.instr_copy.push_back(*i);
             for (bh_instruction &i : replay.instr_copy) replay.instrs.push_back(&i);
-            replays[bhir->_fingerprint] = std::move(replay);
+            replays[fingerprint] = std::move(replay);
         }
     }
     const auto t2 = chrono::steady_clock::now();
@@ -1261,7 +1305,7 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
 void EngineCUDA::handleExtmethod(BhIR *bhir) {
     // Only a list that contains extension methods needs splitting (and copying).
     bool any = false;
-    if (!bhir->_plain && (!comp.extmethods.empty() || !comp.child_extmethods.empty())) {
+    if (!(bhir == cur_ir && cur_hints.plain) && (!comp.extmethods.empty() || !comp.child_extmethods.empty())) {
         for (const bh_instruction &instr : bhir->instr_list) {
             if (comp.extmethods.count(instr.opcode) || comp.child_extmethods.count(instr.opcode)) {
                 any = true;
@@ -1270,7 +1314,9 @@ void EngineCUDA::handleExtmethod(BhIR *bhir) {
         }
     }
     if (!any) return;
-    bhir->_fingerprint = 0; // the list is rewritten below
+    // The list is rewritten below: its registered fingerprint no longer describes it.
+    if (bhir == cur_ir) cur_hints.fingerprint = 0;
+    bh_ir_hints_clear(bhir);
     vector<bh_instruction> instr_list;
     for (bh_instruction &instr : bhir->instr_list) {
         auto ext = comp.extmethods.find(instr.opcode);
@@ -1417,8 +1463,10 @@ string EngineCUDA::userKernel(const string &kernel, vector<bh_view> &operands, c
         CUmodule mod;
         CUfunction f;
         if (api->cuModuleLoadData(&mod, cubin.data()) != CUDA_SUCCESS) return "[CUDA] userKernel: cuModuleLoadData failed";
-        if (api->cuModuleGetFunction(&f, mod, "execute") != CUDA_SUCCESS)
+        if (api->cuModuleGetFunction(&f, mod, "execute") != CUDA_SUCCESS) {
+            api->cuModuleUnload(mod);
             return "[CUDA] userKernel: the source defines no extern \"C\" __global__ function named execute";
+        }
         fn = reinterpret_cast<void *>(f);
         user_functions[h] = fn;
         _stats.time_compile += seconds_since(t0);
@@ -1448,6 +1496,8 @@ string EngineCUDA::userKernel(const string &kernel, vector<bh_view> &operands, c
 
 void EngineCUDA::execute(BhIR *bhir) {
     ++_stats.flushes;
+    cur_ir = bhir;
+    cur_hints = bh_ir_hints_get(bhir);
     bh_base *cond = bhir->getRepeatCondition();
     for (uint64_t i = 0; i < bhir->getNRepeats(); ++i) {
         handleExtmethod(bhir);
@@ -1456,7 +1506,7 @@ void EngineCUDA::execute(BhIR *bhir) {
             copyToHost({cond}, false);
             if (cond->getDataPtr() != nullptr && !static_cast<bool *>(cond->getDataPtr())[0]) break;
         }
-        if (!bhir->_plain) slide_views(bhir);  // a plain list has no sliding views
+        if (!cur_hints.plain) slide_views(bhir);  // a plain list has no sliding views
     }
 }
 
@@ -1484,6 +1534,7 @@ string EngineCUDA::statistics() const {
        << "\nserial_units: " << _stats.serial_units << "\nfuse_cache_hits: " << _stats.fuse_cache_hits
        << "\nfuse_cache_misses: " << _stats.fuse_cache_misses << "\nkernel_cache_hits: " << _stats.kernel_cache_hits
        << "\nkernel_cache_misses: " << _stats.kernel_cache_misses << "\ndisk_cache_hits: " << _stats.disk_cache_hits
+       << "\ndisk_cache_rejected: " << _stats.disk_cache_rejected
        << "\nbytes_h2d: " << _stats.bytes_h2d << "\nbytes_d2h: " << _stats.bytes_d2h
        << "\ntime_fusion: " << _stats.time_fusion << "\ntime_codegen: " << _stats.time_codegen
        << "\ntime_compile: " << _stats.time_compile << "\nparallel_compiles: " << _stats.parallel_compiles

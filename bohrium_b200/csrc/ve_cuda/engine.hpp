@@ -45,7 +45,7 @@ struct Stats {
     uint64_t flushes = 0, kernels = 0, launches = 0, grouped_launches = 0, graph_replays = 0;
     uint64_t fuse_cache_hits = 0, fuse_cache_misses = 0;
     uint64_t plan_cache_hits = 0, plan_cache_misses = 0, replays = 0;
-    uint64_t kernel_cache_hits = 0, kernel_cache_misses = 0, disk_cache_hits = 0;
+    uint64_t kernel_cache_hits = 0, kernel_cache_misses = 0, disk_cache_hits = 0, disk_cache_rejected = 0;
     uint64_t bytes_h2d = 0, bytes_d2h = 0;
     uint64_t serial_units = 0;
     // learned fusion: structures tried with both plans, kept learned / kept greedy, learned plan
@@ -66,6 +66,12 @@ public:
     ~EngineCUDA();
 
     void execute(BhIR *bhir);                  // the repeat loop of one flush
+    const BhIR *cur_ir = nullptr;              // the BhIR execute() runs and its registered hints
+    BhIRHints cur_hints;
+    // Host-side fault injection for tests ("CUDA: inject nvrtc N" / "CUDA: inject alloc N"): the
+    // next N kernel compilations fail as NVRTC failures, the next N array allocations as
+    // cudaErrorMemoryAllocation, without calling NVRTC or the allocator.
+    int inject_nvrtc_failures = 0, inject_alloc_failures = 0;
     void handleExecution(BhIR *bhir);          // one pass over the instruction list
     void handleExtmethod(BhIR *bhir);          // split around extension methods
     // ComponentImpl::userKernel with tag "cuda": compile `kernel` with NVRTC, run its
@@ -187,6 +193,10 @@ private:
     unsigned shared_bytes_of(void *fn) const;
     static int dynamic_shared_bytes(const std::string &source);
     std::vector<char> cubin_for(const std::string &name, const std::string &source, int maxrreg);
+    bool read_cache_file(const std::string &path, std::vector<char> &cubin); // false (and deleted) unless intact
+    void write_cache_file(const std::string &path, const std::vector<char> &cubin);
+    bool compile_cubin(const std::string &name, const std::string &source, const std::vector<std::string> &opts,
+                       std::vector<char> &cubin, std::string &error);
     // Autotuning of plain launches (tune.cpp)
     bool tune_launch(Compiled &c, const LaunchUnit &u, int64_t work, void **args);
     bool tune_batch_launch(Compiled &c, int64_t total, void **args);
@@ -243,7 +253,7 @@ private:
         std::string signature() const; // kernel names by level (plans with equal signatures match)
     };
     std::unordered_map<uint64_t, FlushPlan> plans;
-    // Replay of a fingerprinted BhIR (BhIR::_fingerprint): the plan, the bases in flush order,
+    // Replay of a fingerprinted BhIR (BhIRHints::fingerprint): the plan, the bases in flush order,
     // the bases freed without being computed, and the bases whose constructor flag the plan
     // assumed (first used as an output) with that flag. A replay only has to re-check those flags.
     // A replay's CUDA graph (batch mode "graph", graph.cpp).

@@ -102,6 +102,10 @@ public:
             engine.autotune = msg.substr(15) == "on";
         } else if (msg.rfind("CUDA: learned ", 0) == 0) {
             engine.learned_on = msg.substr(14) == "on";
+        } else if (msg.rfind("CUDA: inject nvrtc ", 0) == 0) {
+            engine.inject_nvrtc_failures = stoi(msg.substr(19));
+        } else if (msg.rfind("CUDA: inject alloc ", 0) == 0) {
+            engine.inject_alloc_failures = stoi(msg.substr(19));
         }
         return ss.str() + child.message(msg);
     }

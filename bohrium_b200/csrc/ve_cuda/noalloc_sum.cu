@@ -19,8 +19,10 @@
 // (and the kernel clears it again when it finishes); the partials are overwritten by every call.
 // Calls whose kernels overlap on the GPU (on different streams, or from several host threads
 // without ordering) race on the array and give wrong results; calls ordered on one stream are safe.
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <cuda_runtime.h>
 
 extern "C" void bhb_set_last_error(const char *msg);
@@ -37,12 +39,15 @@ constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// Per-device set-up, filled by the first call on each device.
+// Per-device set-up, filled by the first call on each device. `scratch` is published with release
+// order after `max_ctas` is written, so a thread that reads a non-null `scratch` (acquire) also
+// sees `max_ctas`; concurrent first calls on one device serialise on g_setup_mutex.
 struct DeviceSetup {
-    unsigned char *scratch = nullptr;  // device address of g_noalloc_scratch
-    int64_t max_ctas = 0;              // SMs x resident CTAs per SM of noalloc_sum_kernel
+    std::atomic<unsigned char *> scratch{nullptr};  // device address of g_noalloc_scratch
+    int64_t max_ctas = 0;                           // SMs x resident CTAs per SM of noalloc_sum_kernel
 };
 DeviceSetup g_setup[kMaxDevices];
+std::mutex g_setup_mutex;
 
 __device__ __forceinline__ double block_sum(double v, double *sm) {
 #pragma unroll
@@ -145,27 +150,33 @@ extern "C" int bh_ve_cuda_sum_f64_noalloc(const double *in, int64_t n, double *o
     // scratch array and the persistent grid size. The first call on a device should come before
     // any stream capture on it.
     DeviceSetup &ds = g_setup[dev];
-    if (ds.scratch == nullptr) {
-        void *ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess) return fail("cudaGetSymbolAddress", e);
-        int sms = 0, occ = 0;
-        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e != cudaSuccess) return fail("cudaDeviceGetAttribute", e);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, noalloc_sum_kernel, kThreads, 0);
-        if (e != cudaSuccess) return fail("cudaOccupancyMaxActiveBlocksPerMultiprocessor", e);
-        ds.max_ctas = static_cast<int64_t>(sms) * (occ > 0 ? occ : 1);
-        ds.scratch = static_cast<unsigned char *>(ptr);
+    unsigned char *scratch = ds.scratch.load(std::memory_order_acquire);
+    if (scratch == nullptr) {
+        std::lock_guard<std::mutex> lock(g_setup_mutex);
+        scratch = ds.scratch.load(std::memory_order_acquire);
+        if (scratch == nullptr) {
+            void *ptr = nullptr;
+            e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+            if (e != cudaSuccess) return fail("cudaGetSymbolAddress", e);
+            int sms = 0, occ = 0;
+            e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (e != cudaSuccess) return fail("cudaDeviceGetAttribute", e);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, noalloc_sum_kernel, kThreads, 0);
+            if (e != cudaSuccess) return fail("cudaOccupancyMaxActiveBlocksPerMultiprocessor", e);
+            ds.max_ctas = static_cast<int64_t>(sms) * (occ > 0 ? occ : 1);
+            scratch = static_cast<unsigned char *>(ptr);
+            ds.scratch.store(scratch, std::memory_order_release);
+        }
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    e = cudaMemsetAsync(ds.scratch + kCounterOffset, 0, sizeof(unsigned int), s);
+    e = cudaMemsetAsync(scratch + kCounterOffset, 0, sizeof(unsigned int), s);
     if (e != cudaSuccess) return fail("cudaMemsetAsync", e);
     if (n == 0) {  // the ADD identity
         e = cudaMemsetAsync(out, 0, sizeof(double), s);
         return e == cudaSuccess ? 0 : fail("cudaMemsetAsync", e);
     }
     const int64_t grid = ntiles < ds.max_ctas ? ntiles : ds.max_ctas;
-    noalloc_sum_kernel<<<static_cast<unsigned>(grid), kThreads, 0, s>>>(in, n, out, ds.scratch);
+    noalloc_sum_kernel<<<static_cast<unsigned>(grid), kThreads, 0, s>>>(in, n, out, scratch);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail("kernel launch", e);
     return 0;

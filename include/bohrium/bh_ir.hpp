@@ -15,16 +15,6 @@ public:
     uint64_t _nrepeats;
     // Repeat while this single BH_BOOL element is true (nullptr: no condition).
     bh_base *_repeat_condition;
-    // Optional content fingerprint set by a caller that executes the same, unmodified BhIR more
-    // than once (0: unknown). An engine may use it to recognise a repeated flush without scanning
-    // the instruction list; the caller must reset it to 0 if it changes the BhIR. (Not part of the
-    // reference's BhIR; callers that never set it see no difference.)
-    uint64_t _fingerprint = 0;
-    // Set by a caller that knows the list has no sliding views and no extension-method opcodes
-    // (ids above BH_MAX_OPCODE_ID): an engine can then skip the per-execution walks over every
-    // instruction that look for them. False (unknown) by default; not part of the reference.
-    bool _plain = false;
-
     BhIR(std::vector<bh_instruction> instr_list, std::set<bh_base *> syncs, uint64_t nrepeats = 1,
          bh_base *repeat_condition = nullptr)
         : instr_list(std::move(instr_list)), _syncs(std::move(syncs)), _nrepeats(nrepeats),
@@ -34,3 +24,22 @@ public:
     uint64_t getNRepeats() const { return _nrepeats; }
     bh_base *getRepeatCondition() { return _repeat_condition; }
 };
+
+// Execution hints for a BhIR, kept beside it rather than inside it so that the BhIR keeps the
+// reference's layout. A caller that executes the same, unmodified BhIR more than once registers
+// them under the BhIR's address; engines look them up at every execution, and a BhIR that nobody
+// registered gets the defaults, which mean "unknown" and change nothing.
+//   fingerprint  a content fingerprint of the instruction list, syncs and repeat settings (0:
+//                unknown): an engine may use it to recognise a repeated flush without scanning
+//                the instruction list.
+//   plain        the list has no sliding views and no extension-method opcodes (ids above
+//                BH_MAX_OPCODE_ID), so the per-execution walks that look for them can be skipped.
+// The caller clears the entry when it changes or destroys the BhIR. The table is shared by the
+// whole process and safe to use from several threads.
+struct BhIRHints {
+    uint64_t fingerprint = 0;
+    bool plain = false;
+};
+void bh_ir_hints_set(const BhIR *ir, const BhIRHints &hints);
+BhIRHints bh_ir_hints_get(const BhIR *ir);
+void bh_ir_hints_clear(const BhIR *ir);

@@ -148,3 +148,60 @@ def scan1d_cumsum(x: np.ndarray) -> np.ndarray:
         r = np.where(valid[:, :, k], r + xs[:, :, k], r)
         out[:, :, k] = carries[:, None] + (e + r)
     return out.reshape(-1)[:n]
+
+
+# ----------------------------------------------------------------------------- error bounds
+# Unit roundoffs of float32 and float64.
+U32 = 2.0 ** -24
+U64 = 2.0 ** -53
+
+
+def gamma(d, u):
+    """gamma_d = d u / (1 - d u): a sum whose every input passes through at most d roundings
+    differs from the exact sum by at most gamma_d * sum(|x|), whatever the order of the additions
+    (N. J. Higham, Accuracy and Stability of Numerical Algorithms, 2nd ed., sec. 4.2)."""
+    d = np.asarray(d, dtype=np.float64)
+    return d * u / (1.0 - d * u)
+
+
+def scan1d_depth(n: int) -> int:
+    """Roundings on the way from any input element to any output of the engine's SCAN1D schedule
+    (see `scan1d_cumsum`), at most: 8 in the thread's run, 5 in the warp scan and 8 over the warp
+    totals of the chunk, the same 8 + 5 + 8 again over the chunk totals of a group, one per group
+    carry, and 3 to combine carry, thread prefix and run -- 45 plus the number of groups, taken
+    as 48 plus the groups."""
+    chunks = -(-n // 2048)
+    groups = -(-chunks // 2048)
+    return 48 + groups
+
+
+def assert_cumsum_within_bound(got, x, depth, u, what=""):
+    """Every output of a cumulative sum of the 1-D `x` is within gamma_depth(i) * sum_{j<=i} |x_j|
+    of the exact prefix sum (float64, or complex128 component by component; exact enough next to
+    a float32 bound). `depth` is a number or one per output."""
+    x = np.asarray(x)
+    got = np.asarray(got)
+    parts = [(np.real, "re"), (np.imag, "im")] if np.iscomplexobj(x) else [(lambda a: a, "")]
+    for f, nm in parts:
+        xv = f(x).astype(np.float64)
+        gv = f(got).astype(np.float64)
+        exact = np.cumsum(xv)
+        bound = gamma(depth, u) * np.cumsum(np.abs(xv))
+        over = np.abs(gv - exact) - bound
+        assert over.max(initial=-1.0) <= 0.0, f"{what} {nm}: worst excess over the bound {over.max():.3g} " \
+                                              f"at {int(np.argmax(over))}"
+
+
+def assert_cumprod_within_bound(got, x, u, per_mult=3.0, what=""):
+    """Every output of a cumulative product of the 1-D `x` is within ((1 + c u)^i - 1) |p_i| of
+    the exact prefix product p_i (complex128), whatever the order of the multiplications: each
+    product of i factors takes at most i - 1 multiplications by something other than 1, and each
+    complex multiplication errs by at most sqrt(5) u relative (Brent, Percival and Zimmermann,
+    Math. Comp. 76, 2007); c = 3 also covers a multiply-add contracted product."""
+    x = np.asarray(x).astype(np.complex128 if np.iscomplexobj(x) else np.float64)
+    got = np.asarray(got).astype(x.dtype)
+    exact = np.cumprod(x)
+    i = np.arange(1, x.size + 1, dtype=np.float64)
+    bound = np.expm1(i * np.log1p(per_mult * u)) * np.abs(exact)
+    over = np.abs(got - exact) - bound
+    assert over.max(initial=-1.0) <= 0.0, f"{what}: worst excess over the bound {over.max():.3g} at {int(np.argmax(over))}"

@@ -363,13 +363,18 @@ def complex_reduce_program(name, dtype, shape, axis, seed=0):
     return prog
 
 
+def complex_accumulate_input(name, dtype, shape, seed=0):
+    """Factors of modulus 0.98-1.02 near the real axis for products (no overflow or underflow over
+    1e6 of them), values in [-2, 2) + i[-2, 2) for sums."""
+    if name == "MULTIPLY_ACCUMULATE":
+        rng = np.random.default_rng(seed)
+        return ((0.98 + 0.04 * rng.random(shape)) * np.exp(0.05j * (rng.random(shape) - 0.5))).astype(dtype)
+    return cdata(shape, dtype, seed)
+
+
 def complex_accumulate_program(name, dtype, shape, axis, seed=0):
     def prog(rt):
-        rng = np.random.default_rng(seed)
-        if name == "MULTIPLY_ACCUMULATE":
-            A = ((0.98 + 0.04 * rng.random(shape)) * np.exp(0.05j * (rng.random(shape) - 0.5))).astype(dtype)
-        else:
-            A = cdata(shape, dtype, seed)
+        A = complex_accumulate_input(name, dtype, shape, seed)
         return [bh.accumulate(name, bh.array(rt, A), axis)]
     return prog
 

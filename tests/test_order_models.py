@@ -98,3 +98,14 @@ def test_grid_reduce_model_is_a_sum(n):
     assert grid_reduce_sum(x) == x.sum()
     f = np.random.default_rng(n).random(n)
     assert abs(float(grid_reduce_sum(f)) - float(np.sum(f.astype(np.longdouble)))) <= 1e-12 * n
+
+
+@pytest.mark.parametrize("n", [5, 2049, 300_001, 4_500_001])
+def test_scan1d_model_within_its_depth_bound(n):
+    """The SCAN1D order model stays inside the rounding-error bound that the GPU tests hold the
+    engine to (gamma of `scan1d_depth` times the prefix sums of |x|), and sequential float32 sums
+    inside the bound of their position."""
+    from tests.harness import U32, assert_cumsum_within_bound, scan1d_depth
+    x = np.random.default_rng(n).standard_normal(n).astype(np.float32)
+    assert_cumsum_within_bound(scan1d_cumsum(x), x, scan1d_depth(n), U32, "model")
+    assert_cumsum_within_bound(np.cumsum(x), x, np.arange(1, n + 1), U32, "sequential")

@@ -475,7 +475,18 @@ def test_scan1d(gpu_rt, oracle_rt, n, dtype, name):
         return [c, c * dtype(2)]
 
     g, o = both(gpu_rt, oracle_rt, prog)
-    tol = 0 if np.dtype(dtype).kind == "i" else (1e-4 if np.dtype(dtype) == np.float32 else 1e-11)
+    if np.dtype(dtype) == np.float32:
+        # The oracle adds sequentially, the engine in SCAN1D's fixed order (bit-exact against its
+        # order model in test_scan1d_order_is_canonical); each is held to its own rounding-error
+        # bound around the exact prefix sums, and the engine to 1e-5 relative of them.
+        from tests.harness import U32, assert_cumsum_within_bound, scan1d_depth
+        for a, b, scale, what in zip(g, o, (1, 2), ("scan", "after")):
+            assert_cumsum_within_bound(np.asarray(a) / scale, host, scan1d_depth(n), U32, what + " engine")
+            assert_cumsum_within_bound(np.asarray(b) / scale, host, np.arange(1, n + 1), U32, what + " oracle")
+            exact = np.cumsum(host.astype(np.float64)) * scale
+            np.testing.assert_allclose(np.asarray(a, dtype=np.float64), exact, rtol=1e-5, atol=0, err_msg=what)
+        return
+    tol = 0 if np.dtype(dtype).kind == "i" else 1e-11
     for a, b, what in zip(g, o, ["scan", "after"]):
         assert_close(a, b, tol, tol, what)
 

@@ -15,7 +15,6 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB = os.path.join(ROOT, "bohrium_b200", "lib")
 MAX_N = 8192 * 2048
-RTOL = 1e-12  # the float64 tolerance of the parity tests
 
 
 def _noalloc():
@@ -45,10 +44,15 @@ def test_noalloc_sum_matches_engine_on_two_calls(gpu_rt):
         x = torch.from_numpy(host).to("cuda")
         out = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
         torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        held0 = torch.cuda.memory_allocated()
         assert f(x.data_ptr(), n, out.data_ptr(), None) == 0, core.bhb_last_error()
         torch.cuda.synchronize()
+        # Nothing was allocated on the device, by the entry point or on its behalf.
+        assert torch.cuda.mem_get_info()[0] == free0 and torch.cuda.memory_allocated() == held0
         got = float(out.item())
-        assert abs(got - expect) <= RTOL * max(abs(expect), 1.0), (n, got, expect)
+        # The same tiles, order and trees as the engine's GRID_REDUCE: bit for bit its result.
+        assert got == expect, (n, got, expect)
         assert abs(got - float(np.sum(host))) <= 1e-9 * np.sum(np.abs(host))
 
 
@@ -66,7 +70,7 @@ def test_noalloc_sum_edge_sizes_and_limit(gpu_rt):
         assert f(x.data_ptr(), n, out.data_ptr(), None) == 0, core.bhb_last_error()
         torch.cuda.synchronize()
         got = float(out.item())
-        assert abs(got - expect) <= RTOL * max(abs(expect), 1.0), (n, got, expect)
+        assert got == expect, (n, got, expect)
     # Above the static scratch's capacity: rejected on the host before anything is enqueued.
     out = torch.zeros(1, dtype=torch.float64, device="cuda")
     assert f(out.data_ptr(), MAX_N + 1, out.data_ptr(), None) == -1
