@@ -799,7 +799,28 @@ public:
         return c;
     }
 
+    // Operand o (1..3) of a fused multiply-add: a view, or the constant -- with two constants,
+    // the multiplier (o = 2) is the real and the addend (o = 3) the imaginary part of the slot.
+    string fma_operand(const bh_instruction &instr, size_t o, const Scope &s) {
+        const bh_view &v = instr.operand[o];
+        if (!v.isConstant()) return name(v, s);
+        const string c = "p.c" + to_string(sym.const_id.at(&instr));
+        if (instr.constant.type == bh_type::COMPLEX64) return c + (o == 2 ? ".re" : ".im");
+        if (instr.constant.type == bh_type::COMPLEX128) return c + (o == 2 ? "_re" : "_im");
+        return c;
+    }
+
     void write_instr(const bh_instruction &instr, const Scope &s, int ind) {
+        if (is_fma_opcode(instr.opcode)) {
+            const string f = instr.operand[0].base->dtype() == bh_type::FLOAT32 ? "fmaf" : "fma";
+            const string o = name(instr.operand[0], s), a = fma_operand(instr, 1, s), b = fma_operand(instr, 2, s),
+                         c = fma_operand(instr, 3, s);
+            indent(ind);
+            if (instr.opcode == BH_X_FMA) out << o << " = " << f << "(" << a << ", " << b << ", " << c << ");\n";
+            if (instr.opcode == BH_X_FMS) out << o << " = " << f << "(" << a << ", " << b << ", -(" << c << "));\n";
+            if (instr.opcode == BH_X_FNMA) out << o << " = " << f << "(-(" << a << "), " << b << ", " << c << ");\n";
+            return;
+        }
         if (bh_opcode_is_system(instr.opcode) || instr.operand.empty()) return;
         vector<string> ops;
         if (instr.opcode == BH_RANGE) {

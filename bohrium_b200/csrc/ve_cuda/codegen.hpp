@@ -39,6 +39,7 @@
 #pragma once
 
 #include <cstdint>
+#include <set>
 #include <string>
 #include <vector>
 #include "../jitk/block.hpp"
@@ -47,6 +48,21 @@ namespace bohrium {
 namespace cuda {
 
 enum class Sched { FLAT, GRID_REDUCE, SPLIT_REDUCE, LANE_REDUCE, OUTER_REDUCE, SCAN1D, SERIAL };
+
+// Engine-internal opcodes made by contract_multiply_add() (contract.cpp), operands (out, a, b, c):
+//   BH_X_FMA   out = a*b + c      BH_X_FMS   out = a*b - c      BH_X_FNMA  out = c - a*b
+// each with one rounding. At most the multiplier b and the addend c are constants; when both are,
+// the instruction's constant is complex of the same precision, (multiplier, addend). Negative ids
+// never collide with the Bohrium bytecode or with extension methods (ids above BH_MAX_OPCODE_ID),
+// and the instructions never leave the engine's own flush.
+constexpr bh_opcode BH_X_FMA = -1001, BH_X_FMS = -1002, BH_X_FNMA = -1003;
+bool is_fma_opcode(bh_opcode op);
+// Rewrites, in place, every float32/float64 `MUL t, a, b` whose only use is one input of the next
+// instruction touching t, an ADD or SUBTRACT, after which t is freed (within 64 instructions each,
+// t not synced, a and b not written in between): the ADD becomes the fused instruction, the MUL
+// becomes BH_NONE, and FREEs of a or b in between move to just after the ADD. Returns the number
+// of contractions.
+int contract_multiply_add(std::vector<bh_instruction> &list, const std::set<bh_base *> &syncs);
 const char *sched_name(Sched s);
 
 constexpr int kThreads = 256;      // threads per CTA for every schedule

@@ -60,6 +60,7 @@ extern "C" const char *bh_ve_cuda_dry_run(bhb_ir *handle, int compile, const cha
     try {
         BhIR &bhir = *static_cast<BhIR *>(bhb_ir_bhir(handle));
         vector<bh_instruction> copy = bhir.instr_list;
+        cuda::contract_multiply_add(copy, bhir._syncs);
         set<bh_base *> frees;
         vector<bh_instruction *> instr_list = jitk::remove_non_computed_system_instr(copy, frees);
         set<const bh_base *> constructed;

@@ -100,6 +100,7 @@ EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
     prof = cfg.defaultGet<bool>("prof", false);
     verbose = cfg.defaultGet<bool>("verbose", false);
     fmad = cfg.defaultGet<bool>("fmad", false);
+    fma_contract = cfg.defaultGet<bool>("fma_contract", true);
     batch_mode = cfg.defaultGet<string>("batch", "off");
     cg_opt.bounds_check = cfg.defaultGet<bool>("bounds_check", false);
     cg_opt.flat_v = cfg.defaultGet<int>("elements_per_thread", 4);
@@ -128,6 +129,12 @@ EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
     cudaStream_t s;
     check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
     _stream = s;
+    eager_upload = cfg.defaultGet<bool>("eager_upload", true);
+    if (eager_upload) {
+        cudaStream_t cs;
+        check(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "cudaStreamCreate(copy)");
+        _copy_stream = cs;
+    }
     // Keep freed device memory in the pool (exact reuse across flushes).
     cudaMemPool_t pool;
     check(cudaDeviceGetDefaultMemPool(&pool, _device), "cudaDeviceGetDefaultMemPool");
@@ -149,9 +156,14 @@ EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
 
 EngineCUDA::~EngineCUDA() {
     try {
+        if (_copy_stream) cudaStreamSynchronize(static_cast<cudaStream_t>(_copy_stream));
         cudaStreamSynchronize(static_cast<cudaStream_t>(_stream));
-        for (auto &kv : buffers)
+        for (auto &kv : buffers) {
+            if (kv.second.arrival) cudaEventDestroy(static_cast<cudaEvent_t>(kv.second.arrival));
             if (kv.second.ptr) cudaFree(kv.second.ptr);
+        }
+        for (void *e : spare_events) cudaEventDestroy(static_cast<cudaEvent_t>(e));
+        if (_copy_stream) cudaStreamDestroy(static_cast<cudaStream_t>(_copy_stream));
         if (scratch) cudaFree(scratch);
         if (counters) cudaFree(counters);
         if (staging_dev) cudaFree(staging_dev);
@@ -193,12 +205,48 @@ void EngineCUDA::copyToDevice(bh_base *base) {
 
 void *EngineCUDA::getBuffer(bh_base *base) {
     copyToDevice(base);
-    return buffers.at(base).ptr;
+    DevBuf &b = buffers.at(base);
+    settle(b);
+    return b.ptr;
+}
+
+void EngineCUDA::settle(DevBuf &b) {
+    if (b.arrival == nullptr) return;
+    check(cudaStreamWaitEvent(static_cast<cudaStream_t>(_stream), static_cast<cudaEvent_t>(b.arrival), 0),
+          "cudaStreamWaitEvent(upload)");
+    spare_events.push_back(b.arrival);
+    b.arrival = nullptr;
+}
+
+void EngineCUDA::eager_copy(bh_base *base) {
+    cudaStream_t cs = static_cast<cudaStream_t>(_copy_stream);
+    DevBuf b;
+    b.nbytes = base->nbytes();
+    // Allocated on the copy stream: the pool only hands out memory whose earlier uses are done.
+    check(inject_alloc_failures > 0 ? (--inject_alloc_failures, cudaErrorMemoryAllocation)
+                                    : cudaMallocAsync(&b.ptr, static_cast<size_t>(b.nbytes), cs),
+          "cudaMallocAsync(upload)");
+    check(cudaMemcpyAsync(b.ptr, base->getDataPtr(), static_cast<size_t>(b.nbytes), cudaMemcpyHostToDevice, cs),
+          "cudaMemcpyAsync(H2D upload)");
+    cudaEvent_t e;
+    if (spare_events.empty()) {
+        check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate(upload)");
+    } else {
+        e = static_cast<cudaEvent_t>(spare_events.back());
+        spare_events.pop_back();
+    }
+    check(cudaEventRecord(e, cs), "cudaEventRecord(upload)");
+    b.arrival = e;
+    buffers[base] = b;
+    _stats.bytes_h2d += static_cast<uint64_t>(b.nbytes);
+    ++_stats.eager_uploads;
+    ++buffer_epoch;
 }
 
 void EngineCUDA::delBuffer(bh_base *base) {
     auto it = buffers.find(base);
     if (it == buffers.end()) return;
+    settle(it->second);
     if (it->second.ptr) {
         if (it->second.external) {
             synchronize();
@@ -287,6 +335,7 @@ void EngineCUDA::copyToHost(const set<bh_base *> &bases, bool evict) {
     for (bh_base *base : bases) {
         auto it = buffers.find(base);
         if (it == buffers.end()) continue;
+        settle(it->second);
         if (host_stale.count(base) || base->getDataPtr() == nullptr) {
             if (base->getDataPtr() == nullptr) ++buffer_epoch;
             bh_data_malloc(base);
@@ -330,6 +379,7 @@ void EngineCUDA::setMemoryPointer(bh_base *base, bool host_ptr, void *mem) {
         delBuffer(base);
         if (base->getDataPtr() != nullptr && base->getDataPtr() != mem) bh_data_free(base);
         base->resetDataPtr(mem);
+        if (eager_upload && mem != nullptr && base->nbytes() > 0 && pinned.count(mem)) eager_copy(base);
     } else {
         // Kernels load whole elements (16 bytes at once for complex128): an address that is not a
         // multiple of the element size would be a misaligned access on the device.
@@ -1255,6 +1305,7 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
     vector<bh_base *> base_ids;
     bool sliding = false;
     Replay replay;
+    if (fma_contract) _stats.fma_contractions += static_cast<uint64_t>(contract_multiply_add(bhir->instr_list, bhir->_syncs));
     const uint64_t key = prepare(bhir->instr_list, instr_list, base_ids, sliding, fingerprint ? &replay : nullptr);
     const auto t1 = chrono::steady_clock::now();
     _stats.time_prepare += chrono::duration<double>(t1 - t0).count();
@@ -1535,6 +1586,7 @@ string EngineCUDA::statistics() const {
        << "\nfuse_cache_misses: " << _stats.fuse_cache_misses << "\nkernel_cache_hits: " << _stats.kernel_cache_hits
        << "\nkernel_cache_misses: " << _stats.kernel_cache_misses << "\ndisk_cache_hits: " << _stats.disk_cache_hits
        << "\ndisk_cache_rejected: " << _stats.disk_cache_rejected
+       << "\nfma_contractions: " << _stats.fma_contractions << "\neager_uploads: " << _stats.eager_uploads
        << "\nbytes_h2d: " << _stats.bytes_h2d << "\nbytes_d2h: " << _stats.bytes_d2h
        << "\ntime_fusion: " << _stats.time_fusion << "\ntime_codegen: " << _stats.time_codegen
        << "\ntime_compile: " << _stats.time_compile << "\nparallel_compiles: " << _stats.parallel_compiles

@@ -46,6 +46,7 @@ struct Stats {
     uint64_t fuse_cache_hits = 0, fuse_cache_misses = 0;
     uint64_t plan_cache_hits = 0, plan_cache_misses = 0, replays = 0;
     uint64_t kernel_cache_hits = 0, kernel_cache_misses = 0, disk_cache_hits = 0, disk_cache_rejected = 0;
+    uint64_t fma_contractions = 0, eager_uploads = 0;
     uint64_t bytes_h2d = 0, bytes_d2h = 0;
     uint64_t serial_units = 0;
     // learned fusion: structures tried with both plans, kept learned / kept greedy, learned plan
@@ -158,6 +159,7 @@ public:
     jitk::FusionConfig fusion_config;
     std::string batch_mode = "off"; // off | grouped | graph
     bool fmad = false;
+    bool fma_contract = true; // multiply-add contraction on the bytecode (contract.cpp)
     bool autotune = true;            // tune register caps of kernels with large work
     int64_t tune_min_elements = 1 << 20;
     std::string cache_dir;
@@ -174,8 +176,18 @@ private:
     struct DevBuf {
         void *ptr = nullptr;
         int64_t nbytes = 0;
-        bool external = false; // adopted from setMemoryPointer(host_ptr=false)
+        bool external = false;    // adopted from setMemoryPointer(host_ptr=false)
+        void *arrival = nullptr;  // cudaEvent_t of an eager upload the engine's stream has not waited for
     };
+    // Eager uploads: page-locked host data handed over with setMemoryPointer(host_ptr=true) is
+    // copied at once on a copy stream of its own, so that the copy overlaps kernels on the
+    // engine's stream that do not read it. The engine's stream waits for the copy (settle) before
+    // anything on it uses the buffer.
+    bool eager_upload = true;
+    void *_copy_stream = nullptr;
+    std::vector<void *> spare_events;
+    void eager_copy(bh_base *base);
+    void settle(DevBuf &b);
     std::unordered_map<bh_base *, DevBuf> buffers;
     std::set<bh_base *> host_stale; // device copy newer than the host copy
     std::set<void *> pinned;        // host blocks from host_alloc()

@@ -63,6 +63,10 @@ bool EngineCUDA::graph_usable(const ReplayGraph &g) const {
 }
 
 void EngineCUDA::graph_launch(ReplayGraph &g) {
+    for (const auto &bp : g.persistent) {
+        auto it = buffers.find(bp.first);
+        if (it != buffers.end()) settle(it->second);
+    }
     check(cudaGraphLaunch(static_cast<cudaGraphExec_t>(g.exec), static_cast<cudaStream_t>(_stream)), "cudaGraphLaunch");
     if (g.stale_epoch != stale_epoch) {
         for (bh_base *b : g.written) host_stale.insert(b);

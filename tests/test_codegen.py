@@ -221,3 +221,47 @@ def test_heat_step_stages_stencil_rows_in_shared_memory():
     assert "bh_work_staged(p, lo, hi)" in src and "bh_stage_ok(p, lo, hi)" in src
     assert "// bh_dynamic_shared_bytes: 65600" in src  # 4 rows of 4,100 floats
     assert "cp.async.cg.shared.global" in src
+
+
+def _fma_count(units):
+    """Fused multiply-adds per element: the FLAT and GRID_REDUCE bodies are written twice (full
+    tiles without bounds checks, the last one with them)."""
+    import re
+    n = sum(len(re.findall(r"\bfmaf?\(", u["source"])) for u in units)
+    assert n % 2 == 0, n
+    return n // 2
+
+
+def test_black_scholes_multiply_adds_are_contracted_on_the_bytecode():
+    """Every product whose only use is one add or subtract, after which it is freed, becomes one
+    fused multiply-add before fusion: 17 per option in a Black-Scholes iteration (the erf
+    polynomials, the drift term, d2 and the call price)."""
+    def prog(rt):
+        S, K, T = (bh.empty(rt, (10000,), np.float64) for _ in range(3))
+        return [W.black_scholes_iteration(rt, S, K, T, 0)]
+    res, units = plan(prog)
+    assert _fma_count(units) == 17
+
+
+@pytest.mark.parametrize("case", ["plain", "synced", "reused", "written_between", "float_only"])
+def test_multiply_add_contraction_conditions(case):
+    """Contraction needs a float product read once by the next instruction that touches it (an
+    add or subtract), freed after that, not synced, with its inputs not written in between."""
+    dt = np.int32 if case == "float_only" else np.float32
+
+    def prog(rt):
+        a = bh.empty(rt, (4096,), dt)
+        b = bh.empty(rt, (4096,), dt)
+        t = a * b
+        outs = []
+        if case == "written_between":
+            bh.binary("ADD", a, dt(1), out=a)
+        r = t + b
+        if case == "reused":
+            outs.append(t * dt(3))
+        if case == "synced":
+            outs.append(t)
+        del t
+        return [r] + outs
+    res, units = plan(prog)
+    assert _fma_count(units) == (1 if case == "plain" else 0), case
