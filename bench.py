@@ -242,26 +242,66 @@ def run_ours(args, world, rank, local):
     del irs, outs, inputs
 
     # ---- end to end through the C ABI with page-locked host buffers ---------------------
-    (s, k, t), hosts, irs, outs, _ = build_black_scholes(bh, W, rt, ex, n, pinned=True)
+    # Every step hands page-locked host inputs (240 MB) to the engine with bhb_data_set, runs the
+    # 10 flushes and reads the 10 means back. Two forms:
+    #   serial     a step hands over its own inputs, then computes on them;
+    #   pipelined  two input sets alternate: a step hands over the NEXT step's inputs before running
+    #              its own flushes, so the engine's eager upload (a copy stream) overlaps them. The
+    #              clock stops after the last upload has landed, so the timed region holds exactly
+    #              one 240 MB upload and one read-back per step.
+    sets = [build_black_scholes(bh, W, rt, ex, n, pinned=True) for _ in range(2)]
 
-    def e2e_step():
-        for arr, h in zip((s, k, t), hosts):
-            ex.lib.bhb_data_set(ex.rt, arr.base.handle, 1, h.ctypes.data)  # hand over host data (re-upload)
-        for ir in irs:
+    def hand_over(st):
+        (s_, k_, t_), hosts, _, _, _ = st
+        for arr, h in zip((s_, k_, t_), hosts):
+            if ex.lib.bhb_data_set(ex.rt, arr.base.handle, 1, h.ctypes.data) != 0:  # new host data: re-upload
+                raise RuntimeError("bhb_data_set failed")
+
+    def run_set(st):
+        for ir in st[2]:
             ir.execute()
-        return sync_read(bh, ex, outs)
+        return sync_read(bh, ex, st[3])
 
-    for _ in range(2):
-        e2e_step()
-    barrier(world)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_step()
-    e2e_s = allreduce_max(world, time.perf_counter() - t0)
+    def serial_step():
+        hand_over(sets[0])
+        return run_set(sets[0])
+
+    cur = [0]
+
+    def pipelined_step():
+        hand_over(sets[1 - cur[0]])
+        r = run_set(sets[cur[0]])
+        cur[0] = 1 - cur[0]
+        return r
+
+    def timed(step_fn, prime=None):
+        if prime:
+            prime()
+        for _ in range(2):
+            step_fn()
+        ex.message("CUDA: sync")
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step_fn()
+        ex.message("CUDA: sync")  # both streams: the last upload has landed
+        return allreduce_max(world, time.perf_counter() - t0)
+
+    e2e_serial_s = timed(serial_step)
+    e2e_s = timed(pipelined_step, prime=lambda: hand_over(sets[0]))
+    want_means = [W.black_scholes_numpy(*sets[0][4], it) for it in range(2)] if rank == 0 else None
+    got_means = [float(v) for v in (ex.peek(o.base)[0] for o in sets[0][3][:2])]
+    e2e_check = rank != 0 or all(abs(g - w) <= 1e-10 * abs(w) for g, w in zip(got_means, want_means))
     e2e = {"value": round(world * bytes_step * args.steps / e2e_s / 1e9, 2), "unit": "GB/s",
            "h2d_bytes_per_step": 3 * 8 * n, "d2h_bytes_per_step": 8 * BS_ITERS,
-           "ms_per_step": round(e2e_s * 1e3 / args.steps, 3)}
-    del irs, outs, s, k, t
+           "ms_per_step": round(e2e_s * 1e3 / args.steps, 3), "form": "pipelined",
+           "serial": {"value": round(world * bytes_step * args.steps / e2e_serial_s / 1e9, 2),
+                      "ms_per_step": round(e2e_serial_s * 1e3 / args.steps, 3)},
+           "result_check": e2e_check,
+           "note": "pipelined: the next step's inputs are handed over before this step's flushes and "
+                   "uploaded on the engine's copy stream while they run; serial: hand-over, upload, "
+                   "flushes, read-back in turn"}
+    del sets
 
     extra = {}
     if args.extra and rank == 0:

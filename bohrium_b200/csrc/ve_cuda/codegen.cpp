@@ -1187,6 +1187,22 @@ void declare_chain_temps(Emitter &em, Symbols &sym, Scope &scope, const vector<c
     }
 }
 
+// A heavy element body -- many instructions, or float64 divisions and transcendentals -- is
+// bound by the arithmetic pipes rather than by memory latency.
+bool heavy_body(const LoopB &L) {
+    int n = 0, heavy = 0;
+    for (const InstrPtr &i : jitk::all_instr(L)) {
+        ++n;
+        const bh_opcode op = i->opcode;
+        const bool f64 = !i->operand.empty() && !i->operand[0].isConstant() &&
+                         i->operand[0].base->dtype() == bh_type::FLOAT64;
+        if (f64 && (op == BH_DIVIDE || op == BH_EXP || op == BH_LOG || op == BH_SQRT || op == BH_POWER ||
+                    op == BH_SIN || op == BH_COS || op == BH_TANH))
+            ++heavy;
+    }
+    return n > 24 || heavy > 0;
+}
+
 // FLAT: `loop` has P >= 1 leading parallel ranks.
 // Views that an innermost element loop only reads: the view's base is an array (not a
 // temporary) that no instruction of the kernel writes, and the view is read by a plain
@@ -1304,7 +1320,8 @@ LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) 
     // the compiler can issue every load of the unrolled loop early), the last chunk with them.
     const string n_inner = "p.n" + to_string(sym.loop_id.at(&inner));
     const string idx_decl = "const bh_i64 i" + to_string(P - 1) + " = cbase + j * " + to_string(kThreads) + ";";
-    const vector<bh_view> pre = u.V > 1 ? preloadable_views(inner, L, sym) : vector<bh_view>{};
+    const vector<bh_view> pre =
+        u.V > 1 && !(heavy_body(inner) && !opt.preload_heavy) ? preloadable_views(inner, L, sym) : vector<bh_view>{};
     for (int path = 0; path < 2; ++path) {
         // path 0: full chunks without bounds checks; path 1: the last chunk, with them.
         const string guard = path == 0 ? "" : "i" + to_string(P - 1) + " >= " + n_inner;
@@ -2181,7 +2198,10 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
     // all K x 8 elements of the thread; the last item checks every index. Tile k accumulates into
     // slot k, elements j = 0..7 in order, in both paths.
     const string n0 = "p.n" + to_string(sym.loop_id.at(&L));
-    const vector<bh_view> pre = preloadable_views(L, L, sym);
+    // Loading every element's inputs up front keeps K x 8 loads in flight for memory-bound bodies;
+    // a heavy body is bound by its arithmetic, and the preloaded registers would cost occupancy
+    // (Black-Scholes: 80 registers and 3 CTAs per SM with them, 48 and 5 without).
+    const vector<bh_view> pre = heavy_body(L) && !opt.preload_heavy ? vector<bh_view>{} : preloadable_views(L, L, sym);
     map<ViewKey, string> acc_k;
     for (size_t k = 0; k < reds.size(); ++k) acc_k[ViewKey(reds[k]->operand[0])] = accs[k] + "[k]";
     for (int path = 0; path < 2; ++path) {

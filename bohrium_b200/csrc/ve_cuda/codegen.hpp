@@ -123,6 +123,7 @@ struct LaunchUnit {
 struct CodegenOptions {
     bool bounds_check = false; // emit index checks that record violations instead of accessing
     int flat_v = 4;            // elements per thread in FLAT
+    bool preload_heavy = false; // preload the inputs of heavy (arithmetic-bound) element bodies too
 };
 
 // Lower one kernel (as produced by jitk::get_kernel_list) into launch units executed in order.

@@ -104,6 +104,7 @@ EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
     batch_mode = cfg.defaultGet<string>("batch", "off");
     cg_opt.bounds_check = cfg.defaultGet<bool>("bounds_check", false);
     cg_opt.flat_v = cfg.defaultGet<int>("elements_per_thread", 4);
+    cg_opt.preload_heavy = cfg.defaultGet<bool>("preload_heavy", false);
     // The GPU reduces over the outermost axis natively, so sweeps may fuse with maps at rank 0.
     fusion_config = jitk::FusionConfig(cfg, false);
     cache_dir = cfg.defaultGet<string>("cache_dir", "");
@@ -182,6 +183,12 @@ EngineCUDA::~EngineCUDA() {
 }
 
 void EngineCUDA::synchronize() { check(cudaStreamSynchronize(static_cast<cudaStream_t>(_stream)), "cudaStreamSynchronize"); }
+
+void EngineCUDA::synchronize_all() {
+    if (_copy_stream)
+        check(cudaStreamSynchronize(static_cast<cudaStream_t>(_copy_stream)), "cudaStreamSynchronize(copy)");
+    synchronize();
+}
 
 // ------------------------------------------------------------------------------------- memory
 void EngineCUDA::copyToDevice(bh_base *base) {

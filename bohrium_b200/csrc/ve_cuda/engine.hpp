@@ -89,6 +89,7 @@ public:
     void *getBuffer(bh_base *base); // device pointer (allocated/uploaded on demand)
     void mark_device_written(bh_base *base) { host_stale.insert(base); }
     void delBuffer(bh_base *base);
+    void synchronize_all();  // the engine stream and the copy stream of eager uploads
     void synchronize();
 
     // Page-locked host memory that the engine frees (cudaFreeHost) when its base is freed.

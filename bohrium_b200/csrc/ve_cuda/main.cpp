@@ -65,7 +65,7 @@ public:
             ss << engine.last_execute_ms();
             return ss.str();
         } else if (msg == "CUDA: sync") {
-            engine.synchronize();
+            engine.synchronize_all();
         } else if (msg == "CUDA: timer start") {
             engine.timer_start();
         } else if (msg == "CUDA: timer stop") {
