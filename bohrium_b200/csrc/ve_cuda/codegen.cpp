@@ -9,6 +9,7 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <regex>
 #include <set>
 #include <sstream>
 #include <stdexcept>
@@ -31,6 +32,7 @@ const char *sched_name(Sched s) {
         case Sched::OUTER_REDUCE: return "outer_reduce";
         case Sched::SCAN1D: return "scan1d";
         case Sched::SERIAL: return "serial";
+        case Sched::TILE2D: return "tile2d";
     }
     return "?";
 }
@@ -53,6 +55,7 @@ int64_t LaunchUnit::work_items() const {
         case Sched::OUTER_REDUCE: return (rows * cols + kThreads - 1) / kThreads;
         case Sched::SCAN1D: return chunks;  // chunks: work items of the phase
         case Sched::SERIAL: return 1;
+        case Sched::TILE2D: return (rows + V - 1) / V * ((cols + 63) / 64);  // V: rows per tile
     }
     return 1;
 }
@@ -339,6 +342,37 @@ template <typename C> __device__ __forceinline__ C bh_cpow(C a, C b) {
 )CUDA";
 
 // ---------------------------------------------------------------------------- operation emitting
+// TMA and mbarrier helpers of TILE2D units (inline PTX for sm_100a). A tensor map is a kernel
+// parameter (the plain kernel's __grid_constant__ struct), so the bulk-tensor copy reads it from
+// parameter space. Waits on an mbarrier poll a bounded number of times and report failure instead
+// of spinning forever.
+const char *kTmaPrelude = R"CUDA(
+struct alignas(64) bh_tmap { unsigned long long w[16]; };
+__device__ __forceinline__ unsigned bh_saddr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void bh_mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bh_saddr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void bh_mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void bh_mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bh_saddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool bh_mbar_try_wait(unsigned long long *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok) : "r"(bh_saddr(bar)), "r"(parity) : "memory");
+    return ok != 0u;
+}
+__device__ __forceinline__ bool bh_mbar_wait(unsigned long long *bar, unsigned parity) {
+    for (int i = 0; i < (1 << 20); ++i)
+        if (bh_mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bh_tma_2d(void *dst, const bh_tmap *map, int x, int y, unsigned long long *bar) {
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                 :: "r"(bh_saddr(dst)), "l"(map), "r"(x), "r"(y), "r"(bh_saddr(bar)) : "memory");
+}
+)CUDA";
+
 bool is_float(bh_type t) { return t == bh_type::FLOAT32 || t == bh_type::FLOAT64; }
 
 // Name of a math function for element type `t` (float uses the f-suffixed variant, as C's
@@ -937,6 +971,25 @@ struct ParamLayout {
         fields.push_back(f);
         decl << "    alignas(8) " << ctype << " " << name << ";\n";
     }
+    // A 128-byte, 64-byte aligned tensor map: 16 slots. Tensor maps come first in P, so no
+    // padding precedes them.
+    void add_tmap(ParamField f, const string &name) {
+        for (int k = 0; k < 16; ++k) {
+            f.part = k;
+            fields.push_back(f);
+        }
+        decl << "    bh_tmap " << name << ";\n";
+    }
+    // Round the struct up to a multiple of 64 bytes (its alignment with tensor maps), so that its
+    // size is exactly 8 bytes per field.
+    void pad64() {
+        int k = 0;
+        while (fields.size() % 8 != 0) add(work_pad(), "bh_i64", "pad" + to_string(k++));
+    }
+    static ParamField work_pad() {
+        ParamField f{ParamField::I64};
+        return f;
+    }
 };
 
 void add_common_fields(Symbols &sym, ParamLayout &pl, const CodegenOptions &opt) {
@@ -1070,6 +1123,7 @@ void finish_source(LaunchUnit &u, const string &params_decl, const string &body,
     src << kPrelude;
     auto uses = [&](const char *name) { return params_decl.find(name) != string::npos || body.find(name) != string::npos; };
     if (uses("bh_c64") || uses("bh_c128")) src << kComplexPrelude;
+    if (uses("bh_tmap")) src << kTmaPrelude;
     if (opt.bounds_check) src << bounds_check_helper();
     src << "struct P {\n" << params_decl << "};\n";
     src << body;
@@ -1343,6 +1397,188 @@ LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) 
     u.elements = rows * u.cols;
     finish_source(u, pl.decl.str(), body.str(), opt);
     return u;
+}
+
+// ------------------------------------------------------------------------------------- TILE2D
+// A 2-D map (loop ranks 0 and 1 parallel, rank 1 innermost) that reads arrays through transposed
+// views: stride 1 along rank 0 and a positive stride (the array's row length) along rank 1. The
+// plain FLAT schedule walks rank 1 across a warp, so each warp load of such a view touches 32
+// rows. Here a work item is a tile of TR rows x 64 columns of the index space, TR = 128 bytes /
+// element size; thread t handles column t % 64 and rows (t / 64) * TR/4 ... + TR/4 - 1, so each
+// output row of the tile is written by consecutive threads. A transposed view's part of a tile is
+// a TR x 64 box of its base array (64 rows of 128 contiguous bytes), brought into a 4-stage
+// shared-memory ring by one TMA copy per tile, up to 4 tiles ahead, with the 128-byte swizzle; a
+// thread reads its TR/4 values as two 16-byte words (distinct banks across every 8 threads).
+constexpr int kTileCols = 64;
+constexpr int kTileStages = 4;
+constexpr int kTileBoxBytes = kTileCols * 128;
+
+// The transposed views of `inner` that TILE2D stages: read-only (their base is not written by the
+// kernel), 2-D, stride 1 along rank 0 and > 1 along rank 1, 4- or 8-byte elements (all the same
+// size), at most two. Empty when the loop does not qualify.
+vector<bh_view> tile2d_views(const LoopB &L, const LoopB &inner, const Symbols &sym, const CodegenOptions &opt) {
+    if (!opt.tile2d || opt.bounds_check || !inner.isInnermost() || !L._sweeps.empty() || !inner._sweeps.empty()) return {};
+    if (L.size < 32 || inner.size < kTileCols) return {};
+    set<const bh_base *> written;
+    for (const InstrPtr &i : jitk::all_instr(L)) {
+        if (bh_opcode_is_sweep(i->opcode)) return {};
+        if (!i->operand.empty() && !i->operand[0].isConstant()) written.insert(i->operand[0].base);
+    }
+    vector<bh_view> ret;
+    set<ViewKey> seen;
+    int esize = 0;
+    for (const bh_view &v : preloadable_views(inner, L, sym)) {
+        if (v.ndim != 2 || v.stride[0] != 1 || v.stride[1] <= 1 || written.count(v.base)) continue;
+        const int es = bh_type_size(v.base->dtype());
+        if (bh_type_is_complex(v.base->dtype()) || (es != 4 && es != 8) || v.base->dtype() == bh_type::R123) continue;
+        if (esize != 0 && es != esize) return {};
+        esize = es;
+        if (seen.insert(ViewKey(v)).second) ret.push_back(v);
+    }
+    if (ret.size() > 2) return {};
+    return ret;
+}
+
+bool lower_tile2d(const LoopB &loop, const CodegenOptions &opt, LaunchUnit &u) {
+    const Block holder(loop);
+    Symbols sym = build_symbols({&holder}, {});
+    const LoopB &L = holder.getLoop();
+    const vector<const LoopB *> chain = jitk::get_first_loop_blocks(L);
+    if (chain.size() < 2) return false;
+    const LoopB &inner = *chain[1];
+    const vector<bh_view> tv = tile2d_views(L, inner, sym, opt);
+    if (tv.empty()) return false;
+    const int esize = bh_type_size(tv[0].base->dtype());
+    const int TR = 128 / esize, RPT = TR / 4;  // rows per tile, rows per thread
+    u = LaunchUnit();
+    u.sched = Sched::TILE2D;
+    u.V = TR;
+    u.rows = L.size;
+    u.cols = inner.size;
+    const int64_t tiles_c = (u.cols + kTileCols - 1) / kTileCols;
+    ParamLayout pl;
+    for (size_t k = 0; k < tv.size(); ++k) {
+        ParamField f{ParamField::TMAP};
+        f.base = tv[k].base;
+        f.i64 = tv[k].start;
+        f.tm_ld = tv[k].stride[1];
+        f.tm_box = TR;
+        f.tm_rows = u.rows;
+        f.tm_cols = u.cols;
+        pl.add_tmap(f, "tm" + to_string(k));
+    }
+    add_common_fields(sym, pl, opt);
+    pl.add(work_field(tiles_c), "bh_i64", "tiles_c");
+    pl.add(work_field(u.work_items()), "bh_i64", "work");
+    for (size_t k = 0; k < tv.size(); ++k) {
+        // Tensor coordinates of the view's element (0, 0): column and row of its base array.
+        const int64_t ld = tv[k].stride[1];
+        pl.add(work_field(tv[k].start >= 0 ? tv[k].start % ld : 0), "bh_i64", "tx" + to_string(k));
+        pl.add(work_field(tv[k].start >= 0 ? tv[k].start / ld : 0), "bh_i64", "ty" + to_string(k));
+    }
+    ParamField ok{ParamField::TMA_OK};
+    pl.add(ok, "bh_i64", "tma_ok");
+    ParamField err{ParamField::SCRATCH};
+    err.i64 = -1;  // the engine's error record
+    pl.add(err, "unsigned long long*", "err");
+    pl.pad64();
+
+    const string T = cuda_type(tv[0].base->dtype());
+    const string rows = "p.n" + to_string(sym.loop_id.at(&L)), cols = "p.n" + to_string(sym.loop_id.at(&inner));
+    stringstream body;
+    body << "// bh_dynamic_shared_bytes: " << kTileStages * static_cast<int>(tv.size()) * kTileBoxBytes + 1024 << "\n";
+    body << "template <bool STAGED> __device__ __forceinline__ void bh_tile(const P &p, bh_i64 w, const unsigned char *stage) {\n";
+    body << pointer_locals(sym);
+    body << "    const bh_i64 tr = w / p.tiles_c;\n";
+    body << "    const bh_i64 tc = w - tr * p.tiles_c;\n";
+    body << "    const int c = threadIdx.x & 63, rq = threadIdx.x >> 6;\n";
+    body << "    const bh_i64 i1 = tc * 64 + c;\n";
+    body << "    const bh_i64 rbase = tr * " << TR << " + rq * " << RPT << ";\n";
+    for (size_t k = 0; k < tv.size(); ++k) {
+        body << "    " << T << " tv" << k << "[" << RPT << "];\n";
+        body << "    if (STAGED) {\n";
+        body << "        const unsigned char *row = stage + " << k * kTileBoxBytes << " + c * 128;\n";
+        body << "        const uint4 q0 = *(const uint4 *)(row + (((2 * rq) ^ (c & 7)) << 4));\n";
+        body << "        const uint4 q1 = *(const uint4 *)(row + (((2 * rq + 1) ^ (c & 7)) << 4));\n";
+        body << "        memcpy(&tv" << k << "[0], &q0, 16);\n";
+        body << "        memcpy((char *)&tv" << k << "[0] + 16, &q1, 16);\n";
+        body << "    }\n";
+    }
+    for (int path = 0; path < 2; ++path) {
+        body << (path == 0 ? "    if (rbase + " + to_string(RPT) + " <= " + rows + " && i1 < " + cols + ") {\n"
+                           : "    } else {\n");
+        Scope scope;
+        Emitter eb(sym, body, opt);
+        for (size_t k = 0; k < tv.size(); ++k) scope.repl[ViewKey(tv[k])] = "tv" + to_string(k) + "[e]";
+        if (path == 0) body << "#pragma unroll\n";
+        body << "        for (int e = 0; e < " << RPT << "; ++e) {\n";
+        body << "            const bh_i64 i0 = rbase + e;\n";
+        if (path == 1) body << "            if (i0 >= " << rows << " || i1 >= " << cols << ") break;\n";
+        for (size_t k = 0; k < tv.size(); ++k)
+            body << "            if (!STAGED) tv" << k << "[e] = " << eb.array_ref(tv[k]) << ";\n";
+        declare_chain_temps(eb, sym, scope, chain, 1, body, 12);
+        eb.write_body(inner, scope, 12);
+        body << "        }\n";
+    }
+    body << "    }\n}\n";
+    body << "__device__ __forceinline__ void bh_work(const P &p, bh_i64 w) { bh_tile<false>(p, w, nullptr); }\n";
+    // One thread issues a tile's boxes: expect their bytes on the stage's barrier, then copy.
+    body << "__device__ __forceinline__ void bh_tile_issue(const P &p, bh_i64 w, unsigned char *stage, unsigned long long *bar) {\n";
+    body << "    const bh_i64 tr = w / p.tiles_c;\n";
+    body << "    const bh_i64 tc = w - tr * p.tiles_c;\n";
+    body << "    bh_mbar_expect_tx(bar, " << tv.size() * kTileBoxBytes << "u);\n";
+    for (size_t k = 0; k < tv.size(); ++k)
+        body << "    bh_tma_2d(stage + " << k * kTileBoxBytes << ", &p.tm" << k << ", (int)(p.tx" << k << " + tr * " << TR
+             << "), (int)(p.ty" << k << " + tc * 64), bar);\n";
+    body << "}\n";
+    const int stage_bytes = static_cast<int>(tv.size()) * kTileBoxBytes;
+    body << R"CUDA(__device__ __forceinline__ void bh_main(const P &p) {
+    if (!p.tma_ok) {
+        for (bh_i64 w = blockIdx.x; w < p.work; w += gridDim.x) bh_tile<false>(p, w, nullptr);
+        return;
+    }
+    extern __shared__ unsigned char bh_dyn[];
+    // The 128-byte swizzle repeats every 1024 bytes: the ring starts on a 1024-byte boundary.
+    unsigned char *ring = bh_dyn + ((1024u - (bh_saddr(bh_dyn) & 1023u)) & 1023u);
+    __shared__ alignas(8) unsigned long long bar[)CUDA" << kTileStages << R"CUDA(];
+    __shared__ int fail;
+    const bh_i64 first = blockIdx.x, step = gridDim.x;
+    const int mine = first < p.work ? (int)((p.work - 1 - first) / step + 1) : 0;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < )CUDA" << kTileStages << R"CUDA(; ++s) bh_mbar_init(&bar[s], 1u);
+        bh_mbar_fence_init();
+        fail = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int it = 0; it < )CUDA" << kTileStages << R"CUDA( && it < mine; ++it)
+            bh_tile_issue(p, first + it * step, ring + it * )CUDA" << stage_bytes << R"CUDA(, &bar[it]);
+    int it = 0;
+    for (; it < mine; ++it) {
+        const int s = it % )CUDA" << kTileStages << R"CUDA(;
+        if (!bh_mbar_wait(&bar[s], (unsigned)((it / )CUDA" << kTileStages << R"CUDA() & 1))) fail = 1;
+        __syncthreads();
+        if (fail) break;
+        bh_tile<true>(p, first + it * step, ring + s * )CUDA" << stage_bytes << R"CUDA();
+        __syncthreads();  // every thread is done with the stage
+        if (threadIdx.x == 0 && it + )CUDA" << kTileStages << R"CUDA( < mine)
+            bh_tile_issue(p, first + (it + )CUDA" << kTileStages << R"CUDA() * step, ring + s * )CUDA" << stage_bytes << R"CUDA(, &bar[s]);
+    }
+    if (fail && threadIdx.x == 0) {
+        // A tile load never completed: record it, and let the copies already issued into the
+        // ring land (bounded) before the CTA leaves.
+        atomicCAS(p.err, 0ull, 0xC000000000000000ull | (unsigned long long)blockIdx.x);
+        for (int j = it; j < mine && j < it + )CUDA" << kTileStages << R"CUDA(; ++j)
+            bh_mbar_wait(&bar[j % )CUDA" << kTileStages << R"CUDA(], (unsigned)((j / )CUDA" << kTileStages << R"CUDA() & 1));
+    }
+}
+)CUDA";
+    body << kKernels;
+    u.fields = pl.fields;
+    u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
+    u.elements = u.rows * u.cols;
+    finish_source(u, pl.decl.str(), body.str(), opt);
+    return true;
 }
 
 // Parallel points below which an inner reduction is split along its swept axis, and the number of
@@ -2074,6 +2310,24 @@ string block_reduce_all_fn(const vector<string> &ctypes, const vector<bh_opcode>
 // Tiles per GRID_REDUCE work item: with many tiles a CTA takes K consecutive tiles at once so that
 // K x 8 loads per thread are in flight together. Every tile keeps its own partial, reduced in the
 // same order, so the result does not depend on K; K only depends on the tile count.
+// The element body of GRID_REDUCE's full tiles written for two elements at once: every line
+// (one statement or declaration per instruction) is followed by its copy for the next element, with
+// temporaries t<N> renamed t<N>_1, the index i0 renamed i0_1 and preloaded slots [k * 8 + j] moved
+// to [k * 8 + j + 1]. Accumulator updates keep their order: element j's before element j + 1's.
+string interleave_second_element(const string &block) {
+    static const regex tmp("\\bt([0-9]+)\\b"), idx("\\bi0\\b");
+    const string slot = "[k * " + to_string(kReduceV) + " + j]", slot1 = "[k * " + to_string(kReduceV) + " + j + 1]";
+    stringstream in(block), out;
+    string line;
+    while (getline(in, line)) {
+        string second = regex_replace(regex_replace(line, tmp, "t$1_1"), idx, "i0_1");
+        for (size_t at = second.find(slot); at != string::npos; at = second.find(slot, at + slot1.size()))
+            second.replace(at, slot.size(), slot1);
+        out << line << "\n" << second << "\n";
+    }
+    return out.str();
+}
+
 int grid_tiles_per_item(int64_t ntiles, const LoopB &L) {
     // Only light element code is memory-latency bound; a heavy body (many instructions, float64
     // math) is compute bound and would only lose occupancy to the extra registers.
@@ -2198,10 +2452,12 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
     // all K x 8 elements of the thread; the last item checks every index. Tile k accumulates into
     // slot k, elements j = 0..7 in order, in both paths.
     const string n0 = "p.n" + to_string(sym.loop_id.at(&L));
-    // Loading every element's inputs up front keeps K x 8 loads in flight for memory-bound bodies;
-    // a heavy body is bound by its arithmetic, and the preloaded registers would cost occupancy
-    // (Black-Scholes: 80 registers and 3 CTAs per SM with them, 48 and 5 without).
-    const vector<bh_view> pre = heavy_body(L) && !opt.preload_heavy ? vector<bh_view>{} : preloadable_views(L, L, sym);
+    const bool heavy = heavy_body(L);
+    // Loading every element's inputs up front keeps K x 8 loads in flight. A heavy body pays for
+    // them in registers (Black-Scholes: 80 and 3 CTAs per SM with them, 48 and 5 without) and is
+    // still faster with them (0.174 vs 0.188 ms per 10M options on a B200), so `preload_heavy`
+    // is on by default.
+    const vector<bh_view> pre = heavy && !opt.preload_heavy ? vector<bh_view>{} : preloadable_views(L, L, sym);
     map<ViewKey, string> acc_k;
     for (size_t k = 0; k < reds.size(); ++k) acc_k[ViewKey(reds[k]->operand[0])] = accs[k] + "[k]";
     for (int path = 0; path < 2; ++path) {
@@ -2230,6 +2486,23 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
         body << "#pragma unroll\n";
         body << "        for (int k = 0; k < " << K << "; ++k) {\n";
         if (path == 1) body << "            if (k >= ktiles) break;\n";
+        if (path == 0 && heavy && opt.interleave == 2) {
+            // Two elements per step, statement by statement (elements j and j + 1; reductions
+            // still fold j before j + 1): independent chains side by side for the scheduler.
+            body << "#pragma unroll\n";
+            body << "            for (int j = 0; j < " << kReduceV << "; j += 2) {\n";
+            body << "                const bh_i64 i0 = (tile0 + k) * " << kReduceTile << " + j * " << kThreads
+                 << " + threadIdx.x;\n";
+            body << "                const bh_i64 i0_1 = i0 + " << kThreads << ";\n";
+            stringstream one;
+            Emitter e1(sym, one, opt);
+            e1.external_acc = acc_k;
+            e1.write_body(L, scope, 16);
+            body << interleave_second_element(one.str());
+            body << "            }\n";
+            body << "        }\n";
+            continue;
+        }
         if (path == 0) body << "#pragma unroll\n";
         body << "            for (int j = 0; j < " << kReduceV << "; ++j) {\n";
         body << "                const bh_i64 i0 = (tile0 + k) * " << kReduceTile << " + j * " << kThreads
@@ -2785,6 +3058,7 @@ LaunchUnit fuse_tail(const LaunchUnit &u1, const LaunchUnit &u2) {
         return false;
     };
     if (uses("bh_c64") || uses("bh_c128")) src << kComplexPrelude;
+    if (uses("bh_tmap")) src << kTmaPrelude;
     src << "namespace bh_u1 {\nstruct P {\n" << u1.params_decl << "};\n" << u1.body_core << "} // namespace bh_u1\n";
     src << "namespace bh_u2 {\nstruct P {\n" << u2.params_decl << "};\n" << u2.body_core << "} // namespace bh_u2\n";
     src << kTailWrappers;
@@ -2851,7 +3125,12 @@ vector<LaunchUnit> lower_kernel(const LoopB &kernel, const CodegenOptions &opt) 
             } else if (sub != nullptr && split_chunks(points, sub->size) > 1) {
                 units.push_back(lower_split_reduce(L, P, opt));
             } else {
-                units.push_back(lower_flat(L, P, opt));
+                LaunchUnit tu;
+                if (P == 2 && lower_tile2d(L, opt, tu)) {
+                    units.push_back(std::move(tu));
+                } else {
+                    units.push_back(lower_flat(L, P, opt));
+                }
             }
             continue;
         }
@@ -2933,7 +3212,9 @@ vector<int> fuse_tails(const vector<LoopB> &kernels, vector<vector<LaunchUnit>> 
             commutes = !meets(writes[m], reads[j]) && !meets(writes[m], writes[j]) && !meets(reads[m], writes[j]);
         if (!commutes || lowered[k].empty() || into[k] >= 0) continue;
         LaunchUnit &u1 = lowered[k].back();
-        if (u1.tail || u1.sched == Sched::SCAN1D || u1.sched == Sched::SERIAL || u1.body_core.empty()) continue;
+        if (u1.tail || u1.sched == Sched::SCAN1D || u1.sched == Sched::SERIAL || u1.sched == Sched::TILE2D ||
+            u1.body_core.empty())
+            continue;
         u1 = fuse_tail(u1, lowered[j][0]);
         lowered[j].clear();
         into[j] = static_cast<int>(k);

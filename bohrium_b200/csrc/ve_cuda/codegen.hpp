@@ -31,6 +31,12 @@
 //                 instructions: three units -- chunk totals, one-CTA exclusive scan of the totals,
 //                 re-scan with the carry -- each with a fixed block scan (order set by the length).
 //   SERIAL        anything else: one thread runs the nest in program order (always correct).
+//   TILE2D        a 2-D map that reads arrays through transposed views (unit stride along the outer
+//                 rank): tiles of (128 bytes / element) rows x 64 columns; each transposed view's
+//                 tile is one box of its base array, loaded by TMA (cp.async.bulk.tensor.2d, 128-byte
+//                 swizzle) into a 4-stage shared-memory ring ahead of the compute, so both the box
+//                 reads and the output rows are contiguous. Grouped launches and views the tensor
+//                 maps cannot describe take the same tiles with plain loads.
 //
 // Loop sizes, view offsets/strides and constants are kernel parameters. The source also fixes a
 // few choices derived from the sizes (lanes per point, tiles per work item, iterations per lane,
@@ -47,7 +53,7 @@
 namespace bohrium {
 namespace cuda {
 
-enum class Sched { FLAT, GRID_REDUCE, SPLIT_REDUCE, LANE_REDUCE, OUTER_REDUCE, SCAN1D, SERIAL };
+enum class Sched { FLAT, GRID_REDUCE, SPLIT_REDUCE, LANE_REDUCE, OUTER_REDUCE, SCAN1D, SERIAL, TILE2D };
 
 // Engine-internal opcodes made by contract_multiply_add() (contract.cpp), operands (out, a, b, c):
 //   BH_X_FMA   out = a*b + c      BH_X_FMS   out = a*b - c      BH_X_FNMA  out = c - a*b
@@ -72,13 +78,21 @@ constexpr int64_t kScanChunk = 4096; // elements per chunk in SCAN1D
 
 // One 8-byte slot (or two for 16-byte constants) of the kernel parameter struct.
 struct ParamField {
-    enum Kind { PTR, I64, CONST, R123_START, R123_KEY, SCRATCH, COUNTER } kind;
+    enum Kind { PTR, I64, CONST, R123_START, R123_KEY, SCRATCH, COUNTER, TMAP, TMA_OK } kind;
     bh_base *base = nullptr; // PTR
     int64_t i64 = 0;         // I64
     bh_constant c{};         // CONST / R123_*
     int64_t origin = -1;     // CONST / R123_*: origin id of the instruction holding the constant
     int part = 0;            // CONST: which 8 bytes of the constant (1: the imaginary part of a complex128)
     int64_t off = 0;         // COUNTER: index offset in the unit's counters
+    // TMAP: one of the 16 slots (`part`) of a TMA tensor map of `base`, which the engine encodes at
+    // launch: a 2-D tiled map of the base seen as rows of `tm_ld` elements (as many whole rows as
+    // it holds), 128-byte swizzle, boxes of `tm_box` x 64 elements. `i64` is the start of the view
+    // the map serves; the view covers `tm_rows` elements along a row and `tm_cols` rows.
+    int64_t tm_ld = 0, tm_box = 0, tm_rows = 0, tm_cols = 0;
+    // TMA_OK: 1 when the engine encoded every tensor map of the unit for a plain launch and each
+    // view lies inside its map with 16-byte aligned rows and start; 0 otherwise (grouped launches,
+    // unaligned views), which selects the unit's code path without TMA.
 };
 
 struct LaunchUnit {
@@ -123,7 +137,9 @@ struct LaunchUnit {
 struct CodegenOptions {
     bool bounds_check = false; // emit index checks that record violations instead of accessing
     int flat_v = 4;            // elements per thread in FLAT
-    bool preload_heavy = false; // preload the inputs of heavy (arithmetic-bound) element bodies too
+    bool preload_heavy = true;  // preload the inputs of heavy (arithmetic-bound) element bodies too
+    int interleave = 1;         // GRID_REDUCE: elements of a heavy body written side by side (1 or 2)
+    bool tile2d = true;         // TILE2D for maps over transposed views (else FLAT)
 };
 
 // Lower one kernel (as produced by jitk::get_kernel_list) into launch units executed in order.

@@ -1,6 +1,7 @@
 // Device-free inspection of the engine's lowering: fuse a BhIR, generate the kernel sources and
 // optionally compile them with NVRTC for sm_100a. Used by the CPU test-suite to check every code
 // path up to the launch on a machine without a GPU.
+#include <cstdlib>
 #include <cstring>
 #include <set>
 #include <sstream>
@@ -93,6 +94,9 @@ extern "C" const char *bh_ve_cuda_dry_run(bhb_ir *handle, int compile, const cha
         cfg.avoid_mixed_sweeps = true;
         const vector<jitk::LoopB> kernels = jitk::get_kernel_list(instr_list, cfg);
         cuda::CodegenOptions opt;
+        // The engine's codegen keys, from the environment as the config would give them.
+        if (const char *v = getenv("BH_CUDA_INTERLEAVE")) opt.interleave = atoi(v);
+        if (const char *v = getenv("BH_CUDA_PRELOAD_HEAVY")) opt.preload_heavy = string(v) == "true" || string(v) == "1";
         vector<vector<cuda::LaunchUnit>> lowered(kernels.size());
         for (size_t k = 0; k < kernels.size(); ++k)
             if (!kernels[k].isSystemOnly()) lowered[k] = cuda::lower_kernel(kernels[k], opt);

@@ -66,6 +66,9 @@ struct DeviceApi {
     CUresult (*cuGetErrorString)(CUresult, const char **) = nullptr;
     CUresult (*cuFuncGetAttribute)(int *, CUfunction_attribute, CUfunction) = nullptr;
     CUresult (*cuFuncSetAttribute)(CUfunction, CUfunction_attribute, int) = nullptr;
+    CUresult (*cuTensorMapEncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                       const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                       CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill) = nullptr;
 
     template <typename F>
     void get(const char *name, F &fp) {
@@ -84,6 +87,7 @@ struct DeviceApi {
         get("cuGetErrorString", cuGetErrorString);
         get("cuFuncGetAttribute", cuFuncGetAttribute);
         get("cuFuncSetAttribute", cuFuncSetAttribute);
+        get("cuTensorMapEncodeTiled", cuTensorMapEncodeTiled);
     }
     void ck(CUresult r, const char *what) const {
         if (r != CUDA_SUCCESS) {
@@ -104,7 +108,9 @@ EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
     batch_mode = cfg.defaultGet<string>("batch", "off");
     cg_opt.bounds_check = cfg.defaultGet<bool>("bounds_check", false);
     cg_opt.flat_v = cfg.defaultGet<int>("elements_per_thread", 4);
-    cg_opt.preload_heavy = cfg.defaultGet<bool>("preload_heavy", false);
+    cg_opt.preload_heavy = cfg.defaultGet<bool>("preload_heavy", true);
+    cg_opt.interleave = cfg.defaultGet<int>("interleave", 1);
+    cg_opt.tile2d = cfg.defaultGet<bool>("tile2d", true);
     // The GPU reduces over the outermost axis natively, so sweeps may fuse with maps at rank 0.
     fusion_config = jitk::FusionConfig(cfg, false);
     cache_dir = cfg.defaultGet<string>("cache_dir", "");
@@ -188,6 +194,22 @@ void EngineCUDA::synchronize_all() {
     if (_copy_stream)
         check(cudaStreamSynchronize(static_cast<cudaStream_t>(_copy_stream)), "cudaStreamSynchronize(copy)");
     synchronize();
+    check_tma_record();
+}
+
+// A TILE2D kernel whose tile loads did not complete within its bounded wait records that in the
+// error record (top bits 11) and skips the rest of its tiles. Read at synchronisation points only,
+// so that flushes stay asynchronous.
+void EngineCUDA::check_tma_record() {
+    if (!tma_check_pending) return;
+    tma_check_pending = false;
+    unsigned long long v = 0;
+    check(cudaMemcpy(&v, err_record, sizeof(v), cudaMemcpyDeviceToHost), "cudaMemcpy(err)");
+    if ((v >> 62) == 3ULL) {
+        check(cudaMemset(err_record, 0, sizeof(v)), "cudaMemset(err)");
+        throw runtime_error("a TILE2D kernel gave up waiting for a TMA tile load (CTA " +
+                            to_string(v & 0xffffffffULL) + "); its outputs are incomplete");
+    }
 }
 
 // ------------------------------------------------------------------------------------- memory
@@ -356,7 +378,10 @@ void EngineCUDA::copyToHost(const set<bh_base *> &bases, bool evict) {
             if (host_stale.erase(base)) ++stale_epoch;
         }
     }
-    if (any) synchronize();
+    if (any) {
+        synchronize();
+        check_tma_record();
+    }
     if (evict)
         for (bh_base *base : bases) delBuffer(base);
 }
@@ -673,15 +698,74 @@ EngineCUDA::Compiled *EngineCUDA::compiled_for(const LaunchUnit &u) {
 // Scratch bytes a unit needs for its partials.
 static int64_t unit_scratch(const LaunchUnit &u) { return u.scratch_bytes(); }
 
+// The TMA tensor map of a TILE2D view (see ParamField::TMAP): base `b` at device address `p` as a
+// 2-D array of rows of tm_ld elements, boxes of tm_box x 64 elements with the 128-byte swizzle.
+// Writes the 128-byte map to `out` and returns true, or returns false (the unit then runs without
+// TMA) when the view does not fit: a TMA copy needs 16-byte aligned base, rows and start column,
+// and the view must lie inside whole rows of the map without wrapping to the next row.
+bool EngineCUDA::encode_tile_map(const ParamField &f, const bh_base *b, void *p, uint8_t *out) {
+    const int64_t esize = bh_type_size(b->dtype());
+    const int64_t ld = f.tm_ld, start = f.i64;
+    if (ld <= 0 || start < 0 || p == nullptr) return false;
+    const int64_t nrows = b->nelem() / ld;
+    const int64_t ocol = start % ld, orow = start / ld;
+    if ((ld * esize) % 16 != 0 || (ocol * esize) % 16 != 0 || reinterpret_cast<uintptr_t>(p) % 16 != 0) return false;
+    if (ocol + f.tm_rows > ld || orow + f.tm_cols > nrows || ld >= (int64_t{1} << 31) || nrows >= (int64_t{1} << 31))
+        return false;
+    CUtensorMapDataType dt;
+    switch (b->dtype()) {
+        case bh_type::FLOAT32: dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT32; break;
+        case bh_type::FLOAT64: dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT64; break;
+        case bh_type::INT32: dt = CU_TENSOR_MAP_DATA_TYPE_INT32; break;
+        case bh_type::UINT32: dt = CU_TENSOR_MAP_DATA_TYPE_UINT32; break;
+        case bh_type::INT64: dt = CU_TENSOR_MAP_DATA_TYPE_INT64; break;
+        case bh_type::UINT64: dt = CU_TENSOR_MAP_DATA_TYPE_UINT64; break;
+        default: return false;
+    }
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(ld), static_cast<cuuint64_t>(nrows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld * esize)};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(f.tm_box), 64u};
+    const cuuint32_t estr[2] = {1u, 1u};
+    CUtensorMap map;
+    if (api->cuTensorMapEncodeTiled(&map, dt, 2, p, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                    CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    static_assert(sizeof(CUtensorMap) == 128, "CUtensorMap is 128 bytes");
+    memcpy(out, &map, sizeof(map));
+    return true;
+}
+
 void EngineCUDA::pack_params(const PlanUnit &pu, const vector<bh_base *> &bases,
                              const vector<bh_instruction *> &instrs, int64_t scratch_off, int64_t counter_idx,
                              uint8_t *out) {
     const LaunchUnit &u = pu.unit;
     memset(out, 0, u.fields.size() * 8);
+    bool tma_ok = !packing_grouped;
     for (size_t i = 0; i < u.fields.size(); ++i) {
         const ParamField &f = u.fields[i];
         uint8_t *slot = out + i * 8;
         switch (f.kind) {
+            case ParamField::TMAP: {
+                // All 16 slots are written with the first one; a grouped launch gets no map.
+                if (f.part != 0 || !tma_ok) break;
+                const int idx = pu.ptr_base[i];
+                bh_base *b = idx >= 0 ? bases[static_cast<size_t>(idx)] : f.base;
+                void *p = ptr_override != nullptr && idx >= 0 && (*ptr_override)[static_cast<size_t>(idx)] != nullptr
+                              ? (*ptr_override)[static_cast<size_t>(idx)]
+                              : getBuffer(b);
+                tma_ok = encode_tile_map(f, b, p, slot);
+                break;
+            }
+            case ParamField::TMA_OK: {
+                const int64_t v = tma_ok ? 1 : 0;
+                memcpy(slot, &v, 8);
+                if (tma_ok) {
+                    tma_check_pending = true;
+                    ++_stats.tma_units;
+                }
+                break;
+            }
             case ParamField::PTR: {
                 const int idx = pu.ptr_base[i];
                 bh_base *b = idx >= 0 ? bases[static_cast<size_t>(idx)] : f.base;
@@ -835,11 +919,13 @@ void EngineCUDA::launch_batched(const vector<const PlanUnit *> &group, const vec
     uint8_t *host = staging_alloc(bytes);
     int64_t *prefix = reinterpret_cast<int64_t *>(host + items_bytes);
     int64_t total = 0;
+    packing_grouped = true;  // tensor maps need the plain kernel's parameter space
     for (size_t k = 0; k < n; ++k) {
         pack_params(*group[k], bases, instrs, scratch_off[k], counter_off[k], host + k * psize);
         prefix[k] = total;
         total += group[k]->unit.work_items();
     }
+    packing_grouped = false;
     prefix[n] = total;
     if (total == 0) return;
     uint8_t *dev = device_staging(bytes);
@@ -1158,7 +1244,8 @@ EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const
                 pu.compiled = compiled_for(u);
                 pu.ptr_base.assign(u.fields.size(), -1);
                 for (size_t f = 0; f < u.fields.size(); ++f)
-                    if (u.fields[f].kind == ParamField::PTR) pu.ptr_base[f] = idx(u.fields[f].base);
+                    if (u.fields[f].kind == ParamField::PTR || u.fields[f].kind == ParamField::TMAP)
+                        pu.ptr_base[f] = idx(u.fields[f].base);
                 pu.unit = std::move(u);
                 pk.units.push_back(std::move(pu));
             }
@@ -1594,6 +1681,7 @@ string EngineCUDA::statistics() const {
        << "\nkernel_cache_misses: " << _stats.kernel_cache_misses << "\ndisk_cache_hits: " << _stats.disk_cache_hits
        << "\ndisk_cache_rejected: " << _stats.disk_cache_rejected
        << "\nfma_contractions: " << _stats.fma_contractions << "\neager_uploads: " << _stats.eager_uploads
+       << "\ntma_units: " << _stats.tma_units
        << "\nbytes_h2d: " << _stats.bytes_h2d << "\nbytes_d2h: " << _stats.bytes_d2h
        << "\ntime_fusion: " << _stats.time_fusion << "\ntime_codegen: " << _stats.time_codegen
        << "\ntime_compile: " << _stats.time_compile << "\nparallel_compiles: " << _stats.parallel_compiles

@@ -46,7 +46,7 @@ struct Stats {
     uint64_t fuse_cache_hits = 0, fuse_cache_misses = 0;
     uint64_t plan_cache_hits = 0, plan_cache_misses = 0, replays = 0;
     uint64_t kernel_cache_hits = 0, kernel_cache_misses = 0, disk_cache_hits = 0, disk_cache_rejected = 0;
-    uint64_t fma_contractions = 0, eager_uploads = 0;
+    uint64_t fma_contractions = 0, eager_uploads = 0, tma_units = 0;
     uint64_t bytes_h2d = 0, bytes_d2h = 0;
     uint64_t serial_units = 0;
     // learned fusion: structures tried with both plans, kept learned / kept greedy, learned plan
@@ -73,6 +73,11 @@ public:
     // next N kernel compilations fail as NVRTC failures, the next N array allocations as
     // cudaErrorMemoryAllocation, without calling NVRTC or the allocator.
     int inject_nvrtc_failures = 0, inject_alloc_failures = 0;
+    // TILE2D tensor maps: encoded per plain launch (grouped launches run those units without TMA).
+    bool packing_grouped = false;
+    bool tma_check_pending = false;  // a TMA unit ran since the error record was last read
+    bool encode_tile_map(const ParamField &f, const bh_base *b, void *p, uint8_t *out);
+    void check_tma_record();
     void handleExecution(BhIR *bhir);          // one pass over the instruction list
     void handleExtmethod(BhIR *bhir);          // split around extension methods
     // ComponentImpl::userKernel with tag "cuda": compile `kernel` with NVRTC, run its

@@ -167,6 +167,7 @@ bool EngineCUDA::build_graph(Replay &r) {
                 L.params.assign(L.items_bytes + (n + 1) * sizeof(int64_t), 0);
                 int64_t *prefix = reinterpret_cast<int64_t *>(L.params.data() + L.items_bytes);
                 int64_t soff = 0, coff = 0, total = 0;
+                packing_grouped = true;
                 for (size_t k = 0; k < n; ++k) {
                     pack_params(*grp[k], bases, instrs, soff, coff, L.params.data() + k * psize);
                     soff += (grp[k]->unit.scratch_bytes() + 255) / 256 * 256;
@@ -174,6 +175,7 @@ bool EngineCUDA::build_graph(Replay &r) {
                     prefix[k] = total;
                     total += grp[k]->unit.work_items();
                 }
+                packing_grouped = false;
                 prefix[n] = total;
                 if (total == 0) continue;
                 L.nitems = static_cast<int>(n);

@@ -141,6 +141,9 @@ class Flush:
     syncs: list = field(default_factory=list)  # Base
     nrepeats: int = 1
     condition: Optional[Base] = None
+    # Bases that the flush's BH_FREEs free: their handles must outlive every execution of the
+    # flush (a compiled flush keeps them until it is destroyed).
+    released: list = field(default_factory=list)
 
 
 def encode(instrs: Sequence[Instr]) -> np.ndarray:

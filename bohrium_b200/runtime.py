@@ -148,7 +148,7 @@ class NativeExecutor:
                                    slides.ctypes.data, len(slides))
         if not h:
             raise RuntimeError("bhb_ir_create: " + _err(self.lib))
-        return NativeIR(self, h, (words, slides))
+        return NativeIR(self, h, (words, slides), flush.released)
 
     def execute(self, flush: ir.Flush) -> None:
         words = ir.encode(flush.instrs)
@@ -187,8 +187,9 @@ class NativeExecutor:
 class NativeIR:
     """A decoded flush that can be executed repeatedly (bhb_ir_execute)."""
 
-    def __init__(self, ex: NativeExecutor, handle, keep):
+    def __init__(self, ex: NativeExecutor, handle, keep, released=()):
         self.ex, self.handle, self._keep = ex, handle, keep
+        self._released = list(released)  # bases freed by the flush: released with the handle
 
     def execute(self):
         if self.ex.lib.bhb_ir_execute(self.ex.rt, self.handle) != 0:
@@ -198,6 +199,9 @@ class NativeIR:
         try:
             if self.handle:
                 self.ex.lib.bhb_ir_destroy(self.handle)
+                self.handle = None
+            for b in self._released:
+                self.ex.release(b)
         except Exception:
             pass
 
@@ -236,6 +240,9 @@ class Runtime:
             self.ex.release(b)
 
     def take(self) -> ir.Flush:
-        """Remove and return the pending instructions as a Flush (not executed)."""
+        """Remove and return the pending instructions as a Flush (not executed). The bases its
+        BH_FREEs free go with it (Flush.released): a compiled flush releases them when it is
+        destroyed, so a later flush of this runtime cannot release bases it still uses."""
         instrs, self.instrs = self.instrs, []
-        return ir.Flush(instrs)
+        released, self._released = self._released, []
+        return ir.Flush(instrs, released=released)

@@ -265,3 +265,31 @@ def test_multiply_add_contraction_conditions(case):
         return [r] + outs
     res, units = plan(prog)
     assert _fma_count(units) == (1 if case == "plain" else 0), case
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64, np.int32])
+def test_transposed_views_lower_to_tma_tiles(dt):
+    """A 2-D map reading through transposed views is a TILE2D unit: TMA boxes of 128 bytes x 64
+    rows per view, the tensor maps first in the parameter struct, the struct a whole number of
+    64-byte blocks."""
+    def prog(rt):
+        a = bh.empty(rt, (300, 500), dt)
+        b = bh.empty(rt, (500, 300), dt)
+        c = bh.empty(rt, (500, 300), dt)
+        return [a + b.T * dt(2) + c.T]
+    res, units = plan(prog)
+    assert [u["sched"] for u in units] == ["tile2d"]
+    src = units[0]["source"]
+    assert src.count("cp.async.bulk.tensor.2d") == 1 and src.count("bh_tma_2d(stage") == 2
+    assert "bh_tmap tm0;" in src and "bh_tmap tm1;" in src
+    assert src.index("bh_tmap tm0;") < src.index("a0;")
+    assert "bh_mbar_wait" in src and "(1 << 20)" in src  # bounded waits
+
+
+def test_untransposed_and_complex_maps_stay_flat():
+    def prog(rt):
+        a = bh.empty(rt, (300, 500), np.float32)
+        z = bh.empty(rt, (500, 300), np.complex64)
+        return [a + a, z.T * z.T]
+    res, units = plan(prog)
+    assert [u["sched"] for u in units] == ["flat", "flat"]
