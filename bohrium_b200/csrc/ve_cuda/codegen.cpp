@@ -69,6 +69,11 @@ int64_t LaunchUnit::scratch_bytes() const {
 
 int64_t LaunchUnit::counters_needed() const {
     int64_t own = 0;
+    if (sched == Sched::SCAN1D && single_pass) {
+        // chunk flags, group flags (one spare), ticket, CTAs that left, abort
+        const int64_t ngroups = (chunks + kThreads * 8 - 1) / (kThreads * 8);
+        own = chunks + ngroups + 1 + 3;
+    }
     if (sched == Sched::GRID_REDUCE) own = 1;
     if (sched == Sched::SPLIT_REDUCE) own = (rows * cols + kThreads - 1) / kThreads;
     if (sched == Sched::SCAN1D && scan_gate) own = 1;
@@ -1333,6 +1338,134 @@ void emit_preload(Emitter &em, const vector<bh_view> &views, int V, const string
     for (size_t k = 0; k < views.size(); ++k) scope.repl[ViewKey(views[k])] = "pl" + to_string(k) + "[j]";
 }
 
+// 128-bit access for FLAT: thread t of a work item handles the 4 consecutive elements
+// cbase .. cbase + 3 (cbase = chunk * 1024 + 4t) of the innermost parallel rank, so a view with
+// unit stride along it is one 16-byte (or 4 x element size) word per thread. Read-only such views
+// are loaded, and arrays written by the element code stored, as whole words when every such view's
+// first element is aligned to the word (checked per work item); otherwise, and for views with other
+// strides, element by element. The written values stay in registers until the words are stored,
+// and later reads of them in the element code use the registers. Every element is computed by the
+// same statements either way, so the results do not depend on the path.
+// Views that can be moved as words: unit stride along the innermost rank `axis`, an array (not a
+// temporary) of any element type.
+bool unit_stride_view(const bh_view &v, int axis, const Symbols &sym) {
+    if (v.isConstant() || sym.temps.count(v.base) || v.ndim != axis + 1) return false;
+    return v.stride[axis] == 1;
+}
+
+// Loads or stores of `bytes` bytes at `addr` (a register array `reg`) as the widest aligned words.
+string word_copy(const string &dst, const string &src, int bytes) {
+    stringstream ss;
+    if (bytes >= 16) {
+        for (int k = 0; k < bytes / 16; ++k)
+            ss << "((uint4 *)(" << dst << "))[" << k << "] = ((const uint4 *)(" << src << "))[" << k << "]; ";
+    } else if (bytes == 8) {
+        ss << "*(uint2 *)(" << dst << ") = *(const uint2 *)(" << src << "); ";
+    } else {
+        ss << "*(unsigned *)(" << dst << ") = *(const unsigned *)(" << src << "); ";
+    }
+    return ss.str();
+}
+
+void emit_flat_vector(Symbols &sym, ostream &body, const CodegenOptions &opt, const LoopB &inner,
+                      const vector<const LoopB *> &chain, unsigned P, const vector<bh_view> &pre, int64_t per,
+                      const string &n_inner, const string &iv) {
+    const int axis = static_cast<int>(P) - 1;
+    // Written views that can be stored as words: outputs of elementwise instructions of `inner`,
+    // unit stride, their base written and read in the kernel through this one view only.
+    map<const bh_base *, set<ViewKey>> touched;
+    for (const InstrPtr &i : jitk::all_instr(inner))
+        for (const bh_view &v : i->operand)
+            if (!v.isConstant()) touched[v.base].insert(ViewKey(v));
+    vector<bh_view> outs;
+    set<ViewKey> seen_out;
+    for (const InstrPtr &i : jitk::all_instr(inner)) {
+        const bh_opcode op = i->opcode;
+        if (bh_opcode_is_system(op) || bh_opcode_is_sweep(op) || op == BH_GATHER || op == BH_SCATTER ||
+            op == BH_COND_SCATTER || i->operand.empty())
+            continue;
+        const bh_view &v = i->operand[0];
+        if (!unit_stride_view(v, axis, sym) || sym.always_array.count(v.base) || touched[v.base].size() != 1) continue;
+        if (seen_out.insert(ViewKey(v)).second) outs.push_back(v);
+    }
+    vector<bool> vec_pre(pre.size());
+    for (size_t k = 0; k < pre.size(); ++k) vec_pre[k] = unit_stride_view(pre[k], axis, sym);
+    Emitter em(sym, body, opt);
+    body << "    const bh_i64 cbase = chunk * " << per << " + threadIdx.x * 4;\n";
+    body << "    if ((chunk + 1) * " << per << " <= " << n_inner << ") {\n";
+    // Word alignment of every word-moved view at element cbase.
+    body << "        bool vec = true;\n";
+    body << "        {\n";
+    body << "            const bh_i64 " << iv << " = cbase;\n";
+    auto align_check = [&](const bh_view &v) {
+        const int bytes = min(16, 4 * static_cast<int>(bh_type_size(v.base->dtype())));
+        body << "            vec = vec && (((unsigned long long)&" << em.array_ref(v) << ") & " << bytes - 1 << "ull) == 0;\n";
+    };
+    for (size_t k = 0; k < pre.size(); ++k)
+        if (vec_pre[k]) align_check(pre[k]);
+    for (const bh_view &v : outs) align_check(v);
+    body << "        }\n";
+    Scope scope;
+    for (size_t k = 0; k < pre.size(); ++k) {
+        const string T = cuda_type(pre[k].base->dtype());
+        body << "        " << T << " pl" << k << "[4];\n";
+        const int bytes = 4 * static_cast<int>(bh_type_size(pre[k].base->dtype()));
+        if (vec_pre[k]) {
+            body << "        if (vec) {\n";
+            body << "            const bh_i64 " << iv << " = cbase;\n";
+            body << "            " << word_copy("pl" + to_string(k), "&" + em.array_ref(pre[k]), bytes) << "\n";
+            body << "        } else {\n";
+        } else {
+            body << "        {\n";
+        }
+        body << "#pragma unroll\n";
+        body << "            for (int j = 0; j < 4; ++j) {\n";
+        body << "                const bh_i64 " << iv << " = cbase + j;\n";
+        body << "                pl" << k << "[j] = " << em.array_ref(pre[k]) << ";\n";
+        body << "            }\n";
+        body << "        }\n";
+        scope.repl[ViewKey(pre[k])] = "pl" + to_string(k) + "[j]";
+    }
+    for (size_t k = 0; k < outs.size(); ++k) {
+        body << "        " << cuda_type(outs[k].base->dtype()) << " so" << k << "[4];\n";
+        scope.repl[ViewKey(outs[k])] = "so" + to_string(k) + "[j]";
+    }
+    body << "#pragma unroll\n";
+    body << "        for (int j = 0; j < 4; ++j) {\n";
+    body << "            const bh_i64 " << iv << " = cbase + j;\n";
+    {
+        Emitter eb(sym, body, opt);
+        declare_chain_temps(eb, sym, scope, chain, P - 1, body, 12);
+        eb.write_body(inner, scope, 12);
+    }
+    body << "        }\n";
+    for (size_t k = 0; k < outs.size(); ++k) {
+        const int bytes = 4 * static_cast<int>(bh_type_size(outs[k].base->dtype()));
+        body << "        if (vec) {\n";
+        body << "            const bh_i64 " << iv << " = cbase;\n";
+        body << "            " << word_copy("&" + em.array_ref(outs[k]), "so" + to_string(k), bytes) << "\n";
+        body << "        } else {\n";
+        body << "#pragma unroll\n";
+        body << "            for (int j = 0; j < 4; ++j) {\n";
+        body << "                const bh_i64 " << iv << " = cbase + j;\n";
+        body << "                " << em.array_ref(outs[k]) << " = so" << k << "[j];\n";
+        body << "            }\n";
+        body << "        }\n";
+    }
+    body << "    } else {\n";
+    {
+        Scope s1;
+        Emitter eb(sym, body, opt);
+        body << "        for (int j = 0; j < 4; ++j) {\n";
+        body << "            const bh_i64 " << iv << " = cbase + j;\n";
+        body << "            if (" << iv << " >= " << n_inner << ") break;\n";
+        declare_chain_temps(eb, sym, s1, chain, P - 1, body, 12);
+        eb.write_body(inner, s1, 12);
+        body << "        }\n";
+    }
+    body << "    }\n";
+}
+
 LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) {
     LaunchUnit u;
     u.sched = Sched::FLAT;
@@ -1369,13 +1502,23 @@ LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) 
         }
     }
     body << "    (void)rem;\n";
+    const vector<bh_view> pre =
+        u.V > 1 && !(heavy_body(inner) && !opt.preload_heavy) ? preloadable_views(inner, L, sym) : vector<bh_view>{};
+    const string n_inner = "p.n" + to_string(sym.loop_id.at(&inner));
+    const string iv = "i" + to_string(P - 1);
+    if (u.V == 4 && opt.vector_access && !opt.bounds_check) {
+        emit_flat_vector(sym, body, opt, inner, chain, P, pre, per, n_inner, iv);
+        body << "}\n" << kWrappers;
+        u.fields = pl.fields;
+        u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
+        u.elements = rows * u.cols;
+        finish_source(u, pl.decl.str(), body.str(), opt);
+        return u;
+    }
     body << "    const bh_i64 cbase = chunk * " << per << " + threadIdx.x;\n";
     // The element body is written once and used twice: full chunks run without bounds checks (so
     // the compiler can issue every load of the unrolled loop early), the last chunk with them.
-    const string n_inner = "p.n" + to_string(sym.loop_id.at(&inner));
     const string idx_decl = "const bh_i64 i" + to_string(P - 1) + " = cbase + j * " + to_string(kThreads) + ";";
-    const vector<bh_view> pre =
-        u.V > 1 && !(heavy_body(inner) && !opt.preload_heavy) ? preloadable_views(inner, L, sym) : vector<bh_view>{};
     for (int path = 0; path < 2; ++path) {
         // path 0: full chunks without bounds checks; path 1: the last chunk, with them.
         const string guard = path == 0 ? "" : "i" + to_string(P - 1) + " >= " + n_inner;
@@ -2889,6 +3032,335 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
     return units;
 }
 
+// SCAN1D in one pass (single_pass): every CTA takes chunks by ticket (an atomic counter, so all
+// lower chunks belong to CTAs that are already running), stages and folds its chunk as unit A
+// does, publishes the chunk total behind a release flag, and then looks back: it waits for the
+// totals of the chunks before it in its group of 2048 and evaluates unit B's per-thread folds and
+// block scan over them (entries past its own are left out, which does not change the prefix at
+// its own position), and waits for the carry into its group, which the last chunk of the previous
+// group publishes as that group's carry op its total. The chunk then rescans its staged elements
+// as unit C does. Every value is formed by the same operations in the same order as in the three
+// units, so the result is bit-identical to them, while each element is read from memory once.
+// Waits poll a bounded number of times (`p.spin_cap`; negative: none); when one runs out, or
+// another CTA gave up, the chunk is abandoned and an abort flag raised. The CTA that leaves last
+// then recomputes the whole scan alone with the three units' steps, and resets the flags and
+// counters for the next launch.
+LaunchUnit lower_scan1d_single(const LoopB &loop, const InstrPtr &acc, const CodegenOptions &opt) {
+    const Block holder(loop);
+    const LoopB &L = holder.getLoop();
+    const int64_t n = L.size;
+    const int64_t nchunks = (n + kScanTile - 1) / kScanTile;
+    const int64_t ngroups = (nchunks + kScanTile - 1) / kScanTile;
+    const bh_type t = acc->operand[0].base->dtype();
+    const string T = cuda_type(t);
+    const bh_opcode rop = scan_reduce_op(acc->opcode);
+    const string ident = constant_literal(jitk::sweep_identity(rop, t));
+    auto op = [&](const string &a, const string &b) { return reduce_expr(rop, a, b); };
+    LaunchUnit u;
+    u.sched = Sched::SCAN1D;
+    u.single_pass = true;
+    u.no_batch = true;
+    u.cols = n;
+    u.chunks = nchunks;
+    Symbols sym = build_symbols({&holder}, {});
+    ParamLayout pl;
+    add_common_fields(sym, pl, opt);
+    pl.add(work_field(nchunks), "bh_i64", "nchunks");
+    pl.add(work_field(ngroups), "bh_i64", "ngroups");
+    pl.add(work_field(nchunks), "bh_i64", "work");
+    ParamField cap{ParamField::I64};
+    cap.i64 = opt.scan_spin_cap;
+    pl.add(cap, "bh_i64", "spin_cap");
+    ParamField fs{ParamField::SCRATCH};
+    pl.add(fs, "unsigned char*", "scratch");
+    ParamField fc{ParamField::COUNTER};
+    pl.add(fc, "unsigned int*", "counter");
+    stringstream body;
+    Emitter em(sym, body, opt);
+    body << block_scan_fn(T, "bh_block_scan", rop, ident);
+    body << R"CUDA(__device__ __forceinline__ unsigned bh_ld_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void bh_st_release(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+// Poll *flag until it is set: false when `cap` polls ran out (at once for a negative cap) or
+// another CTA raised the abort flag.
+__device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *abort_flag, long long cap) {
+    long long spins = 0;
+    while (bh_ld_acquire(flag) == 0u) {
+        if (cap < 0 || ++spins > cap || bh_ld_acquire(abort_flag) != 0u) return false;
+    }
+    return true;
+}
+)CUDA";
+    const string n0 = "p.n" + to_string(sym.loop_id.at(&L));
+    auto emit_inputs = [&](Scope &scope, int ind) {
+        for (const Block &b : L._block_list) {
+            const InstrPtr &i = b.getInstr();
+            if (i == acc) break;
+            if (bh_opcode_is_system(i->opcode)) continue;
+            em.write_instr(*i, scope, ind);
+        }
+    };
+    auto declare_temps = [&](Scope &scope, int ind) {
+        for (const bh_base *b : em.sorted_temps(L)) {
+            if (sym.temps.count(b) && !scope.is_tmp(b)) {
+                scope.tmps.insert(b);
+                body << string(static_cast<size_t>(ind), ' ') << cuda_type(b->dtype()) << " t" << sym.base_index(b) << ";\n";
+            }
+        }
+    };
+    bool reread = false;
+    {
+        bool after = false;
+        for (const Block &b : L._block_list) {
+            const InstrPtr &i = b.getInstr();
+            if (i == acc) {
+                after = true;
+                continue;
+            }
+            if (!after || bh_opcode_is_system(i->opcode)) continue;
+            for (size_t o = 1; o < i->operand.size(); ++o) {
+                const bh_view &v = i->operand[o];
+                if (!v.isConstant() && v.base != acc->operand[0].base) reread = true;
+            }
+        }
+    }
+    // Chunk c's accumulate inputs, computed at coalesced positions and staged (as unit A).
+    body << "__device__ __forceinline__ void bh_stage_in(const P &p, bh_i64 c, " << T << " *stage) {\n";
+    body << pointer_locals(sym);
+    body << "    const bh_i64 cbase = c * " << kScanTile << ";\n";
+    {
+        Scope scope;
+        body << "#pragma unroll\n";
+        body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+        body << "        const int q = k * " << kThreads << " + (int)threadIdx.x;\n";
+        body << "        const bh_i64 i0 = cbase + q;\n";
+        body << "        " << T << " x = " << ident << ";\n";
+        body << "        if (i0 < " << n0 << ") {\n";
+        declare_temps(scope, 12);
+        emit_inputs(scope, 12);
+        body << "            x = " << em.name(acc->operand[1], scope) << ";\n";
+        body << "        }\n";
+        body << "        stage[q + (q >> 3)] = x;\n";
+        body << "    }\n";
+    }
+    body << "}\n";
+    // Chunk c's scanned values from the stage to memory, then the instructions after the
+    // accumulate (as unit C).
+    body << "__device__ __forceinline__ void bh_stage_out(const P &p, bh_i64 c, const " << T << " *stage) {\n";
+    body << pointer_locals(sym);
+    body << "    const bh_i64 cbase = c * " << kScanTile << ";\n";
+    {
+        Scope scope;
+        body << "#pragma unroll\n";
+        body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+        body << "        const int q = k * " << kThreads << " + (int)threadIdx.x;\n";
+        body << "        const bh_i64 i0 = cbase + q;\n";
+        body << "        if (i0 < " << n0 << ") {\n";
+        declare_temps(scope, 12);
+        if (reread) emit_inputs(scope, 12);
+        body << "            const " << T << " out = stage[q + (q >> 3)];\n";
+        if (sym.temps.count(acc->operand[0].base)) {
+            body << "            t" << sym.base_index(acc->operand[0].base) << " = out;\n";
+        } else {
+            body << "            " << em.array_ref(acc->operand[0]) << " = out;\n";
+            scope.repl[ViewKey(acc->operand[0])] = "out";
+        }
+        bool after = false;
+        for (const Block &b : L._block_list) {
+            const InstrPtr &i = b.getInstr();
+            if (i == acc) {
+                after = true;
+                continue;
+            }
+            if (after && !bh_opcode_is_system(i->opcode)) em.write_instr(*i, scope, 12);
+        }
+        body << "        }\n";
+        body << "    }\n";
+    }
+    body << "}\n";
+    // Thread t's fold of elements 8t..8t+7 (kept in xs) and the chunk's block scan (unit A/C).
+    body << "__device__ __forceinline__ " << T << " bh_chunk_fold(const P &p, bh_i64 c, const " << T << " *stage, " << T
+         << " (&xs)[" << kScanPerThread << "], " << T << " &total, " << T << " *sm) {\n";
+    body << "    const bh_i64 cbase = c * " << kScanTile << ";\n";
+    body << "    " << T << " s = " << ident << ";\n";
+    body << "#pragma unroll\n";
+    body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+    body << "        const int q = (int)threadIdx.x * " << kScanPerThread << " + k;\n";
+    body << "        xs[k] = stage[q + (q >> 3)];\n";
+    body << "        if (cbase + q < " << n0 << ") s = " << op("s", "xs[k]") << ";\n";
+    body << "    }\n";
+    body << "    return bh_block_scan(s, total, sm);\n";
+    body << "}\n";
+    // The carried values of chunk c into the stage (unit C).
+    body << "__device__ __forceinline__ void bh_chunk_rescan(const P &p, bh_i64 c, " << T << " *stage, const " << T
+         << " (&xs)[" << kScanPerThread << "], " << T << " e, " << T << " carry) {\n";
+    body << "    const bh_i64 cbase = c * " << kScanTile << ";\n";
+    body << "    " << T << " r = " << ident << ";\n";
+    body << "#pragma unroll\n";
+    body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+    body << "        const int j = (int)threadIdx.x * " << kScanPerThread << " + k;\n";
+    body << "        if (cbase + j < " << n0 << ") {\n";
+    body << "            r = " << op("r", "xs[k]") << ";\n";
+    body << "            const " << T << " inner = " << op("e", "r") << ";\n";
+    body << "            stage[j + (j >> 3)] = " << op("carry", "inner") << ";\n";
+    body << "        }\n";
+    body << "    }\n";
+    body << "}\n";
+    // Unit B's scan of the chunk totals of group g over entries 0..upto (entries after `upto` are
+    // left out: they do not change the prefixes at or before it). Returns the prefix at position
+    // `upto` (in every thread) and the group total in `gt`.
+    body << "__device__ __forceinline__ " << T << " bh_group_prefix(const P &p, const " << T << " *totals, bh_i64 g, int upto, "
+         << T << " &gt, " << T << " *sm, " << T << " *bcast) {\n";
+    body << "    const bh_i64 base = g * " << kScanTile << ";\n";
+    body << "    " << T << " v[" << kScanPerThread << "];\n";
+    body << "    " << T << " s = " << ident << ";\n";
+    body << "#pragma unroll\n";
+    body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+    body << "        const int jj = (int)threadIdx.x * " << kScanPerThread << " + k;\n";
+    body << "        v[k] = s;\n";
+    body << "        if (jj <= upto && base + jj < p.nchunks) { const " << T << " x = bh_ldcg(totals + base + jj); s = "
+         << op("s", "x") << "; }\n";
+    body << "    }\n";
+    body << "    const " << T << " e = bh_block_scan(s, gt, sm);\n";
+    body << "    if ((int)threadIdx.x == upto / " << kScanPerThread << ") {\n";
+    body << "#pragma unroll\n";
+    body << "        for (int k = 0; k < " << kScanPerThread << "; ++k)\n";
+    body << "            if (k == upto % " << kScanPerThread << ") *bcast = " << op("e", "v[k]") << ";\n";
+    body << "    }\n";
+    body << "    __syncthreads();\n";
+    body << "    const " << T << " r = *bcast;\n";
+    body << "    __syncthreads();\n";
+    body << "    return r;\n";
+    body << "}\n";
+    body << "__device__ void bh_work(const P &p, bh_i64 w) {}\n";  // never launched grouped
+    body << "__device__ __forceinline__ void bh_main(const P &p) {\n";
+    body << "    __shared__ " << T << " stage[" << kScanTile + kScanTile / kScanPerThread << "];\n";
+    body << "    __shared__ " << T << " sm[" << 2 * (kThreads / 32) + 1 << "];\n";
+    body << "    __shared__ " << T << " bcast;\n";
+    body << "    __shared__ bh_i64 ticket;\n";
+    body << "    __shared__ bool last;\n";
+    body << "    " << T << "* totals = (" << T << "*)p.scratch;\n";
+    body << "    " << T << "* carries = totals + p.nchunks;\n";
+    body << "    " << T << "* gcarry = carries + p.nchunks;\n";
+    body << "    unsigned* flags = p.counter;\n";
+    body << "    unsigned* gflags = flags + p.nchunks;\n";
+    body << "    unsigned* ctr = gflags + p.ngroups + 1;  // ticket, CTAs that left, abort\n";
+    body << "    " << T << " xs[" << kScanPerThread << "];\n";
+    body << R"CUDA(    for (;;) {
+        if (threadIdx.x == 0) ticket = bh_ld_acquire(ctr + 2) != 0u ? p.nchunks : (bh_i64)atomicAdd(ctr, 1u);
+        __syncthreads();
+        const bh_i64 c = ticket;
+        if (c >= p.nchunks) break;
+        bh_stage_in(p, c, stage);
+        __syncthreads();
+)CUDA";
+    body << "        " << T << " total;\n";
+    body << "        const " << T << " e = bh_chunk_fold(p, c, stage, xs, total, sm);\n";
+    body << R"CUDA(        if (threadIdx.x == 0) {
+            totals[c] = total;
+            bh_st_release(flags + c, 1u);
+        }
+        // Look back: the totals of the chunks before c in its group, then the carry into the group.
+        const bh_i64 g = c / )CUDA" << kScanTile << R"CUDA(;
+        const int q = (int)(c - g * )CUDA" << kScanTile << R"CUDA();
+        bool ok = true;
+        for (int k = 0; k < )CUDA" << kScanPerThread << R"CUDA( && ok; ++k) {
+            const int jj = (int)threadIdx.x * )CUDA" << kScanPerThread << R"CUDA( + k;
+            if (jj < q) ok = bh_await(flags + g * )CUDA" << kScanTile << R"CUDA( + jj, ctr + 2, p.spin_cap);
+        }
+        if (threadIdx.x == 0 && ok && g > 0) ok = bh_await(gflags + g, ctr + 2, p.spin_cap);
+        if (!__syncthreads_and(ok)) {
+            if (threadIdx.x == 0) atomicExch(ctr + 2, 1u);
+            break;
+        }
+)CUDA";
+    body << "        " << T << " gt;\n";
+    body << "        const " << T << " within = bh_group_prefix(p, totals, g, q, gt, sm, &bcast);\n";
+    body << "        const " << T << " grun = g > 0 ? bh_ldcg(gcarry + g) : " << ident << ";\n";
+    body << "        if (threadIdx.x == 0 && q == " << kScanTile - 1 << " && g + 1 < p.ngroups) {\n";
+    body << "            gcarry[g + 1] = " << op("grun", "gt") << ";\n";
+    body << "            bh_st_release(gflags + g + 1, 1u);\n";
+    body << "        }\n";
+    body << "        bh_chunk_rescan(p, c, stage, xs, e, " << op("grun", "within") << ");\n";
+    body << R"CUDA(        __syncthreads();
+        bh_stage_out(p, c, stage);
+        __syncthreads();  // stage reads before the next chunk's writes
+    }
+    // The CTA that leaves last: the fallback if any CTA gave up, then the reset for the next launch.
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ctr + 1, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    bh_acquire();
+    if (bh_ld_acquire(ctr + 2) != 0u) {
+        for (bh_i64 c = 0; c < p.nchunks; ++c) {
+            bh_stage_in(p, c, stage);
+            __syncthreads();
+)CUDA";
+    body << "            " << T << " total;\n";
+    body << "            bh_chunk_fold(p, c, stage, xs, total, sm);\n";
+    body << "            if (threadIdx.x == 0) totals[c] = total;\n";
+    body << "            __syncthreads();\n";
+    body << "        }\n";
+    body << "        __threadfence_block();\n";
+    body << "        __syncthreads();\n";
+    body << "        " << T << " run = " << ident << ";\n";
+    body << "        for (bh_i64 g = 0; g < p.ngroups; ++g) {\n";
+    // unit B's per-group step, for every chunk of the group at once
+    body << "            const bh_i64 base = g * " << kScanTile << ";\n";
+    body << "            " << T << " v[" << kScanPerThread << "];\n";
+    body << "            " << T << " s = " << ident << ";\n";
+    body << "            for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+    body << "                const bh_i64 j = base + threadIdx.x * " << kScanPerThread << " + k;\n";
+    body << "                v[k] = s;\n";
+    body << "                if (j < p.nchunks) { const " << T << " x = totals[j]; s = " << op("s", "x") << "; }\n";
+    body << "            }\n";
+    body << "            " << T << " gt;\n";
+    body << "            const " << T << " e = bh_block_scan(s, gt, sm);\n";
+    body << "            for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+    body << "                const bh_i64 j = base + threadIdx.x * " << kScanPerThread << " + k;\n";
+    body << "                if (j < p.nchunks) carries[j] = " << op("run", op("e", "v[k]")) << ";\n";
+    body << "            }\n";
+    body << "            run = " << op("run", "gt") << ";\n";
+    body << "            __syncthreads();\n";
+    body << "        }\n";
+    body << "        __threadfence_block();\n";
+    body << "        __syncthreads();\n";
+    body << "        for (bh_i64 c = 0; c < p.nchunks; ++c) {\n";
+    body << "            bh_stage_in(p, c, stage);\n";
+    body << "            __syncthreads();\n";
+    body << "            " << T << " total;\n";
+    body << "            const " << T << " e = bh_chunk_fold(p, c, stage, xs, total, sm);\n";
+    body << "            bh_chunk_rescan(p, c, stage, xs, e, carries[c]);\n";
+    body << "            __syncthreads();\n";
+    body << "            bh_stage_out(p, c, stage);\n";
+    body << "            __syncthreads();\n";
+    body << "        }\n";
+    body << "    }\n";
+    body << R"CUDA(    for (bh_i64 i = threadIdx.x; i < p.nchunks + p.ngroups + 1; i += blockDim.x) flags[i] = 0u;
+    if (threadIdx.x == 0) {
+        ctr[0] = 0u;
+        ctr[1] = 0u;
+        ctr[2] = 0u;
+    }
+}
+)CUDA";
+    body << kKernels;
+    u.fields = pl.fields;
+    u.scan_bytes = (2 * nchunks + ngroups + 1) * static_cast<int64_t>(bh_type_size(t));
+    u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
+    u.elements = n;
+    u.red_orders.emplace_back(acc->origin_id, "scan:" + to_string(kScanTile) + ":" + to_string(n));
+    finish_source(u, pl.decl.str(), body.str(), opt);
+    return u;
+}
+
 // OUTER_REDUCE: rank 0 sweeps (reductions) with a single parallel sub-nest and no instructions
 // directly at rank 0. Threads own points of the sub-nest and loop over the reduced axis in order.
 bool outer_reduce_applicable(const LoopB &L) {
@@ -3144,7 +3616,11 @@ vector<LaunchUnit> lower_kernel(const LoopB &kernel, const CodegenOptions &opt) 
             }
             if (ok) {
                 pending_id_loops.clear();
-                for (LaunchUnit &su : lower_scan1d(L, scan_acc, opt)) units.push_back(std::move(su));
+                if (opt.scan_single_pass && !opt.bounds_check) {
+                    units.push_back(lower_scan1d_single(L, scan_acc, opt));
+                } else {
+                    for (LaunchUnit &su : lower_scan1d(L, scan_acc, opt)) units.push_back(std::move(su));
+                }
                 continue;
             }
         }

@@ -110,6 +110,8 @@ struct LaunchUnit {
     int64_t scan_bytes = 0;     // SCAN1D: its chunk totals and carries and group totals and carries
     int64_t scan_offset = 0;    // SCAN1D: offset of scan_bytes in the scan arena (set by the plan)
     bool scan_gate = false;     // SCAN1D carry unit: one completion counter
+    bool single_pass = false;   // SCAN1D in one pass (lower_scan1d_single): chunks = chunk count
+    bool no_batch = false;      // always launched alone (its CTAs wait on one another's results)
     // The parameter members and the device code (without the kernel wrappers) of the source;
     // body_core is empty for sources with wrappers of their own.
     std::string params_decl, body_core;
@@ -140,6 +142,9 @@ struct CodegenOptions {
     bool preload_heavy = true;  // preload the inputs of heavy (arithmetic-bound) element bodies too
     int interleave = 1;         // GRID_REDUCE: elements of a heavy body written side by side (1 or 2)
     bool tile2d = true;         // TILE2D for maps over transposed views (else FLAT)
+    bool vector_access = true;  // FLAT: 4 consecutive elements per thread, moved as 128-bit words
+    bool scan_single_pass = true; // SCAN1D as one pass with look-back (else three units)
+    int64_t scan_spin_cap = int64_t{1} << 22; // polls per look-back wait (negative: give up at once)
 };
 
 // Lower one kernel (as produced by jitk::get_kernel_list) into launch units executed in order.

@@ -97,6 +97,9 @@ extern "C" const char *bh_ve_cuda_dry_run(bhb_ir *handle, int compile, const cha
         // The engine's codegen keys, from the environment as the config would give them.
         if (const char *v = getenv("BH_CUDA_INTERLEAVE")) opt.interleave = atoi(v);
         if (const char *v = getenv("BH_CUDA_PRELOAD_HEAVY")) opt.preload_heavy = string(v) == "true" || string(v) == "1";
+        if (const char *v = getenv("BH_CUDA_TILE2D")) opt.tile2d = string(v) == "true" || string(v) == "1";
+        if (const char *v = getenv("BH_CUDA_VECTOR_ACCESS")) opt.vector_access = string(v) == "true" || string(v) == "1";
+        if (const char *v = getenv("BH_CUDA_SCAN_SINGLE_PASS")) opt.scan_single_pass = string(v) == "true" || string(v) == "1";
         vector<vector<cuda::LaunchUnit>> lowered(kernels.size());
         for (size_t k = 0; k < kernels.size(); ++k)
             if (!kernels[k].isSystemOnly()) lowered[k] = cuda::lower_kernel(kernels[k], opt);

@@ -111,6 +111,9 @@ EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
     cg_opt.preload_heavy = cfg.defaultGet<bool>("preload_heavy", true);
     cg_opt.interleave = cfg.defaultGet<int>("interleave", 1);
     cg_opt.tile2d = cfg.defaultGet<bool>("tile2d", true);
+    cg_opt.vector_access = cfg.defaultGet<bool>("vector_access", true);
+    cg_opt.scan_single_pass = cfg.defaultGet<bool>("scan_single_pass", true);
+    cg_opt.scan_spin_cap = cfg.defaultGet<int64_t>("scan_spin_cap", int64_t{1} << 22);
     // The GPU reduces over the outermost axis natively, so sweeps may fuse with maps at rank 0.
     fusion_config = jitk::FusionConfig(cfg, false);
     cache_dir = cfg.defaultGet<string>("cache_dir", "");
@@ -1337,8 +1340,8 @@ void EngineCUDA::run_plan(const FlushPlan &plan, const vector<bh_base *> &bases,
         }
         for (const Compiled *c : order) {
             const auto &g = groups[c];
-            if (g.size() == 1) {
-                launch_plain(*g[0], bases, instrs);
+            if (g.size() == 1 || g[0]->unit.no_batch) {
+                for (const PlanUnit *pu : g) launch_plain(*pu, bases, instrs);
             } else {
                 launch_batched(g, bases, instrs);
             }

@@ -127,7 +127,14 @@ bool EngineCUDA::build_graph(Replay &r) {
                 if (!groups.count(pu->compiled)) order.push_back(pu->compiled);
                 groups[pu->compiled].push_back(pu);
             }
-            for (const Compiled *c : order) launches.push_back(groups[c]);
+            for (const Compiled *c : order) {
+                const auto &g = groups[c];
+                if (g.size() > 1 && g[0]->unit.no_batch) {
+                    for (const PlanUnit *pu : g) launches.push_back({pu});
+                } else {
+                    launches.push_back(g);
+                }
+            }
         }
     }
     // Size the arenas once, then pack every launch.
