@@ -2603,28 +2603,100 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
     const vector<bh_view> pre = heavy && !opt.preload_heavy ? vector<bh_view>{} : preloadable_views(L, L, sym);
     map<ViewKey, string> acc_k;
     for (size_t k = 0; k < reds.size(); ++k) acc_k[ViewKey(reds[k]->operand[0])] = accs[k] + "[k]";
+    // Element j (0..7) of a thread's part of tile k: 4 consecutive elements at 4t and 4 at 1024 + 4t
+    // of the tile, so a view with unit stride is two 4-element words per thread; the thread folds
+    // them in that order, on every path.
+    const string elem_index = "(tile0 + k) * " + to_string(kReduceTile) + " + (j >> 2) * " + to_string(kReduceTile / 2) +
+                              " + threadIdx.x * 4 + (j & 3)";
+    // Views moved as words on full tiles: read-only inputs and arrays written by the element code
+    // with unit stride (see emit_flat_vector).
+    const bool vectorized = opt.vector_access && !opt.bounds_check && !(heavy && opt.interleave == 2);
+    vector<bool> vec_pre(pre.size());
+    for (size_t v = 0; v < pre.size(); ++v) vec_pre[v] = vectorized && unit_stride_view(pre[v], 0, sym);
+    vector<bh_view> wouts;
+    if (vectorized) {
+        map<const bh_base *, set<ViewKey>> touched;
+        for (const InstrPtr &i : jitk::all_instr(L))
+            for (const bh_view &v : i->operand)
+                if (!v.isConstant()) touched[v.base].insert(ViewKey(v));
+        set<ViewKey> seen;
+        for (const InstrPtr &i : jitk::all_instr(L)) {
+            const bh_opcode op = i->opcode;
+            if (bh_opcode_is_system(op) || bh_opcode_is_sweep(op) || op == BH_GATHER || op == BH_SCATTER ||
+                op == BH_COND_SCATTER || i->operand.empty())
+                continue;
+            const bh_view &v = i->operand[0];
+            if (!unit_stride_view(v, 0, sym) || sym.always_array.count(v.base) || touched[v.base].size() != 1) continue;
+            if (acc_k.count(ViewKey(v))) continue;
+            if (seen.insert(ViewKey(v)).second) wouts.push_back(v);
+        }
+    }
     for (int path = 0; path < 2; ++path) {
         body << (path == 0 ? "    if ((tile0 + " + to_string(K) + ") * " + to_string(kReduceTile) + " <= " + n0 + ") {\n"
                            : "    } else {\n");
         Scope scope;
         Emitter eb(sym, body, opt);
         eb.external_acc = acc_k;
+        if (path == 0 && vectorized) {
+            // Word alignment of every word-moved view (the same for every group of 4 elements).
+            body << "        bool vec = true;\n";
+            body << "        {\n";
+            body << "            const bh_i64 i0 = tile0 * " << kReduceTile << " + threadIdx.x * 4;\n";
+            for (size_t v = 0; v < pre.size(); ++v) {
+                if (!vec_pre[v]) continue;
+                const int bytes = min(16, 4 * static_cast<int>(bh_type_size(pre[v].base->dtype())));
+                body << "            vec = vec && (((unsigned long long)&" << eb.array_ref(pre[v]) << ") & " << bytes - 1
+                     << "ull) == 0;\n";
+            }
+            for (const bh_view &v : wouts) {
+                const int bytes = min(16, 4 * static_cast<int>(bh_type_size(v.base->dtype())));
+                body << "            vec = vec && (((unsigned long long)&" << eb.array_ref(v) << ") & " << bytes - 1
+                     << "ull) == 0;\n";
+            }
+            body << "        }\n";
+        }
         if (path == 0 && !pre.empty()) {
             for (size_t v = 0; v < pre.size(); ++v)
                 body << "        " << cuda_type(pre[v].base->dtype()) << " pl" << v << "[" << K * kReduceV << "];\n";
             body << "#pragma unroll\n";
             body << "        for (int k = 0; k < " << K << "; ++k) {\n";
-            body << "#pragma unroll\n";
-            body << "            for (int j = 0; j < " << kReduceV << "; ++j) {\n";
-            body << "                const bh_i64 i0 = (tile0 + k) * " << kReduceTile << " + j * " << kThreads
-                 << " + threadIdx.x;\n";
-            for (size_t v = 0; v < pre.size(); ++v)
-                body << "                pl" << v << "[k * " << kReduceV << " + j] = " << eb.array_ref(pre[v]) << ";\n";
-            body << "            }\n";
+            if (vectorized) {
+                // Two words of 4 elements per view and tile: elements 4t..4t+3 and 1024+4t..1024+4t+3.
+                body << "#pragma unroll\n";
+                body << "            for (int g = 0; g < 2; ++g) {\n";
+                body << "                const bh_i64 i0 = (tile0 + k) * " << kReduceTile << " + g * " << kReduceTile / 2
+                     << " + threadIdx.x * 4;\n";
+                for (size_t v = 0; v < pre.size(); ++v) {
+                    const string dst = "&pl" + to_string(v) + "[k * " + to_string(kReduceV) + " + g * 4]";
+                    const int bytes = 4 * static_cast<int>(bh_type_size(pre[v].base->dtype()));
+                    if (vec_pre[v]) {
+                        body << "                if (vec) { " << word_copy(dst, "&" + eb.array_ref(pre[v]), bytes) << "} else {\n";
+                    } else {
+                        body << "                {\n";
+                    }
+                    body << "#pragma unroll\n";
+                    body << "                    for (int e = 0; e < 4; ++e) {\n";
+                    body << "                        const bh_i64 i0e = i0 + e;\n";
+                    body << "                        pl" << v << "[k * " << kReduceV << " + g * 4 + e] = "
+                         << regex_replace(eb.array_ref(pre[v]), regex("\\bi0\\b"), "i0e") << ";\n";
+                    body << "                    }\n";
+                    body << "                }\n";
+                }
+                body << "            }\n";
+            } else {
+                body << "#pragma unroll\n";
+                body << "            for (int j = 0; j < " << kReduceV << "; ++j) {\n";
+                body << "                const bh_i64 i0 = " << elem_index << ";\n";
+                for (size_t v = 0; v < pre.size(); ++v)
+                    body << "                pl" << v << "[k * " << kReduceV << " + j] = " << eb.array_ref(pre[v]) << ";\n";
+                body << "            }\n";
+            }
             body << "        }\n";
             for (size_t v = 0; v < pre.size(); ++v)
                 scope.repl[ViewKey(pre[v])] = "pl" + to_string(v) + "[k * " + to_string(kReduceV) + " + j]";
         }
+        if (path == 0 && vectorized)
+            for (size_t m = 0; m < wouts.size(); ++m) scope.repl[ViewKey(wouts[m])] = "so" + to_string(m) + "[j]";
         // k always runs to the constant K (unrolled), so the accumulator slots stay registers.
         body << "#pragma unroll\n";
         body << "        for (int k = 0; k < " << K << "; ++k) {\n";
@@ -2634,9 +2706,8 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
             // still fold j before j + 1): independent chains side by side for the scheduler.
             body << "#pragma unroll\n";
             body << "            for (int j = 0; j < " << kReduceV << "; j += 2) {\n";
-            body << "                const bh_i64 i0 = (tile0 + k) * " << kReduceTile << " + j * " << kThreads
-                 << " + threadIdx.x;\n";
-            body << "                const bh_i64 i0_1 = i0 + " << kThreads << ";\n";
+            body << "                const bh_i64 i0 = " << elem_index << ";\n";
+            body << "                const bh_i64 i0_1 = " << regex_replace(elem_index, regex("\\bj\\b"), "(j + 1)") << ";\n";
             stringstream one;
             Emitter e1(sym, one, opt);
             e1.external_acc = acc_k;
@@ -2646,13 +2717,35 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
             body << "        }\n";
             continue;
         }
+        if (path == 0 && vectorized)
+            for (size_t m = 0; m < wouts.size(); ++m)
+                body << "            " << cuda_type(wouts[m].base->dtype()) << " so" << m << "[" << kReduceV << "];\n";
         if (path == 0) body << "#pragma unroll\n";
         body << "            for (int j = 0; j < " << kReduceV << "; ++j) {\n";
-        body << "                const bh_i64 i0 = (tile0 + k) * " << kReduceTile << " + j * " << kThreads
-             << " + threadIdx.x;\n";
+        body << "                const bh_i64 i0 = " << elem_index << ";\n";
         if (path == 1) body << "                if (i0 >= " << n0 << ") break;\n";
         eb.write_body(L, scope, 16);
         body << "            }\n";
+        if (path == 0 && vectorized) {
+            // The written arrays' words: 4 elements at 4t and 4 at 1024 + 4t.
+            body << "#pragma unroll\n";
+            body << "            for (int g = 0; g < 2; ++g) {\n";
+            body << "                const bh_i64 i0 = (tile0 + k) * " << kReduceTile << " + g * " << kReduceTile / 2
+                 << " + threadIdx.x * 4;\n";
+            for (size_t m = 0; m < wouts.size(); ++m) {
+                const int bytes = 4 * static_cast<int>(bh_type_size(wouts[m].base->dtype()));
+                body << "                if (vec) { " << word_copy("&" + eb.array_ref(wouts[m]), "&so" + to_string(m) + "[g * 4]", bytes)
+                     << "} else {\n";
+                body << "#pragma unroll\n";
+                body << "                    for (int e = 0; e < 4; ++e) {\n";
+                body << "                        const bh_i64 i0e = i0 + e;\n";
+                body << "                        " << regex_replace(eb.array_ref(wouts[m]), regex("\\bi0\\b"), "i0e")
+                     << " = so" << m << "[g * 4 + e];\n";
+                body << "                    }\n";
+                body << "                }\n";
+            }
+            body << "            }\n";
+        }
         body << "        }\n";
     }
     body << "    }\n";

@@ -9,7 +9,8 @@
 //
 // Order of operations (the same as the GRID_REDUCE schedule, so the result equals the engine's
 // ADD_REDUCE of the same array): tiles of 256 threads x 8 elements, thread x adds elements
-// tile*2048 + j*256 + x for j = 0..7 in order, a warp-shuffle butterfly (xor 16, 8, 4, 2, 1) and
+// tile*2048 + (j/4)*1024 + 4x + j%4 for j = 0..7 in order (two 16-byte words), a warp-shuffle
+// butterfly (xor 16, 8, 4, 2, 1) and
 // the same butterfly over the 8 warp sums gives the tile partial; the CTA that completes the last
 // tile folds the partials (thread t adds tiles t, t+256, ... in order) with the same CTA tree.
 //
@@ -82,10 +83,11 @@ __global__ void __launch_bounds__(kThreads) noalloc_sum_kernel(const double *__r
         double acc = 0.0;
         if ((tile + 1) * kTile <= n) {
 #pragma unroll
-            for (int j = 0; j < kPerThread; ++j) acc = acc + in[tile * kTile + j * kThreads + threadIdx.x];
+            for (int j = 0; j < kPerThread; ++j)
+                acc = acc + in[tile * kTile + (j >> 2) * (kTile / 2) + threadIdx.x * 4 + (j & 3)];
         } else {
             for (int j = 0; j < kPerThread; ++j) {
-                const int64_t i = tile * kTile + j * kThreads + threadIdx.x;
+                const int64_t i = tile * kTile + (j >> 2) * (kTile / 2) + threadIdx.x * 4 + (j & 3);
                 if (i >= n) break;
                 acc = acc + in[i];
             }

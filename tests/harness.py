@@ -48,20 +48,21 @@ def compare(a_results, b_results, tol=None, what=""):
 def grid_reduce_sum(x: np.ndarray) -> np.ndarray:
     """Exact model of the summation order of the engine's GRID_REDUCE schedule for an ADD_REDUCE
     of a contiguous 1-D array: tiles of 256 threads x 8 elements (thread t adds elements
-    t, t+256, ..., t+1792 of its tile in order, starting from 0), a halving tree over the 32 lanes
-    of each warp and over the 8 warp sums (padded with 0), then the same per-thread fold and trees
-    over the tile partials (thread t adds partials t, t+256, ...). Vectorised NumPy in the array's
-    own dtype, so the result is bit-exact."""
+    4t, 4t+1, 4t+2, 4t+3, 1024+4t, ..., 1024+4t+3 of its tile in order, starting from 0 -- two
+    128-bit words' worth), a halving tree over the 32 lanes of each warp and over the 8 warp sums
+    (padded with 0), then the same per-thread fold and trees over the tile partials (thread t adds
+    partials t, t+256, ...). Vectorised NumPy in the array's own dtype, so the result is
+    bit-exact."""
     dt = x.dtype
     zero = dt.type(0)
     n = x.size
     ntiles = -(-n // 2048)
     pad = np.zeros(ntiles * 2048, dtype=dt)
     pad[:n] = x
-    t = pad.reshape(ntiles, 8, 256)
+    t = pad.reshape(ntiles, 2, 256, 4)
     acc = np.full((ntiles, 256), zero, dtype=dt)
     for j in range(8):
-        acc = acc + t[:, j, :]
+        acc = acc + t[:, j >> 2, :, j & 3]
 
     def cta_tree(a):  # a: (rows, 256) -> (rows,)
         w = a.reshape(a.shape[0], 8, 32)

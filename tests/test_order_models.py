@@ -109,3 +109,52 @@ def test_scan1d_model_within_its_depth_bound(n):
     x = np.random.default_rng(n).standard_normal(n).astype(np.float32)
     assert_cumsum_within_bound(scan1d_cumsum(x), x, scan1d_depth(n), U32, "model")
     assert_cumsum_within_bound(np.cumsum(x), x, np.arange(1, n + 1), U32, "sequential")
+
+
+def _scalar_block_tree(vals, dt):
+    """One CTA's tree written out per thread: xor butterfly in each warp (lane l adds lane l^m),
+    warp sums in shared memory, the same butterfly over them in warp 0 (lanes >= 8 give 0)."""
+    v = [dt.type(x) for x in vals]
+    for m in (16, 8, 4, 2, 1):
+        v = [dt.type(v[i] + v[(i & ~31) | ((i & 31) ^ m)]) for i in range(256)]
+    w = [v[32 * k] for k in range(8)] + [dt.type(0)] * 24
+    for m in (16, 8, 4, 2, 1):
+        w = [dt.type(w[i] + w[i ^ m]) for i in range(32)]
+    return w[0]
+
+
+@pytest.mark.parametrize("n", [1, 2047, 2049, 5000, 600_001])
+def test_grid_reduce_model_matches_a_scalar_transcription(n):
+    """The GRID_REDUCE order model against the kernel's steps written out thread by thread:
+    thread t of a tile adds its elements 4t..4t+3 and 1024+4t..1024+4t+3 in order (the two
+    128-bit words it loads), then the CTA tree; the tile partials are folded and reduced the same
+    way by one CTA. Bit for bit."""
+    dt = np.dtype(np.float32)
+    x = np.random.default_rng(n).standard_normal(n).astype(dt)
+    ntiles = -(-n // 2048)
+    parts = []
+    for tile in range(ntiles if n < 100_000 else 0):
+        sums = []
+        for t in range(256):
+            acc = dt.type(0)
+            for j in range(8):
+                i = tile * 2048 + (j >> 2) * 1024 + 4 * t + (j & 3)
+                if i >= n:
+                    break
+                acc = dt.type(acc + x[i])
+            sums.append(acc)
+        parts.append(_scalar_block_tree(sums, dt))
+    if n >= 100_000:  # the thread folds vectorised, the trees still written out
+        pad = np.zeros(ntiles * 2048, dt)
+        pad[:n] = x
+        t4 = pad.reshape(ntiles, 2, 256, 4)
+        acc = np.zeros((ntiles, 256), dt)
+        for j in range(8):
+            acc = acc + t4[:, j >> 2, :, j & 3]
+        parts = [_scalar_block_tree(acc[k], dt) for k in range(ntiles)]
+    fold = [dt.type(0)] * 256
+    for t in range(256):
+        for k in range(t, ntiles, 256):
+            fold[t] = dt.type(fold[t] + parts[k])
+    want = _scalar_block_tree(fold, dt)
+    assert grid_reduce_sum(x).tobytes() == np.asarray(want, dtype=dt).tobytes()
