@@ -1556,10 +1556,14 @@ constexpr int kTileCols = 64;
 constexpr int kTileStages = 4;
 constexpr int kTileBoxBytes = kTileCols * 128;
 
-// The transposed views of `inner` that TILE2D stages: read-only (their base is not written by the
-// kernel), 2-D, stride 1 along rank 0 and > 1 along rank 1, 4- or 8-byte elements (all the same
-// size), at most two. Empty when the loop does not qualify.
-vector<bh_view> tile2d_views(const LoopB &L, const LoopB &inner, const Symbols &sym, const CodegenOptions &opt) {
+// The views of `inner` that TILE2D stages: first the transposed ones -- read-only (their base is
+// not written by the kernel), 2-D, stride 1 along rank 0 and > 1 along rank 1 -- at most two; then
+// read-only row-wise ones (stride 1 along rank 1, > 1 along rank 0), up to three views in all. All
+// of 4- or 8-byte elements of one size. `transposed[k]` tells the kinds apart. Empty when the loop
+// has no transposed view or does not qualify.
+vector<bh_view> tile2d_views(const LoopB &L, const LoopB &inner, const Symbols &sym, const CodegenOptions &opt,
+                             vector<bool> &transposed) {
+    transposed.clear();
     if (!opt.tile2d || opt.bounds_check || !inner.isInnermost() || !L._sweeps.empty() || !inner._sweeps.empty()) return {};
     if (L.size < 32 || inner.size < kTileCols) return {};
     set<const bh_base *> written;
@@ -1567,18 +1571,37 @@ vector<bh_view> tile2d_views(const LoopB &L, const LoopB &inner, const Symbols &
         if (bh_opcode_is_sweep(i->opcode)) return {};
         if (!i->operand.empty() && !i->operand[0].isConstant()) written.insert(i->operand[0].base);
     }
+    auto usable = [&](const bh_view &v) {
+        const int es = bh_type_size(v.base->dtype());
+        return v.ndim == 2 && !written.count(v.base) && !bh_type_is_complex(v.base->dtype()) && (es == 4 || es == 8) &&
+               v.base->dtype() != bh_type::R123;
+    };
+    const vector<bh_view> cand = preloadable_views(inner, L, sym);
     vector<bh_view> ret;
     set<ViewKey> seen;
     int esize = 0;
-    for (const bh_view &v : preloadable_views(inner, L, sym)) {
-        if (v.ndim != 2 || v.stride[0] != 1 || v.stride[1] <= 1 || written.count(v.base)) continue;
+    for (const bh_view &v : cand) {
+        if (!usable(v) || v.stride[0] != 1 || v.stride[1] <= 1) continue;
         const int es = bh_type_size(v.base->dtype());
-        if (bh_type_is_complex(v.base->dtype()) || (es != 4 && es != 8) || v.base->dtype() == bh_type::R123) continue;
         if (esize != 0 && es != esize) return {};
         esize = es;
-        if (seen.insert(ViewKey(v)).second) ret.push_back(v);
+        if (seen.insert(ViewKey(v)).second) {
+            ret.push_back(v);
+            transposed.push_back(true);
+        }
     }
-    if (ret.size() > 2) return {};
+    if (ret.empty() || ret.size() > 2) {
+        transposed.clear();
+        return {};
+    }
+    for (const bh_view &v : cand) {
+        if (ret.size() >= 3) break;
+        if (!usable(v) || v.stride[1] != 1 || v.stride[0] <= 1 || bh_type_size(v.base->dtype()) != esize) continue;
+        if (seen.insert(ViewKey(v)).second) {
+            ret.push_back(v);
+            transposed.push_back(false);
+        }
+    }
     return ret;
 }
 
@@ -1589,8 +1612,10 @@ bool lower_tile2d(const LoopB &loop, const CodegenOptions &opt, LaunchUnit &u) {
     const vector<const LoopB *> chain = jitk::get_first_loop_blocks(L);
     if (chain.size() < 2) return false;
     const LoopB &inner = *chain[1];
-    const vector<bh_view> tv = tile2d_views(L, inner, sym, opt);
+    vector<bool> tpose;
+    const vector<bh_view> tv = tile2d_views(L, inner, sym, opt, tpose);
     if (tv.empty()) return false;
+    const int stages = tv.size() <= 2 ? kTileStages : kTileStages - 1;
     const int esize = bh_type_size(tv[0].base->dtype());
     const int TR = 128 / esize, RPT = TR / 4;  // rows per tile, rows per thread
     u = LaunchUnit();
@@ -1601,13 +1626,17 @@ bool lower_tile2d(const LoopB &loop, const CodegenOptions &opt, LaunchUnit &u) {
     const int64_t tiles_c = (u.cols + kTileCols - 1) / kTileCols;
     ParamLayout pl;
     for (size_t k = 0; k < tv.size(); ++k) {
+        // A transposed view's tile is TR elements along its base rows x 64 rows (128-byte swizzle);
+        // a row-wise view's tile is 64 elements along its base rows x TR rows (no swizzle).
         ParamField f{ParamField::TMAP};
         f.base = tv[k].base;
         f.i64 = tv[k].start;
-        f.tm_ld = tv[k].stride[1];
-        f.tm_box = TR;
-        f.tm_rows = u.rows;
-        f.tm_cols = u.cols;
+        f.tm_ld = tpose[k] ? tv[k].stride[1] : tv[k].stride[0];
+        f.tm_box_x = tpose[k] ? TR : kTileCols;
+        f.tm_box_y = tpose[k] ? kTileCols : TR;
+        f.tm_xspan = tpose[k] ? u.rows : u.cols;
+        f.tm_yspan = tpose[k] ? u.cols : u.rows;
+        f.tm_swizzle = tpose[k];
         pl.add_tmap(f, "tm" + to_string(k));
     }
     add_common_fields(sym, pl, opt);
@@ -1615,7 +1644,7 @@ bool lower_tile2d(const LoopB &loop, const CodegenOptions &opt, LaunchUnit &u) {
     pl.add(work_field(u.work_items()), "bh_i64", "work");
     for (size_t k = 0; k < tv.size(); ++k) {
         // Tensor coordinates of the view's element (0, 0): column and row of its base array.
-        const int64_t ld = tv[k].stride[1];
+        const int64_t ld = tpose[k] ? tv[k].stride[1] : tv[k].stride[0];
         pl.add(work_field(tv[k].start >= 0 ? tv[k].start % ld : 0), "bh_i64", "tx" + to_string(k));
         pl.add(work_field(tv[k].start >= 0 ? tv[k].start / ld : 0), "bh_i64", "ty" + to_string(k));
     }
@@ -1629,7 +1658,7 @@ bool lower_tile2d(const LoopB &loop, const CodegenOptions &opt, LaunchUnit &u) {
     const string T = cuda_type(tv[0].base->dtype());
     const string rows = "p.n" + to_string(sym.loop_id.at(&L)), cols = "p.n" + to_string(sym.loop_id.at(&inner));
     stringstream body;
-    body << "// bh_dynamic_shared_bytes: " << kTileStages * static_cast<int>(tv.size()) * kTileBoxBytes + 1024 << "\n";
+    body << "// bh_dynamic_shared_bytes: " << stages * static_cast<int>(tv.size()) * kTileBoxBytes + 1024 << "\n";
     body << "template <bool STAGED> __device__ __forceinline__ void bh_tile(const P &p, bh_i64 w, const unsigned char *stage) {\n";
     body << pointer_locals(sym);
     body << "    const bh_i64 tr = w / p.tiles_c;\n";
@@ -1639,6 +1668,12 @@ bool lower_tile2d(const LoopB &loop, const CodegenOptions &opt, LaunchUnit &u) {
     body << "    const bh_i64 rbase = tr * " << TR << " + rq * " << RPT << ";\n";
     for (size_t k = 0; k < tv.size(); ++k) {
         body << "    " << T << " tv" << k << "[" << RPT << "];\n";
+        if (!tpose[k]) {
+            // row-wise: row r of the tile at r * 64 elements, read in the element loop
+            body << "    const " << T << " *tr" << k << " = (const " << T << " *)(stage + " << k * kTileBoxBytes
+                 << ") + (rq * " << RPT << ") * 64 + c;\n";
+            continue;
+        }
         body << "    if (STAGED) {\n";
         body << "        const unsigned char *row = stage + " << k * kTileBoxBytes << " + c * 128;\n";
         body << "        const uint4 q0 = *(const uint4 *)(row + (((2 * rq) ^ (c & 7)) << 4));\n";
@@ -1657,8 +1692,13 @@ bool lower_tile2d(const LoopB &loop, const CodegenOptions &opt, LaunchUnit &u) {
         body << "        for (int e = 0; e < " << RPT << "; ++e) {\n";
         body << "            const bh_i64 i0 = rbase + e;\n";
         if (path == 1) body << "            if (i0 >= " << rows << " || i1 >= " << cols << ") break;\n";
-        for (size_t k = 0; k < tv.size(); ++k)
-            body << "            if (!STAGED) tv" << k << "[e] = " << eb.array_ref(tv[k]) << ";\n";
+        for (size_t k = 0; k < tv.size(); ++k) {
+            if (tpose[k]) {
+                body << "            if (!STAGED) tv" << k << "[e] = " << eb.array_ref(tv[k]) << ";\n";
+            } else {
+                body << "            tv" << k << "[e] = STAGED ? tr" << k << "[e * 64] : " << eb.array_ref(tv[k]) << ";\n";
+            }
+        }
         declare_chain_temps(eb, sym, scope, chain, 1, body, 12);
         eb.write_body(inner, scope, 12);
         body << "        }\n";
@@ -1670,9 +1710,15 @@ bool lower_tile2d(const LoopB &loop, const CodegenOptions &opt, LaunchUnit &u) {
     body << "    const bh_i64 tr = w / p.tiles_c;\n";
     body << "    const bh_i64 tc = w - tr * p.tiles_c;\n";
     body << "    bh_mbar_expect_tx(bar, " << tv.size() * kTileBoxBytes << "u);\n";
-    for (size_t k = 0; k < tv.size(); ++k)
-        body << "    bh_tma_2d(stage + " << k * kTileBoxBytes << ", &p.tm" << k << ", (int)(p.tx" << k << " + tr * " << TR
-             << "), (int)(p.ty" << k << " + tc * 64), bar);\n";
+    for (size_t k = 0; k < tv.size(); ++k) {
+        if (tpose[k]) {
+            body << "    bh_tma_2d(stage + " << k * kTileBoxBytes << ", &p.tm" << k << ", (int)(p.tx" << k << " + tr * " << TR
+                 << "), (int)(p.ty" << k << " + tc * 64), bar);\n";
+        } else {
+            body << "    bh_tma_2d(stage + " << k * kTileBoxBytes << ", &p.tm" << k << ", (int)(p.tx" << k
+                 << " + tc * 64), (int)(p.ty" << k << " + tr * " << TR << "), bar);\n";
+        }
+    }
     body << "}\n";
     const int stage_bytes = static_cast<int>(tv.size()) * kTileBoxBytes;
     body << R"CUDA(__device__ __forceinline__ void bh_main(const P &p) {
@@ -1683,36 +1729,36 @@ bool lower_tile2d(const LoopB &loop, const CodegenOptions &opt, LaunchUnit &u) {
     extern __shared__ unsigned char bh_dyn[];
     // The 128-byte swizzle repeats every 1024 bytes: the ring starts on a 1024-byte boundary.
     unsigned char *ring = bh_dyn + ((1024u - (bh_saddr(bh_dyn) & 1023u)) & 1023u);
-    __shared__ alignas(8) unsigned long long bar[)CUDA" << kTileStages << R"CUDA(];
+    __shared__ alignas(8) unsigned long long bar[)CUDA" << stages << R"CUDA(];
     __shared__ int fail;
     const bh_i64 first = blockIdx.x, step = gridDim.x;
     const int mine = first < p.work ? (int)((p.work - 1 - first) / step + 1) : 0;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < )CUDA" << kTileStages << R"CUDA(; ++s) bh_mbar_init(&bar[s], 1u);
+        for (int s = 0; s < )CUDA" << stages << R"CUDA(; ++s) bh_mbar_init(&bar[s], 1u);
         bh_mbar_fence_init();
         fail = 0;
     }
     __syncthreads();
     if (threadIdx.x == 0)
-        for (int it = 0; it < )CUDA" << kTileStages << R"CUDA( && it < mine; ++it)
+        for (int it = 0; it < )CUDA" << stages << R"CUDA( && it < mine; ++it)
             bh_tile_issue(p, first + it * step, ring + it * )CUDA" << stage_bytes << R"CUDA(, &bar[it]);
     int it = 0;
     for (; it < mine; ++it) {
-        const int s = it % )CUDA" << kTileStages << R"CUDA(;
-        if (!bh_mbar_wait(&bar[s], (unsigned)((it / )CUDA" << kTileStages << R"CUDA() & 1))) fail = 1;
+        const int s = it % )CUDA" << stages << R"CUDA(;
+        if (!bh_mbar_wait(&bar[s], (unsigned)((it / )CUDA" << stages << R"CUDA() & 1))) fail = 1;
         __syncthreads();
         if (fail) break;
         bh_tile<true>(p, first + it * step, ring + s * )CUDA" << stage_bytes << R"CUDA();
         __syncthreads();  // every thread is done with the stage
-        if (threadIdx.x == 0 && it + )CUDA" << kTileStages << R"CUDA( < mine)
-            bh_tile_issue(p, first + (it + )CUDA" << kTileStages << R"CUDA() * step, ring + s * )CUDA" << stage_bytes << R"CUDA(, &bar[s]);
+        if (threadIdx.x == 0 && it + )CUDA" << stages << R"CUDA( < mine)
+            bh_tile_issue(p, first + (it + )CUDA" << stages << R"CUDA() * step, ring + s * )CUDA" << stage_bytes << R"CUDA(, &bar[s]);
     }
     if (fail && threadIdx.x == 0) {
         // A tile load never completed: record it, and let the copies already issued into the
         // ring land (bounded) before the CTA leaves.
         atomicCAS(p.err, 0ull, 0xC000000000000000ull | (unsigned long long)blockIdx.x);
-        for (int j = it; j < mine && j < it + )CUDA" << kTileStages << R"CUDA(; ++j)
-            bh_mbar_wait(&bar[j % )CUDA" << kTileStages << R"CUDA(], (unsigned)((j / )CUDA" << kTileStages << R"CUDA() & 1));
+        for (int j = it; j < mine && j < it + )CUDA" << stages << R"CUDA(; ++j)
+            bh_mbar_wait(&bar[j % )CUDA" << stages << R"CUDA(], (unsigned)((j / )CUDA" << stages << R"CUDA() & 1));
     }
 }
 )CUDA";

@@ -34,9 +34,10 @@
 //   TILE2D        a 2-D map that reads arrays through transposed views (unit stride along the outer
 //                 rank): tiles of (128 bytes / element) rows x 64 columns; each transposed view's
 //                 tile is one box of its base array, loaded by TMA (cp.async.bulk.tensor.2d, 128-byte
-//                 swizzle) into a 4-stage shared-memory ring ahead of the compute, so both the box
-//                 reads and the output rows are contiguous. Grouped launches and views the tensor
-//                 maps cannot describe take the same tiles with plain loads.
+//                 swizzle) into a shared-memory ring ahead of the compute, so both the box reads and
+//                 the output rows are contiguous; a read-only row-wise view beside them is staged
+//                 the same way (one box of its rows). Grouped launches and views the tensor maps
+//                 cannot describe take the same tiles with plain loads.
 //
 // Loop sizes, view offsets/strides and constants are kernel parameters. The source also fixes a
 // few choices derived from the sizes (lanes per point, tiles per work item, iterations per lane,
@@ -45,6 +46,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <set>
 #include <string>
 #include <vector>
@@ -68,7 +70,10 @@ bool is_fma_opcode(bh_opcode op);
 // t not synced, a and b not written in between): the ADD becomes the fused instruction, the MUL
 // becomes BH_NONE, and FREEs of a or b in between move to just after the ADD. Returns the number
 // of contractions.
-int contract_multiply_add(std::vector<bh_instruction> &list, const std::set<bh_base *> &syncs);
+// `holds_nothing(t)`, when given, says that no data is held for the product's array t (no device
+// buffer, no host data): t's FREE is then dropped as well.
+int contract_multiply_add(std::vector<bh_instruction> &list, const std::set<bh_base *> &syncs,
+                          const std::function<bool(const bh_base *)> &holds_nothing = nullptr);
 const char *sched_name(Sched s);
 
 constexpr int kThreads = 256;      // threads per CTA for every schedule
@@ -87,9 +92,11 @@ struct ParamField {
     int64_t off = 0;         // COUNTER: index offset in the unit's counters
     // TMAP: one of the 16 slots (`part`) of a TMA tensor map of `base`, which the engine encodes at
     // launch: a 2-D tiled map of the base seen as rows of `tm_ld` elements (as many whole rows as
-    // it holds), 128-byte swizzle, boxes of `tm_box` x 64 elements. `i64` is the start of the view
-    // the map serves; the view covers `tm_rows` elements along a row and `tm_cols` rows.
-    int64_t tm_ld = 0, tm_box = 0, tm_rows = 0, tm_cols = 0;
+    // it holds), boxes of tm_box_x (along a row) x tm_box_y elements, with the 128-byte swizzle
+    // when `tm_swizzle`. `i64` is the start of the view the map serves; the view covers tm_xspan
+    // elements along a row from its start and tm_yspan rows.
+    int64_t tm_ld = 0, tm_box_x = 0, tm_box_y = 0, tm_xspan = 0, tm_yspan = 0;
+    bool tm_swizzle = false;
     // TMA_OK: 1 when the engine encoded every tensor map of the unit for a plain launch and each
     // view lies inside its map with 16-byte aligned rows and start; 0 otherwise (grouped launches,
     // unaligned views), which selects the unit's code path without TMA.

@@ -9,6 +9,7 @@
 // default -ffp-contract=fast contracts wherever the fused code allows), so results agree with the
 // oracle within the elementwise tolerance either way.
 #include <algorithm>
+#include <functional>
 #include <map>
 #include "codegen.hpp"
 
@@ -41,7 +42,8 @@ bool plain_float(const bh_instruction &in, const bh_view &v, bh_type t) {
 
 bool is_fma_opcode(bh_opcode op) { return op == BH_X_FMA || op == BH_X_FMS || op == BH_X_FNMA; }
 
-int contract_multiply_add(vector<bh_instruction> &list, const set<bh_base *> &syncs) {
+int contract_multiply_add(vector<bh_instruction> &list, const set<bh_base *> &syncs,
+                          const function<bool(const bh_base *)> &holds_nothing) {
     int made = 0;
     const size_t n = list.size();
     map<size_t, vector<bh_instruction>> moved;  // FREEs of multiply inputs, re-inserted after the add
@@ -118,6 +120,13 @@ int contract_multiply_add(vector<bh_instruction> &list, const set<bh_base *> &sy
         add = std::move(fma);
         mul.opcode = BH_NONE;
         mul.operand.clear();
+        // The product's array is now never computed; when nothing is held for it, its FREE has
+        // nothing to release either and goes too (an engine would otherwise free it on every
+        // execution of the flush).
+        if (holds_nothing && holds_nothing(list[f].operand[0].base)) {
+            list[f] = bh_instruction();
+            list[f].opcode = BH_NONE;
+        }
         for (size_t k : frees) {
             moved[j].push_back(std::move(list[k]));
             list[k] = bh_instruction();

@@ -702,10 +702,11 @@ EngineCUDA::Compiled *EngineCUDA::compiled_for(const LaunchUnit &u) {
 static int64_t unit_scratch(const LaunchUnit &u) { return u.scratch_bytes(); }
 
 // The TMA tensor map of a TILE2D view (see ParamField::TMAP): base `b` at device address `p` as a
-// 2-D array of rows of tm_ld elements, boxes of tm_box x 64 elements with the 128-byte swizzle.
-// Writes the 128-byte map to `out` and returns true, or returns false (the unit then runs without
-// TMA) when the view does not fit: a TMA copy needs 16-byte aligned base, rows and start column,
-// and the view must lie inside whole rows of the map without wrapping to the next row.
+// 2-D array of rows of tm_ld elements, boxes of tm_box_x x tm_box_y elements, with the 128-byte
+// swizzle when asked. Writes the 128-byte map to `out` and returns true, or returns false (the
+// unit then runs without TMA) when the view does not fit: a TMA copy needs 16-byte aligned base,
+// rows and start column, and the view must lie inside whole rows of the map without wrapping to
+// the next row.
 bool EngineCUDA::encode_tile_map(const ParamField &f, const bh_base *b, void *p, uint8_t *out) {
     const int64_t esize = bh_type_size(b->dtype());
     const int64_t ld = f.tm_ld, start = f.i64;
@@ -713,7 +714,7 @@ bool EngineCUDA::encode_tile_map(const ParamField &f, const bh_base *b, void *p,
     const int64_t nrows = b->nelem() / ld;
     const int64_t ocol = start % ld, orow = start / ld;
     if ((ld * esize) % 16 != 0 || (ocol * esize) % 16 != 0 || reinterpret_cast<uintptr_t>(p) % 16 != 0) return false;
-    if (ocol + f.tm_rows > ld || orow + f.tm_cols > nrows || ld >= (int64_t{1} << 31) || nrows >= (int64_t{1} << 31))
+    if (ocol + f.tm_xspan > ld || orow + f.tm_yspan > nrows || ld >= (int64_t{1} << 31) || nrows >= (int64_t{1} << 31))
         return false;
     CUtensorMapDataType dt;
     switch (b->dtype()) {
@@ -727,12 +728,12 @@ bool EngineCUDA::encode_tile_map(const ParamField &f, const bh_base *b, void *p,
     }
     const cuuint64_t dims[2] = {static_cast<cuuint64_t>(ld), static_cast<cuuint64_t>(nrows)};
     const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld * esize)};
-    const cuuint32_t box[2] = {static_cast<cuuint32_t>(f.tm_box), 64u};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(f.tm_box_x), static_cast<cuuint32_t>(f.tm_box_y)};
     const cuuint32_t estr[2] = {1u, 1u};
     CUtensorMap map;
     if (api->cuTensorMapEncodeTiled(&map, dt, 2, p, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                    CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                                    f.tm_swizzle ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return false;
     static_assert(sizeof(CUtensorMap) == 128, "CUtensorMap is 128 bytes");
     memcpy(out, &map, sizeof(map));
@@ -1402,7 +1403,13 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
     vector<bh_base *> base_ids;
     bool sliding = false;
     Replay replay;
-    if (fma_contract) _stats.fma_contractions += static_cast<uint64_t>(contract_multiply_add(bhir->instr_list, bhir->_syncs));
+    if (fma_contract) {
+        auto holds_nothing = [this](const bh_base *b) {
+            return b->getDataPtr() == nullptr && !buffers.count(const_cast<bh_base *>(b));
+        };
+        _stats.fma_contractions +=
+            static_cast<uint64_t>(contract_multiply_add(bhir->instr_list, bhir->_syncs, holds_nothing));
+    }
     const uint64_t key = prepare(bhir->instr_list, instr_list, base_ids, sliding, fingerprint ? &replay : nullptr);
     const auto t1 = chrono::steady_clock::now();
     _stats.time_prepare += chrono::duration<double>(t1 - t0).count();

@@ -287,8 +287,8 @@ def test_multiply_add_contraction_conditions(case):
 @pytest.mark.parametrize("dt", [np.float32, np.float64, np.int32])
 def test_transposed_views_lower_to_tma_tiles(dt):
     """A 2-D map reading through transposed views is a TILE2D unit: TMA boxes of 128 bytes x 64
-    rows per view, the tensor maps first in the parameter struct, the struct a whole number of
-    64-byte blocks."""
+    rows per transposed view, 64 elements x TR rows for the row-wise view beside them, the tensor
+    maps first in the parameter struct."""
     def prog(rt):
         a = bh.empty(rt, (300, 500), dt)
         b = bh.empty(rt, (500, 300), dt)
@@ -297,8 +297,9 @@ def test_transposed_views_lower_to_tma_tiles(dt):
     res, units = plan(prog)
     assert [u["sched"] for u in units] == ["tile2d"]
     src = units[0]["source"]
-    assert src.count("cp.async.bulk.tensor.2d") == 1 and src.count("bh_tma_2d(stage") == 2
-    assert "bh_tmap tm0;" in src and "bh_tmap tm1;" in src
+    assert src.count("cp.async.bulk.tensor.2d") == 1 and src.count("bh_tma_2d(stage") == 3
+    assert "bh_tmap tm0;" in src and "bh_tmap tm1;" in src and "bh_tmap tm2;" in src
+    assert src.count("+ tc * 64), (int)(p.ty") == 1  # the row-wise view's box moves along its rows
     assert src.index("bh_tmap tm0;") < src.index("a0;")
     assert "bh_mbar_wait" in src and "(1 << 20)" in src  # bounded waits
 

@@ -421,10 +421,13 @@ def _stat(ex, key):
     return 0.0
 
 
-def test_autotuned_variants_are_bit_identical(gpu_executor):
+def test_autotuned_variants_are_bit_identical(monkeypatch):
     """The first launches of a large kernel rotate through register-capped variants (autotuning);
-    every launch gives the same bits."""
+    every launch gives the same bits. A fresh engine without a kernel cache directory, so no
+    earlier process's tuning choice applies."""
     from bohrium_b200 import workloads as W
+    monkeypatch.setenv("BH_CUDA_CACHE_DIR", "NONE")
+    gpu_executor = bh.NativeExecutor(stack="cuda")
     rt = bh.Runtime(gpu_executor)
     n = 3 << 20
     S, K, T = W.black_scholes_inputs(n, 5)
@@ -443,6 +446,8 @@ def test_autotuned_variants_are_bit_identical(gpu_executor):
     want = float(np.sum(np.sqrt(S) * np.log(K) / (T + 1.5) - np.exp(-T) * 0.25))
     got = float(np.frombuffer(seen.pop(), dtype=np.float64)[0])
     assert abs(got - want) <= 1e-11 * abs(want)  # NumPy's exp/log differ from CUDA's by ulps
+    del ir, m, s, k, t
+    gpu_executor.close()
 
 
 @pytest.mark.parametrize("n,dtype", [(1_000_003, np.float32), (16_000_000, np.float64), (45_000_001, np.float32)])

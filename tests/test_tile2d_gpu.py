@@ -43,7 +43,9 @@ def test_transpose_add_matches_oracle(gpu_executor, gpu_rt, oracle_rt, dt, shape
     for k, (x, y) in enumerate(zip(g, o)):
         assert np.asarray(x).tobytes() == np.asarray(y).tobytes(), k
     assert_close(g[0], A + B.T, 0, 0, "vs numpy")
-    assert _stats(gpu_executor)["tma_units"] > t0  # the tiles came through TMA
+    # TMA needs rows of B on 16-byte boundaries; (33, 64) has rows of 33 elements: plain loads.
+    tma = (shape[0] * np.dtype(dt).itemsize) % 16 == 0
+    assert (_stats(gpu_executor)["tma_units"] > t0) == tma
 
 
 def test_two_transposed_views_and_fallbacks(gpu_executor, gpu_rt, oracle_rt):
