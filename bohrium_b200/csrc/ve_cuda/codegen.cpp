@@ -70,9 +70,9 @@ int64_t LaunchUnit::scratch_bytes() const {
 int64_t LaunchUnit::counters_needed() const {
     int64_t own = 0;
     if (sched == Sched::SCAN1D && single_pass) {
-        // chunk flags, group flags (one spare), ticket, CTAs that left, abort
+        // chunk, thread-sum, warp-total and group flags (one spare), ticket, CTAs that left, abort
         const int64_t ngroups = (chunks + kThreads * 8 - 1) / (kThreads * 8);
-        own = chunks + ngroups + 1 + 3;
+        own = chunks + (chunks + 7) / 8 + (chunks + 255) / 256 + ngroups + 1 + 3;
     }
     if (sched == Sched::GRID_REDUCE) own = 1;
     if (sched == Sched::SPLIT_REDUCE) own = (rows * cols + kThreads - 1) / kThreads;
@@ -141,6 +141,14 @@ template <typename T> __device__ __forceinline__ T bh_shfl_xor(T v, int m) {
         x = __shfl_xor_sync(0xffffffffu, x, m);
         T r; memcpy(&r, &x, sizeof(T)); return r;
     }
+}
+
+template <typename T> __device__ __forceinline__ T bh_shfl_idx(T v, int src) {
+    long long x[2] = {0, 0};
+    memcpy(x, &v, sizeof(T));
+    x[0] = __shfl_sync(0xffffffffu, x[0], src);
+    if (sizeof(T) > 8) x[1] = __shfl_sync(0xffffffffu, x[1], src);
+    T r; memcpy(&r, x, sizeof(T)); return r;
 }
 
 template <typename T> __device__ __forceinline__ T bh_shfl_up(T v, int d) {
@@ -3173,13 +3181,14 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
 
 // SCAN1D in one pass (single_pass): every CTA takes chunks by ticket (an atomic counter, so all
 // lower chunks belong to CTAs that are already running), stages and folds its chunk as unit A
-// does, publishes the chunk total behind a release flag, and then looks back: it waits for the
-// totals of the chunks before it in its group of 2048 and evaluates unit B's per-thread folds and
-// block scan over them (entries past its own are left out, which does not change the prefix at
-// its own position), and waits for the carry into its group, which the last chunk of the previous
-// group publishes as that group's carry op its total. The chunk then rescans its staged elements
-// as unit C does. Every value is formed by the same operations in the same order as in the three
-// units, so the result is bit-identical to them, while each element is read from memory once.
+// does, publishes the chunk total behind a release flag, and then looks back with warp 0. In unit
+// B's scan of the chunk totals, chunk c is entry k of thread t (lane l of warp w) of group g; the
+// chunk that closes a thread (k = 7) publishes the thread's sum, the one that closes a warp
+// (k = 7, l = 31) the warp's total from the same 32-lane shuffle scan, and the one that closes a
+// group the carry into the next group. Chunk c waits for at most 7 chunk totals, 31 thread sums,
+// 7 warp totals and its group's carry, and combines them with unit B's and C's operations in
+// their order, so the result is bit-identical to the three units while each element is read from
+// memory once.
 // Waits poll a bounded number of times (`p.spin_cap`; negative: none); when one runs out, or
 // another CTA gave up, the chunk is abandoned and an abort flag raised. The CTA that leaves last
 // then recomputes the whole scan alone with the three units' steps, and resets the flags and
@@ -3350,32 +3359,6 @@ __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *a
     body << "        }\n";
     body << "    }\n";
     body << "}\n";
-    // Unit B's scan of the chunk totals of group g over entries 0..upto (entries after `upto` are
-    // left out: they do not change the prefixes at or before it). Returns the prefix at position
-    // `upto` (in every thread) and the group total in `gt`.
-    body << "__device__ __forceinline__ " << T << " bh_group_prefix(const P &p, const " << T << " *totals, bh_i64 g, int upto, "
-         << T << " &gt, " << T << " *sm, " << T << " *bcast) {\n";
-    body << "    const bh_i64 base = g * " << kScanTile << ";\n";
-    body << "    " << T << " v[" << kScanPerThread << "];\n";
-    body << "    " << T << " s = " << ident << ";\n";
-    body << "#pragma unroll\n";
-    body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
-    body << "        const int jj = (int)threadIdx.x * " << kScanPerThread << " + k;\n";
-    body << "        v[k] = s;\n";
-    body << "        if (jj <= upto && base + jj < p.nchunks) { const " << T << " x = bh_ldcg(totals + base + jj); s = "
-         << op("s", "x") << "; }\n";
-    body << "    }\n";
-    body << "    const " << T << " e = bh_block_scan(s, gt, sm);\n";
-    body << "    if ((int)threadIdx.x == upto / " << kScanPerThread << ") {\n";
-    body << "#pragma unroll\n";
-    body << "        for (int k = 0; k < " << kScanPerThread << "; ++k)\n";
-    body << "            if (k == upto % " << kScanPerThread << ") *bcast = " << op("e", "v[k]") << ";\n";
-    body << "    }\n";
-    body << "    __syncthreads();\n";
-    body << "    const " << T << " r = *bcast;\n";
-    body << "    __syncthreads();\n";
-    body << "    return r;\n";
-    body << "}\n";
     body << "__device__ void bh_work(const P &p, bh_i64 w) {}\n";  // never launched grouped
     body << "__device__ __forceinline__ void bh_main(const P &p) {\n";
     body << "    __shared__ " << T << " stage[" << kScanTile + kScanTile / kScanPerThread << "];\n";
@@ -3383,12 +3366,22 @@ __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *a
     body << "    __shared__ " << T << " bcast;\n";
     body << "    __shared__ bh_i64 ticket;\n";
     body << "    __shared__ bool last;\n";
+    // Published values (scan arena) and their flags (counters): chunk totals; thread sums (the fold
+    // of 8 consecutive chunk totals, unit B's per-thread step); warp totals (unit B's shuffle scan
+    // over 32 thread sums); group carries.
+    body << "    const bh_i64 nthr = (p.nchunks + 7) / 8, nwarp = (p.nchunks + 255) / 256;\n";
     body << "    " << T << "* totals = (" << T << "*)p.scratch;\n";
     body << "    " << T << "* carries = totals + p.nchunks;\n";
-    body << "    " << T << "* gcarry = carries + p.nchunks;\n";
+    body << "    " << T << "* tsum = carries + p.nchunks;\n";
+    body << "    " << T << "* wtot = tsum + nthr;\n";
+    body << "    " << T << "* gcarry = wtot + nwarp;\n";
     body << "    unsigned* flags = p.counter;\n";
-    body << "    unsigned* gflags = flags + p.nchunks;\n";
+    body << "    unsigned* sflags = flags + p.nchunks;\n";
+    body << "    unsigned* wflags = sflags + nthr;\n";
+    body << "    unsigned* gflags = wflags + nwarp;\n";
     body << "    unsigned* ctr = gflags + p.ngroups + 1;  // ticket, CTAs that left, abort\n";
+    body << "    __shared__ " << T << " lb_carry;\n";
+    body << "    __shared__ int lb_ok;\n";
     body << "    " << T << " xs[" << kScanPerThread << "];\n";
     body << R"CUDA(    for (;;) {
         if (threadIdx.x == 0) ticket = bh_ld_acquire(ctr + 2) != 0u ? p.nchunks : (bh_i64)atomicAdd(ctr, 1u);
@@ -3404,28 +3397,86 @@ __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *a
             totals[c] = total;
             bh_st_release(flags + c, 1u);
         }
-        // Look back: the totals of the chunks before c in its group, then the carry into the group.
-        const bh_i64 g = c / )CUDA" << kScanTile << R"CUDA(;
-        const int q = (int)(c - g * )CUDA" << kScanTile << R"CUDA();
-        bool ok = true;
-        for (int k = 0; k < )CUDA" << kScanPerThread << R"CUDA( && ok; ++k) {
-            const int jj = (int)threadIdx.x * )CUDA" << kScanPerThread << R"CUDA( + k;
-            if (jj < q) ok = bh_await(flags + g * )CUDA" << kScanTile << R"CUDA( + jj, ctr + 2, p.spin_cap);
-        }
-        if (threadIdx.x == 0 && ok && g > 0) ok = bh_await(gflags + g, ctr + 2, p.spin_cap);
-        if (!__syncthreads_and(ok)) {
+        // Look back (warp 0; the other warps wait at the barrier below). Chunk c is entry k of
+        // thread t = lane l of warp w of group g in unit B's scan of the chunk totals.
+        if (threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            const bh_i64 g = c / )CUDA" << kScanTile << R"CUDA(;
+            const int q = (int)(c - g * )CUDA" << kScanTile << R"CUDA();
+            const int k = q & 7, t = q >> 3, l = t & 31, w = t >> 5;
+            const bh_i64 tg = c >> 3, wg = c >> 8;  // global thread and warp of c
+            bool ok = true;
+)CUDA";
+    body << "            " << T << " x1 = " << ident << ", x2 = " << ident << ", x3 = " << ident << ";\n";
+    body << R"CUDA(            if (lane < k) {  // totals of the entries before k in thread t
+                ok = bh_await(flags + c - k + lane, ctr + 2, p.spin_cap);
+                if (ok) x1 = bh_ldcg(totals + c - k + lane);
+            }
+            if (ok && lane < l) {  // thread sums of the lanes before l in warp w
+                ok = bh_await(sflags + tg - l + lane, ctr + 2, p.spin_cap);
+                if (ok) x2 = bh_ldcg(tsum + tg - l + lane);
+            }
+            if (ok && lane < w) {  // totals of the warps before w in group g
+                ok = bh_await(wflags + wg - w + lane, ctr + 2, p.spin_cap);
+                if (ok) x3 = bh_ldcg(wtot + wg - w + lane);
+            }
+            if (ok && lane == 0 && g > 0) ok = bh_await(gflags + g, ctr + 2, p.spin_cap);
+            ok = __all_sync(0xffffffffu, ok);
+            if (ok) {
+)CUDA";
+    // v: unit B's exclusive running fold in thread t before entry k; s: its thread sum
+    body << "                " << T << " v = " << ident << ";\n";
+    body << "                for (int i = 0; i < k; ++i) { const " << T << " y = bh_shfl_idx(x1, i); v = " << op("v", "y") << "; }\n";
+    body << "                const " << T << " sT = " << op("v", "total") << ";\n";
+    body << R"CUDA(                if (k == 7 && lane == 0) {
+                    tsum[tg] = sT;
+                    bh_st_release(sflags + tg, 1u);
+                }
+)CUDA";
+    // unit B's shuffle scan within warp w (lanes after l do not change lanes up to l)
+    body << "                " << T << " xk = lane < l ? x2 : (lane == l && k == 7 ? sT : " << ident << ");\n";
+    body << "#pragma unroll\n";
+    body << "                for (int d = 1; d < 32; d <<= 1) {\n";
+    body << "                    " << T << " y = bh_shfl_up(xk, d);\n";
+    body << "                    if (lane >= d) xk = " << op("y", "xk") << ";\n";
+    body << "                }\n";
+    body << "                const " << T << " exv = bh_shfl_idx(xk, l > 0 ? l - 1 : 0);\n";
+    body << "                const " << T << " ex = l > 0 ? exv : " << ident << ";\n";
+    body << "                const " << T << " wt = bh_shfl_idx(xk, 31);\n";
+    body << R"CUDA(                if (k == 7 && l == 31 && lane == 0) {
+                    wtot[wg] = wt;
+                    bh_st_release(wflags + wg, 1u);
+                }
+)CUDA";
+    // warp offsets: serial run over the warp totals before w
+    body << "                " << T << " wo = " << ident << ";\n";
+    body << "                " << T << " gt = " << ident << ";\n";
+    body << "                for (int i = 0; i < 8; ++i) {\n";
+    body << "                    const " << T << " y = bh_shfl_idx(x3, i);\n";
+    body << "                    if (i < w) wo = " << op("wo", "y") << ";\n";
+    body << "                    if (i < 7) gt = " << op("gt", "y") << ";\n";
+    body << "                }\n";
+    body << "                const " << T << " within = " << op(op("wo", "ex"), "v") << ";\n";
+    body << "                const " << T << " grun = g > 0 ? bh_ldcg(gcarry + g) : " << ident << ";\n";
+    body << "                if (lane == 0) {\n";
+    body << "                    lb_carry = " << op("grun", "within") << ";\n";
+    body << "                    if (q == " << kScanTile - 1 << " && g + 1 < p.ngroups) {\n";
+    body << "                        gt = " << op("gt", "wt") << ";\n";
+    body << "                        gcarry[g + 1] = " << op("grun", "gt") << ";\n";
+    body << "                        bh_st_release(gflags + g + 1, 1u);\n";
+    body << "                    }\n";
+    body << "                }\n";
+    body << "            }\n";
+    body << "            if (lane == 0) lb_ok = ok ? 1 : 0;\n";
+    body << "        }\n";
+    body << R"CUDA(        __syncthreads();
+        if (!lb_ok) {
             if (threadIdx.x == 0) atomicExch(ctr + 2, 1u);
             break;
         }
+        bh_chunk_rescan(p, c, stage, xs, e, lb_carry);
 )CUDA";
-    body << "        " << T << " gt;\n";
-    body << "        const " << T << " within = bh_group_prefix(p, totals, g, q, gt, sm, &bcast);\n";
-    body << "        const " << T << " grun = g > 0 ? bh_ldcg(gcarry + g) : " << ident << ";\n";
-    body << "        if (threadIdx.x == 0 && q == " << kScanTile - 1 << " && g + 1 < p.ngroups) {\n";
-    body << "            gcarry[g + 1] = " << op("grun", "gt") << ";\n";
-    body << "            bh_st_release(gflags + g + 1, 1u);\n";
-    body << "        }\n";
-    body << "        bh_chunk_rescan(p, c, stage, xs, e, " << op("grun", "within") << ");\n";
+
     body << R"CUDA(        __syncthreads();
         bh_stage_out(p, c, stage);
         __syncthreads();  // stage reads before the next chunk's writes
@@ -3482,7 +3533,7 @@ __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *a
     body << "            __syncthreads();\n";
     body << "        }\n";
     body << "    }\n";
-    body << R"CUDA(    for (bh_i64 i = threadIdx.x; i < p.nchunks + p.ngroups + 1; i += blockDim.x) flags[i] = 0u;
+    body << R"CUDA(    for (bh_i64 i = threadIdx.x; i < p.nchunks + nthr + nwarp + p.ngroups + 1; i += blockDim.x) flags[i] = 0u;
     if (threadIdx.x == 0) {
         ctr[0] = 0u;
         ctr[1] = 0u;
@@ -3492,7 +3543,8 @@ __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *a
 )CUDA";
     body << kKernels;
     u.fields = pl.fields;
-    u.scan_bytes = (2 * nchunks + ngroups + 1) * static_cast<int64_t>(bh_type_size(t));
+    u.scan_bytes = (2 * nchunks + (nchunks + 7) / 8 + (nchunks + 255) / 256 + ngroups + 1) *
+                   static_cast<int64_t>(bh_type_size(t));
     u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
     u.elements = n;
     u.red_orders.emplace_back(acc->origin_id, "scan:" + to_string(kScanTile) + ":" + to_string(n));

@@ -158,3 +158,66 @@ def test_grid_reduce_model_matches_a_scalar_transcription(n):
             fold[t] = dt.type(fold[t] + parts[k])
     want = _scalar_block_tree(fold, dt)
     assert grid_reduce_sum(x).tobytes() == np.asarray(want, dtype=dt).tobytes()
+
+
+def _single_pass_scan(x):
+    """The single-pass SCAN1D's arithmetic chunk by chunk, as its look-back forms it: each chunk's
+    exclusive prefix within its thread (v), the thread sums and warp totals that the closing chunks
+    publish (32-lane shuffle scan), the warp offsets, and the group carries chained group by group.
+    The chunk totals and in-chunk scans are unit A/C's (the model's own helpers)."""
+    from tests.harness import _block_scan
+    dt = x.dtype
+    zero = dt.type(0)
+    n = x.size
+    nch = -(-n // 2048)
+    pad = np.zeros(nch * 2048, dtype=dt)
+    pad[:n] = x
+    xs = pad.reshape(nch, 256, 8)
+    valid = (np.arange(nch * 2048) < n).reshape(nch, 256, 8)
+    s = np.full((nch, 256), zero, dtype=dt)
+    for k in range(8):
+        s = np.where(valid[:, :, k], s + xs[:, :, k], s)
+    e, totals = _block_scan(s)
+    tsum, wtot, gcarry = {}, {}, {0: zero}
+    carry = np.empty(nch, dtype=dt)
+    for c in range(nch):  # in ticket order: everything a chunk waits for is published before it
+        g, q = divmod(c, 2048)
+        k, t = q & 7, q >> 3
+        l, w = t & 31, t >> 5
+        v = zero
+        for i in range(k):
+            v = dt.type(v + totals[c - k + i])
+        sT = dt.type(v + totals[c])
+        if k == 7:
+            tsum[c >> 3] = sT
+        lanes = [tsum[(c >> 3) - l + i] if i < l else (sT if i == l and k == 7 else zero) for i in range(32)]
+        for d in (1, 2, 4, 8, 16):
+            lanes = [dt.type(lanes[i - d] + lanes[i]) if i >= d else lanes[i] for i in range(32)]
+        ex = lanes[l - 1] if l > 0 else zero
+        if k == 7 and l == 31:
+            wtot[c >> 8] = lanes[31]
+        wo = zero
+        for i in range(w):
+            wo = dt.type(wo + wtot[(c >> 8) - w + i])
+        within = dt.type(dt.type(wo + ex) + v)
+        carry[c] = dt.type(gcarry[g] + within)
+        if q == 2047:
+            gt = zero
+            for i in range(7):
+                gt = dt.type(gt + wtot[(c >> 8) - 7 + i])
+            gt = dt.type(gt + lanes[31])
+            gcarry[g + 1] = dt.type(gcarry[g] + gt)
+    out = np.empty((nch, 256, 8), dtype=dt)
+    r = np.full((nch, 256), zero, dtype=dt)
+    for k in range(8):
+        r = np.where(valid[:, :, k], r + xs[:, :, k], r)
+        out[:, :, k] = carry[:, None] + (e + r)
+    return out.reshape(-1)[:n]
+
+
+@pytest.mark.parametrize("n", [5, 2049, 300_001, 4_500_001])
+def test_single_pass_lookback_equals_the_order_model(n):
+    """The single-pass scan's look-back (thread sums, warp totals, group carries published by the
+    chunks that close them) rebuilds exactly the three units' carries: bit for bit the model."""
+    x = np.random.default_rng(n + 1).standard_normal(n).astype(np.float32)
+    assert _single_pass_scan(x).tobytes() == scan1d_cumsum(x).tobytes()
