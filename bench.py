@@ -552,17 +552,23 @@ def extra_scan(bh, W, ex, rt, out, n=50_000_000):
     del ir, y, x
 
 
-def extra_learned(bh, W, ex, rt, out, train_seeds=24, eval_seeds=12):
+def extra_learned(bh, W, ex, rt, out, train_seeds=24, eval_seeds=12, holdout_seeds=48):
     """The learned-fuser workload: seeded random bytecode DAGs (50-400 operations, 1e3-1e8
     elements, float32/float64/int32, transposed/reversed/broadcast views, 0-3 reductions). The
     engine records per-kernel device times on the training DAGs, the cost model is trained on the
-    GPU, and held-out DAGs are timed under the plain engine (greedy plan, one launch per kernel),
-    the batched engine (CUDA-graph replay) and the batched + learned engine."""
+    GPU, its prediction error is measured on the recorded kernels of other DAGs (held out), and
+    held-out DAGs are timed under the plain engine (greedy plan, one launch per kernel), the
+    batched engine (CUDA-graph replay) and the batched + learned engine."""
     from bohrium_b200 import learn
     t0 = time.perf_counter()
     X, t = learn.collect(ex, seeds=range(train_seeds), max_elems=1e7)
     t1 = time.perf_counter()
     model, loss = learn.train(X, t, epochs=300)
+    t2 = time.perf_counter()
+    Xh, th = learn.collect(ex, seeds=range(5000, 5000 + holdout_seeds), max_elems=1e7, variants=learn.VARIANTS[:2])
+    holdout = learn.holdout_error(model, Xh, th)
+    holdout.update({"dags": holdout_seeds, "train_r2": learn.holdout_error(model, X, t)["r2"],
+                    "collect_s": round(time.perf_counter() - t2, 1)})
     t2 = time.perf_counter()
     fd, path = tempfile.mkstemp(suffix=".cm")
     os.close(fd)
@@ -572,7 +578,8 @@ def extra_learned(bh, W, ex, rt, out, train_seeds=24, eval_seeds=12):
     finally:
         os.unlink(path)
     res = learn.summary(rows)
-    res.update({"records": int(X.shape[0]), "train_loss": round(loss, 4), "collect_s": round(t1 - t0, 1),
+    res.update({"records": int(X.shape[0]), "train_loss": round(loss, 4), "holdout": holdout,
+                "collect_s": round(t1 - t0, 1),
                 "train_s": round(t2 - t1, 2), "eval_s": round(time.perf_counter() - t2, 1),
                 "per_dag_speedup_vs_plain": [round(r["plain_ms"] / r["learned_ms"], 2) for r in rows]})
     out["learned_fuser_random_dags"] = res

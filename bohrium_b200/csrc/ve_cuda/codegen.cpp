@@ -3240,6 +3240,7 @@ __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *a
     long long spins = 0;
     while (bh_ld_acquire(flag) == 0u) {
         if (cap < 0 || ++spins > cap || bh_ld_acquire(abort_flag) != 0u) return false;
+        __nanosleep(32);  // fewer polls of L2 while the producer works
     }
     return true;
 }
@@ -3407,64 +3408,67 @@ __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *a
             const bh_i64 tg = c >> 3, wg = c >> 8;  // global thread and warp of c
             bool ok = true;
 )CUDA";
+    // Each value is published as soon as its own inputs are in, before the waits it does not
+    // depend on: a thread sum needs only its 8 chunk totals, a warp total only its 32 thread
+    // sums, the next group's carry only this group's warp totals and carry.
     body << "            " << T << " x1 = " << ident << ", x2 = " << ident << ", x3 = " << ident << ";\n";
     body << R"CUDA(            if (lane < k) {  // totals of the entries before k in thread t
                 ok = bh_await(flags + c - k + lane, ctr + 2, p.spin_cap);
                 if (ok) x1 = bh_ldcg(totals + c - k + lane);
             }
+            ok = __all_sync(0xffffffffu, ok);
+)CUDA";
+    // v: unit B's exclusive running fold in thread t before entry k; sT: the thread's sum
+    body << "            " << T << " v = " << ident << ";\n";
+    body << "            for (int i = 0; i < k; ++i) { const " << T << " y = bh_shfl_idx(x1, i); v = " << op("v", "y") << "; }\n";
+    body << "            const " << T << " sT = " << op("v", "total") << ";\n";
+    body << R"CUDA(            if (ok && k == 7 && lane == 0) {
+                tsum[tg] = sT;
+                bh_st_release(sflags + tg, 1u);
+            }
             if (ok && lane < l) {  // thread sums of the lanes before l in warp w
                 ok = bh_await(sflags + tg - l + lane, ctr + 2, p.spin_cap);
                 if (ok) x2 = bh_ldcg(tsum + tg - l + lane);
+            }
+            ok = __all_sync(0xffffffffu, ok);
+)CUDA";
+    // unit B's shuffle scan within warp w (lanes after l do not change lanes up to l)
+    body << "            " << T << " xk = lane < l ? x2 : (lane == l && k == 7 ? sT : " << ident << ");\n";
+    body << "#pragma unroll\n";
+    body << "            for (int d = 1; d < 32; d <<= 1) {\n";
+    body << "                " << T << " y = bh_shfl_up(xk, d);\n";
+    body << "                if (lane >= d) xk = " << op("y", "xk") << ";\n";
+    body << "            }\n";
+    body << "            const " << T << " exv = bh_shfl_idx(xk, l > 0 ? l - 1 : 0);\n";
+    body << "            const " << T << " ex = l > 0 ? exv : " << ident << ";\n";
+    body << "            const " << T << " wt = bh_shfl_idx(xk, 31);\n";
+    body << R"CUDA(            if (ok && k == 7 && l == 31 && lane == 0) {
+                wtot[wg] = wt;
+                bh_st_release(wflags + wg, 1u);
             }
             if (ok && lane < w) {  // totals of the warps before w in group g
                 ok = bh_await(wflags + wg - w + lane, ctr + 2, p.spin_cap);
                 if (ok) x3 = bh_ldcg(wtot + wg - w + lane);
             }
-            if (ok && lane == 0 && g > 0) ok = bh_await(gflags + g, ctr + 2, p.spin_cap);
             ok = __all_sync(0xffffffffu, ok);
-            if (ok) {
 )CUDA";
-    // v: unit B's exclusive running fold in thread t before entry k; s: its thread sum
-    body << "                " << T << " v = " << ident << ";\n";
-    body << "                for (int i = 0; i < k; ++i) { const " << T << " y = bh_shfl_idx(x1, i); v = " << op("v", "y") << "; }\n";
-    body << "                const " << T << " sT = " << op("v", "total") << ";\n";
-    body << R"CUDA(                if (k == 7 && lane == 0) {
-                    tsum[tg] = sT;
-                    bh_st_release(sflags + tg, 1u);
-                }
-)CUDA";
-    // unit B's shuffle scan within warp w (lanes after l do not change lanes up to l)
-    body << "                " << T << " xk = lane < l ? x2 : (lane == l && k == 7 ? sT : " << ident << ");\n";
-    body << "#pragma unroll\n";
-    body << "                for (int d = 1; d < 32; d <<= 1) {\n";
-    body << "                    " << T << " y = bh_shfl_up(xk, d);\n";
-    body << "                    if (lane >= d) xk = " << op("y", "xk") << ";\n";
-    body << "                }\n";
-    body << "                const " << T << " exv = bh_shfl_idx(xk, l > 0 ? l - 1 : 0);\n";
-    body << "                const " << T << " ex = l > 0 ? exv : " << ident << ";\n";
-    body << "                const " << T << " wt = bh_shfl_idx(xk, 31);\n";
-    body << R"CUDA(                if (k == 7 && l == 31 && lane == 0) {
-                    wtot[wg] = wt;
-                    bh_st_release(wflags + wg, 1u);
-                }
-)CUDA";
-    // warp offsets: serial run over the warp totals before w
-    body << "                " << T << " wo = " << ident << ";\n";
-    body << "                " << T << " gt = " << ident << ";\n";
-    body << "                for (int i = 0; i < 8; ++i) {\n";
-    body << "                    const " << T << " y = bh_shfl_idx(x3, i);\n";
-    body << "                    if (i < w) wo = " << op("wo", "y") << ";\n";
-    body << "                    if (i < 7) gt = " << op("gt", "y") << ";\n";
-    body << "                }\n";
-    body << "                const " << T << " within = " << op(op("wo", "ex"), "v") << ";\n";
+    // warp offsets: serial run over the warp totals before w (and the group total's first 7)
+    body << "            " << T << " wo = " << ident << ";\n";
+    body << "            " << T << " gt = " << ident << ";\n";
+    body << "            for (int i = 0; i < 8; ++i) {\n";
+    body << "                const " << T << " y = bh_shfl_idx(x3, i);\n";
+    body << "                if (i < w) wo = " << op("wo", "y") << ";\n";
+    body << "                if (i < 7) gt = " << op("gt", "y") << ";\n";
+    body << "            }\n";
+    body << "            if (ok && lane == 0 && g > 0) ok = bh_await(gflags + g, ctr + 2, p.spin_cap);\n";
+    body << "            ok = __all_sync(0xffffffffu, ok);\n";
+    body << "            if (ok && lane == 0) {\n";
     body << "                const " << T << " grun = g > 0 ? bh_ldcg(gcarry + g) : " << ident << ";\n";
-    body << "                if (lane == 0) {\n";
-    body << "                    lb_carry = " << op("grun", "within") << ";\n";
-    body << "                    if (q == " << kScanTile - 1 << " && g + 1 < p.ngroups) {\n";
-    body << "                        gt = " << op("gt", "wt") << ";\n";
-    body << "                        gcarry[g + 1] = " << op("grun", "gt") << ";\n";
-    body << "                        bh_st_release(gflags + g + 1, 1u);\n";
-    body << "                    }\n";
+    body << "                lb_carry = " << op("grun", op(op("wo", "ex"), "v")) << ";\n";
+    body << "                if (q == " << kScanTile - 1 << " && g + 1 < p.ngroups) {\n";
+    body << "                    gt = " << op("gt", "wt") << ";\n";
+    body << "                    gcarry[g + 1] = " << op("grun", "gt") << ";\n";
+    body << "                    bh_st_release(gflags + g + 1, 1u);\n";
     body << "                }\n";
     body << "            }\n";
     body << "            if (lane == 0) lb_ok = ok ? 1 : 0;\n";

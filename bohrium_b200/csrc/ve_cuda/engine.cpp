@@ -682,15 +682,16 @@ EngineCUDA::Compiled *EngineCUDA::compiled_for(const LaunchUnit &u) {
     auto tc = tune_choices.find(h);
     if (tc != tune_choices.end()) {
         c.tuned = true;
-        if (tc->second.first > 0 || tc->second.second > 0) {
-            c.variants.push_back(make_variant(c, tc->second.first, tc->second.second));
+        if (tc->second.maxrreg > 0 || tc->second.unroll > 0) {
+            c.variants.push_back(make_variant(c, tc->second.maxrreg, tc->second.unroll));
             c.chosen = 1;
         }
+        c.variants.back().ctas = tc->second.ctas;
     }
     const Compiled::Variant &v = c.variants[static_cast<size_t>(c.chosen)];
     c.fn = v.fn;
     c.fn_batch = v.fn_batch;
-    c.occ = v.occ;
+    c.occ = v.ctas_per_sm();
     c.occ_batch = v.occ_batch;
     _stats.time_compile += seconds_since(t0);
     if (verbose) cerr << "[ve_cuda] compiled " << u.name << "\n" << u.source << endl;
@@ -1278,7 +1279,10 @@ EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const
             }
         }
         pk.writes.assign(writes.begin(), writes.end());
-        if ((record || learned_on) && !pk.units.empty()) pk.feat = jitk::block_features(kernel);
+        // Features of every kernel, whether recording is on or not: a plan built before recording
+        // is switched on is reused by the recorded executions (computing them only when recording
+        // left those kernels with all-zero features).
+        if (!pk.units.empty()) pk.feat = jitk::block_features(kernel);
         // Summation order of the floating-point sums and products: "seq" (one thread folds in
         // index order) unless a unit reduces the sweep across threads.
         for (const LoopB *part : parts)

@@ -124,7 +124,9 @@ public:
         struct Variant {
             void *fn = nullptr, *fn_batch = nullptr;
             int occ = 1, occ_batch = 1, maxrreg = 0, unroll = 0, regs = 0;
+            int ctas = 0;  // CTAs per SM of the plain launch (0: as many as fit)
             std::vector<float> ms, ms_batch;
+            int ctas_per_sm() const { return ctas > 0 && ctas < occ ? ctas : occ; }
         };
         std::vector<Variant> variants; // [0]: the default compilation
         std::string name, source;
@@ -219,9 +221,12 @@ private:
     bool tune_launch(Compiled &c, const LaunchUnit &u, int64_t work, void **args);
     bool tune_batch_launch(Compiled &c, int64_t total, void **args);
     void ensure_variants(Compiled &c);
-    std::map<uint64_t, std::pair<int, int>> tune_choices; // source hash -> (register cap, unroll); 0: default
+    struct TuneChoice {
+        int maxrreg = 0, unroll = 0, ctas = 0;  // 0: the default
+    };
+    std::map<uint64_t, TuneChoice> tune_choices; // source hash -> the variant chosen by an earlier run
     void load_tune_choices();
-    void save_tune_choice(uint64_t hash, int maxrreg, int unroll);
+    void save_tune_choice(uint64_t hash, int maxrreg, int unroll, int ctas);
     Compiled::Variant make_variant(const Compiled &c, int maxrreg, int unroll);
     // NVRTC-compile the sources of `units` that are not cached yet, in parallel host threads.
     void precompile(const std::vector<const LaunchUnit *> &units);

@@ -1,9 +1,11 @@
-// Autotuning of launch shapes: register caps and inner-loop unrolling.
+// Autotuning of launch shapes: register caps, inner-loop unrolling and CTAs per SM.
 //
 // A kernel with large work (at least `tune_min_elements` elements) is compiled a few more times:
 // with NVRTC's --maxrregcount below its natural register count (more resident CTAs per SM,
 // possibly at the cost of spills) and, where the source marks its element loop, with that loop
-// unrolled 2 or 4 times (more loads in flight per thread). Its first plain launches rotate through
+// unrolled 2 or 4 times (more loads in flight per thread); and its plain launch is also tried with
+// half the CTAs per SM that fit, and with one (a smaller persistent grid: less contention on
+// shared counters and L2 sets, longer runs per CTA). Its first plain launches rotate through
 // the variants, each timed alone with CUDA events. After three timings of every variant the fastest
 // one is kept for that source, and the choice is written to the kernel cache directory
 // (tune.txt) so that later processes start with it. Register caps and unrolling change neither
@@ -43,16 +45,22 @@ constexpr size_t kTuneSamples = 3;  // timed launches per variant (the fastest c
 void EngineCUDA::load_tune_choices() {
     if (cache_dir.empty()) return;
     ifstream in(cache_dir + "/tune.txt");
-    string hex_hash;
-    int cap = 0, unroll = 0;
-    while (in >> hex_hash >> cap >> unroll) tune_choices[stoull(hex_hash, nullptr, 16)] = {cap, unroll};
+    string line;
+    while (getline(in, line)) {
+        stringstream ss(line);
+        string hex_hash;
+        TuneChoice c;
+        if (!(ss >> hex_hash >> c.maxrreg >> c.unroll)) continue;
+        if (!(ss >> c.ctas)) c.ctas = 0;
+        tune_choices[stoull(hex_hash, nullptr, 16)] = c;
+    }
 }
 
-void EngineCUDA::save_tune_choice(uint64_t hash, int maxrreg, int unroll) {
-    tune_choices[hash] = {maxrreg, unroll};
+void EngineCUDA::save_tune_choice(uint64_t hash, int maxrreg, int unroll, int ctas) {
+    tune_choices[hash] = TuneChoice{maxrreg, unroll, ctas};
     if (cache_dir.empty()) return;
     ofstream out(cache_dir + "/tune.txt", ios::app);
-    out << hex << hash << " " << dec << maxrreg << " " << unroll << "\n";
+    out << hex << hash << " " << dec << maxrreg << " " << unroll << " " << ctas << "\n";
 }
 
 EngineCUDA::Compiled::Variant EngineCUDA::make_variant(const Compiled &c, int maxrreg, int unroll) {
@@ -78,6 +86,18 @@ void EngineCUDA::ensure_variants(Compiled &c) {
         if (c.source.find(kUnrollMarker) != string::npos) {
             for (int unroll : {2, 4}) c.variants.push_back(make_variant(c, 0, unroll));
             if (!caps.empty()) c.variants.push_back(make_variant(c, caps.back(), 4));
+        }
+        // Launch shape: fewer resident CTAs per SM than fit (the same code, a smaller grid).
+        const int occ = c.variants[0].occ;
+        for (int ctas : {occ / 2, 1}) {
+            if (ctas < 1 || ctas >= occ) continue;
+            Compiled::Variant v = c.variants[0];
+            v.ms.clear();
+            v.ms_batch.clear();
+            v.ctas = ctas;
+            bool dup = false;
+            for (const Compiled::Variant &x : c.variants) dup = dup || (x.maxrreg == 0 && x.unroll == 0 && x.ctas == ctas);
+            if (!dup) c.variants.push_back(v);
         }
     }
 }
@@ -142,7 +162,7 @@ bool EngineCUDA::tune_launch(Compiled &c, const LaunchUnit &u, int64_t work, voi
     ensure_variants(c);
     if (c.variants.size() == 1) {
         c.tuned = true;
-        save_tune_choice(h, 0, 0);
+        save_tune_choice(h, 0, 0, 0);
         return false;
     }
     // The variant with the fewest timings runs next.
@@ -158,7 +178,7 @@ bool EngineCUDA::tune_launch(Compiled &c, const LaunchUnit &u, int64_t work, voi
         rec_e1 = b;
     }
     cudaStream_t s = static_cast<cudaStream_t>(_stream);
-    const int64_t grid = max<int64_t>(1, min<int64_t>(work, static_cast<int64_t>(_sm_count) * v.occ));
+    const int64_t grid = max<int64_t>(1, min<int64_t>(work, static_cast<int64_t>(_sm_count) * v.ctas_per_sm()));
     check_rt(cudaEventRecord(static_cast<cudaEvent_t>(rec_e0), s), "cudaEventRecord");
     if (launch_raw(v.fn, grid, args) != 0) throw runtime_error("cuLaunchKernel (tuning) failed for " + u.name);
     check_rt(cudaEventRecord(static_cast<cudaEvent_t>(rec_e1), s), "cudaEventRecord");
@@ -183,15 +203,15 @@ bool EngineCUDA::tune_launch(Compiled &c, const LaunchUnit &u, int64_t work, voi
         c.chosen = static_cast<int>(best);
         const Compiled::Variant &b = c.variants[best];
         c.fn = b.fn;
-        c.occ = b.occ;
+        c.occ = b.ctas_per_sm();
         if (!c.tuned_batch) {
             c.fn_batch = b.fn_batch;
             c.occ_batch = b.occ_batch;
         }
         c.tuned = true;
         ++_stats.tuned_kernels;
-        if (b.maxrreg > 0 || b.unroll > 0) ++_stats.tuned_capped;
-        save_tune_choice(h, b.maxrreg, b.unroll);
+        if (b.maxrreg > 0 || b.unroll > 0 || b.ctas > 0) ++_stats.tuned_capped;
+        save_tune_choice(h, b.maxrreg, b.unroll, b.ctas);
     }
     return true;
 }

@@ -5,6 +5,7 @@ views; 0-3 reductions).
     collect(ex, seeds)      run every DAG under several fusion plans with per-kernel timing on
                             and return the engine's records (features, device microseconds)
     train(X, t)             fit the cost model on the GPU (bohrium_b200.costmodel)
+    holdout_error(m, X, t)  R^2 and median |log error| of the model on records of other DAGs
     evaluate(ex, seeds)     per DAG: device time of a flush with the plain greedy plan and with
                             the learned engine (the greedy plan and the learned plan timed on the
                             device, the faster kept), plus a check that the outputs are identical
@@ -84,6 +85,16 @@ def collect(ex, seeds, max_elems: float = 2e7, variants=VARIANTS):
         return read_records(path)
     finally:
         os.unlink(path)
+
+
+def holdout_error(model: CostModel, X, t_us) -> dict:
+    """Prediction error of `model` on records it was not trained on: R^2 of the log device time
+    and the median |log(predicted / measured)|."""
+    y = np.log(np.maximum(np.asarray(t_us, dtype=np.float64), 1e-3))
+    p = np.log(np.maximum(model.predict_us(X), 1e-30))
+    ss_tot = float(np.sum((y - y.mean()) ** 2))
+    r2 = 1.0 - float(np.sum((y - p) ** 2)) / ss_tot if ss_tot > 0 else float("nan")
+    return {"records": int(len(y)), "r2": round(r2, 4), "median_abs_log_err": round(float(np.median(np.abs(y - p))), 4)}
 
 
 def train(X, t_us, epochs: int = 300, seed: int = 0) -> tuple[CostModel, float]:
