@@ -3203,7 +3203,8 @@ LaunchUnit lower_scan1d_single(const LoopB &loop, const InstrPtr &acc, const Cod
     const string T = cuda_type(t);
     const bh_opcode rop = scan_reduce_op(acc->opcode);
     const string ident = constant_literal(jitk::sweep_identity(rop, t));
-    auto op = [&](const string &a, const string &b) { return reduce_expr(rop, a, b); };
+    // Parenthesised: nested uses must keep their association (a op (b op c) is not (a op b) op c).
+    auto op = [&](const string &a, const string &b) { return "(" + reduce_expr(rop, a, b) + ")"; };
     LaunchUnit u;
     u.sched = Sched::SCAN1D;
     u.single_pass = true;

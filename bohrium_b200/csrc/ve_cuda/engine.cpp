@@ -236,10 +236,13 @@ void EngineCUDA::copyToDevice(bh_base *base) {
 }
 
 void *EngineCUDA::getBuffer(bh_base *base) {
-    copyToDevice(base);
-    DevBuf &b = buffers.at(base);
-    settle(b);
-    return b.ptr;
+    auto it = buffers.find(base);
+    if (it == buffers.end()) {
+        copyToDevice(base);
+        it = buffers.find(base);
+    }
+    settle(it->second);
+    return it->second.ptr;
 }
 
 void EngineCUDA::settle(DevBuf &b) {

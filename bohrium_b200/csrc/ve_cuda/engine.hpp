@@ -18,6 +18,7 @@
 #include <set>
 #include <string>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 #include <bohrium/bh_component.hpp>
 #include "../jitk/costmodel.hpp"
@@ -197,7 +198,7 @@ private:
     void eager_copy(bh_base *base);
     void settle(DevBuf &b);
     std::unordered_map<bh_base *, DevBuf> buffers;
-    std::set<bh_base *> host_stale; // device copy newer than the host copy
+    std::unordered_set<bh_base *> host_stale; // device copy newer than the host copy
     std::set<void *> pinned;        // host blocks from host_alloc()
     void *ev_begin = nullptr, *ev_end = nullptr, *tm_begin = nullptr, *tm_end = nullptr;
 
