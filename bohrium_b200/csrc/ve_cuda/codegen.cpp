@@ -3236,17 +3236,12 @@ __device__ __forceinline__ void bh_st_release(unsigned *p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
 // Poll *flag until it is set: false when `cap` polls ran out (at once for a negative cap) or
-// another CTA raised the abort flag. The shared abort flag is read every 64 polls only (every
-// waiting lane of the grid reading one word would make its L2 slice a hot spot), and the polls back
-// off from 32 to 512 ns.
+// another CTA raised the abort flag.
 __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *abort_flag, long long cap) {
     long long spins = 0;
-    unsigned ns = 32;
     while (bh_ld_acquire(flag) == 0u) {
-        if (cap < 0 || ++spins > cap) return false;
-        if ((spins & 63) == 0 && *(volatile const unsigned *)abort_flag != 0u) return false;
-        __nanosleep(ns);
-        if (ns < 512) ns <<= 1;
+        if (cap < 0 || ++spins > cap || bh_ld_acquire(abort_flag) != 0u) return false;
+        __nanosleep(32);  // fewer polls of L2 while the producer works
     }
     return true;
 }
@@ -3284,53 +3279,12 @@ __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *a
             }
         }
     }
-    // The read-only arrays that the instructions before the accumulate read: their elements of a
-    // chunk are loaded into registers (bh_prefetch) while the chunk before is still being finished,
-    // and the chunk's accumulate inputs are then computed from them at coalesced positions and
-    // staged (as unit A).
-    vector<bh_view> pf;
-    {
-        set<const bh_base *> written;
-        for (const InstrPtr &i : jitk::all_instr(L))
-            if (!i->operand.empty() && !i->operand[0].isConstant()) written.insert(i->operand[0].base);
-        set<ViewKey> seen;
-        for (const Block &b : L._block_list) {
-            const InstrPtr &i = b.getInstr();
-            if (i == acc) break;
-            const bh_opcode o = i->opcode;
-            if (bh_opcode_is_system(o) || o == BH_GATHER || o == BH_SCATTER || o == BH_COND_SCATTER || o == BH_RANGE ||
-                o == BH_RANDOM)
-                continue;
-            for (size_t k = 1; k < i->operand.size(); ++k) {
-                const bh_view &v = i->operand[k];
-                if (v.isConstant() || sym.temps.count(v.base) || written.count(v.base)) continue;
-                if (seen.insert(ViewKey(v)).second) pf.push_back(v);
-            }
-        }
-        if (pf.size() > 4) pf.clear();  // registers: at most 4 x 8 prefetched elements
-    }
-    string pf_params, pf_args;
-    for (size_t v = 0; v < pf.size(); ++v) {
-        pf_params += ", " + cuda_type(pf[v].base->dtype()) + " (&pf" + to_string(v) + ")[" + to_string(kScanPerThread) + "]";
-        pf_args += ", pf" + to_string(v);
-    }
-    body << "__device__ __forceinline__ void bh_prefetch(const P &p, bh_i64 c" << pf_params << ") {\n";
-    body << pointer_locals(sym);
-    body << "    const bh_i64 cbase = c * " << kScanTile << ";\n";
-    body << "#pragma unroll\n";
-    body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
-    body << "        const bh_i64 i0 = cbase + k * " << kThreads << " + (int)threadIdx.x;\n";
-    body << "        if (i0 < " << n0 << ") {\n";
-    for (size_t v = 0; v < pf.size(); ++v) body << "            pf" << v << "[k] = " << em.array_ref(pf[v]) << ";\n";
-    body << "        }\n";
-    body << "    }\n";
-    body << "}\n";
-    body << "__device__ __forceinline__ void bh_stage_in(const P &p, bh_i64 c, " << T << " *stage" << pf_params << ") {\n";
+    // Chunk c's accumulate inputs, computed at coalesced positions and staged (as unit A).
+    body << "__device__ __forceinline__ void bh_stage_in(const P &p, bh_i64 c, " << T << " *stage) {\n";
     body << pointer_locals(sym);
     body << "    const bh_i64 cbase = c * " << kScanTile << ";\n";
     {
         Scope scope;
-        for (size_t v = 0; v < pf.size(); ++v) scope.repl[ViewKey(pf[v])] = "pf" + to_string(v) + "[k]";
         body << "#pragma unroll\n";
         body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
         body << "        const int q = k * " << kThreads << " + (int)threadIdx.x;\n";
@@ -3344,7 +3298,6 @@ __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *a
         body << "        stage[q + (q >> 3)] = x;\n";
         body << "    }\n";
     }
-    body << "    (void)p;\n";
     body << "}\n";
     // Chunk c's scanned values from the stage to memory, then the instructions after the
     // accumulate (as unit C).
@@ -3432,15 +3385,12 @@ __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *a
     body << "    __shared__ " << T << " lb_carry;\n";
     body << "    __shared__ int lb_ok;\n";
     body << "    " << T << " xs[" << kScanPerThread << "];\n";
-    for (size_t v = 0; v < pf.size(); ++v)
-        body << "    " << cuda_type(pf[v].base->dtype()) << " pf" << v << "[" << kScanPerThread << "];\n";
-    body << R"CUDA(    if (threadIdx.x == 0) ticket = bh_ld_acquire(ctr + 2) != 0u ? p.nchunks : (bh_i64)atomicAdd(ctr, 1u);
-    __syncthreads();
-    bh_i64 c = ticket;
-    if (c < p.nchunks) bh_prefetch(p, c)CUDA" << pf_args << R"CUDA();
-    for (;;) {
+    body << R"CUDA(    for (;;) {
+        if (threadIdx.x == 0) ticket = bh_ld_acquire(ctr + 2) != 0u ? p.nchunks : (bh_i64)atomicAdd(ctr, 1u);
+        __syncthreads();
+        const bh_i64 c = ticket;
         if (c >= p.nchunks) break;
-        bh_stage_in(p, c, stage)CUDA" << pf_args << R"CUDA();
+        bh_stage_in(p, c, stage);
         __syncthreads();
 )CUDA";
     body << "        " << T << " total;\n";
@@ -3448,12 +3398,7 @@ __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *a
     body << R"CUDA(        if (threadIdx.x == 0) {
             totals[c] = total;
             bh_st_release(flags + c, 1u);
-            ticket = bh_ld_acquire(ctr + 2) != 0u ? p.nchunks : (bh_i64)atomicAdd(ctr, 1u);
         }
-        __syncthreads();
-        // The next chunk's loads go out before the look-back, which they overlap.
-        const bh_i64 cn = ticket;
-        if (cn < p.nchunks) bh_prefetch(p, cn)CUDA" << pf_args << R"CUDA();
         // Look back (warp 0; the other warps wait at the barrier below). Chunk c is entry k of
         // thread t = lane l of warp w of group g in unit B's scan of the chunk totals.
         if (threadIdx.x < 32) {
@@ -3540,7 +3485,6 @@ __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *a
     body << R"CUDA(        __syncthreads();
         bh_stage_out(p, c, stage);
         __syncthreads();  // stage reads before the next chunk's writes
-        c = cn;
     }
     // The CTA that leaves last: the fallback if any CTA gave up, then the reset for the next launch.
     __threadfence();
@@ -3551,8 +3495,7 @@ __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *a
     bh_acquire();
     if (bh_ld_acquire(ctr + 2) != 0u) {
         for (bh_i64 c = 0; c < p.nchunks; ++c) {
-            bh_prefetch(p, c)CUDA" << pf_args << R"CUDA();
-            bh_stage_in(p, c, stage)CUDA" << pf_args << R"CUDA();
+            bh_stage_in(p, c, stage);
             __syncthreads();
 )CUDA";
     body << "            " << T << " total;\n";
@@ -3585,8 +3528,7 @@ __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *a
     body << "        __threadfence_block();\n";
     body << "        __syncthreads();\n";
     body << "        for (bh_i64 c = 0; c < p.nchunks; ++c) {\n";
-    body << "            bh_prefetch(p, c" << pf_args << ");\n";
-    body << "            bh_stage_in(p, c, stage" << pf_args << ");\n";
+    body << "            bh_stage_in(p, c, stage);\n";
     body << "            __syncthreads();\n";
     body << "            " << T << " total;\n";
     body << "            const " << T << " e = bh_chunk_fold(p, c, stage, xs, total, sm);\n";
