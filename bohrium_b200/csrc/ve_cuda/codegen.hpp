@@ -150,7 +150,7 @@ struct CodegenOptions {
     int interleave = 1;         // GRID_REDUCE: elements of a heavy body written side by side (1 or 2)
     bool tile2d = true;         // TILE2D for maps over transposed views (else FLAT)
     bool vector_access = true;  // FLAT: 4 consecutive elements per thread, moved as 128-bit words
-    bool scan_single_pass = true; // SCAN1D as one pass with look-back (else three units)
+    bool scan_single_pass = false; // SCAN1D as one pass with look-back (else three units; see lower_scan1d_single)
     int64_t scan_spin_cap = int64_t{1} << 22; // polls per look-back wait (negative: give up at once)
 };
 

@@ -112,7 +112,7 @@ EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
     cg_opt.interleave = cfg.defaultGet<int>("interleave", 1);
     cg_opt.tile2d = cfg.defaultGet<bool>("tile2d", true);
     cg_opt.vector_access = cfg.defaultGet<bool>("vector_access", true);
-    cg_opt.scan_single_pass = cfg.defaultGet<bool>("scan_single_pass", true);
+    cg_opt.scan_single_pass = cfg.defaultGet<bool>("scan_single_pass", false);
     cg_opt.scan_spin_cap = cfg.defaultGet<int64_t>("scan_spin_cap", int64_t{1} << 22);
     // The GPU reduces over the outermost axis natively, so sweeps may fuse with maps at rank 0.
     fusion_config = jitk::FusionConfig(cfg, false);

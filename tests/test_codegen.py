@@ -150,19 +150,19 @@ def test_row_reductions_of_contiguous_rows_use_lanes():
     assert "lane_reduce" not in [u["sched"] for u in units]
 
 
-def test_one_dimensional_accumulate_lowers_to_one_pass_or_three_scan_units(monkeypatch):
-    """By default a 1-D accumulate is one single-pass unit (look-back with bounded waits and a
-    fallback); with scan_single_pass off it is the three units (chunk totals, carries, re-scan)."""
+def test_one_dimensional_accumulate_lowers_to_three_scan_units_or_one_pass(monkeypatch):
+    """By default a 1-D accumulate is the three units (chunk totals, carries, re-scan); with
+    scan_single_pass on it is one unit (look-back with bounded waits and a fallback)."""
     def prog(rt):
         a = bh.empty(rt, (100000,), np.float64)
         return [bh.accumulate("ADD_ACCUMULATE", a * 2.0 + 1.0, 0) * 3.0]
     res, units = plan(prog)
+    assert [u["sched"] for u in units] == ["scan1d", "scan1d", "scan1d"], [u["sched"] for u in units]
+    monkeypatch.setenv("BH_CUDA_SCAN_SINGLE_PASS", "true")
+    res, units = plan(prog)
     assert [u["sched"] for u in units] == ["scan1d"], [u["sched"] for u in units]
     src = units[0]["source"]
     assert "bh_await" in src and "p.spin_cap" in src and "atomicExch(ctr + 2, 1u)" in src
-    monkeypatch.setenv("BH_CUDA_SCAN_SINGLE_PASS", "false")
-    res, units = plan(prog)
-    assert [u["sched"] for u in units] == ["scan1d", "scan1d", "scan1d"], [u["sched"] for u in units]
 
 
 @pytest.mark.parametrize("dtype", [np.float64, np.int8, np.complex128])
@@ -183,17 +183,17 @@ def test_scan_units_stage_elements_at_coalesced_positions(dtype):
         return [c, c - x * dtype(3)]
 
     for prog in (kept, recomputed):
-        _, units = plan(prog)  # one pass: both stagings in the one unit
+        import os
+        os.environ["BH_CUDA_SCAN_SINGLE_PASS"] = "true"
+        try:
+            _, units = plan(prog)  # one pass: both stagings in the one unit
+        finally:
+            del os.environ["BH_CUDA_SCAN_SINGLE_PASS"]
         assert [u["sched"] for u in units] == ["scan1d"]
         src = units[0]["source"]
         assert "const int q = k * 256 + (int)threadIdx.x;" in src
         assert "stage[q + (q >> 3)] = x;" in src and "= stage[q + (q >> 3)];" in src
-        import os
-        os.environ["BH_CUDA_SCAN_SINGLE_PASS"] = "false"
-        try:
-            _, units = plan(prog)
-        finally:
-            del os.environ["BH_CUDA_SCAN_SINGLE_PASS"]
+        _, units = plan(prog)
         assert [u["sched"] for u in units] == ["scan1d"] * 3
         for phase in (0, 2):
             src = units[phase]["source"]

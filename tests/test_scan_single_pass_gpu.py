@@ -1,5 +1,6 @@
-"""The single-pass SCAN1D (chunk tickets, look-back over published chunk totals with bounded
-waits): bit-identical to the three-unit scan and to its order model, across repeated and graph-
+"""The single-pass SCAN1D (scan_single_pass = true; chunk tickets, look-back over published chunk
+totals with bounded waits): bit-identical to the three-unit scan (the default) and to its order
+model, across repeated and graph-
 replayed launches (its flags and counters reset themselves), and through its fallback, forced by
 a negative wait cap: every chunk that must wait gives up, and the CTA that leaves last redoes the
 whole scan alone."""
@@ -29,15 +30,15 @@ def _with(monkeypatch, **keys):
 @pytest.mark.parametrize("n,dtype", [(4_500_001, np.float64), (9_000_000, np.float32), (70_000, np.float64)])
 def test_single_pass_equals_three_units_and_model(gpu_rt, monkeypatch, n, dtype):
     x = np.random.default_rng(n).standard_normal(n).astype(dtype)
-    got = run(gpu_rt, _prog(x))
+    three = run(gpu_rt, _prog(x))  # the default: three units
+    ex = _with(monkeypatch, scan_single_pass="true", cache_dir="NONE")
+    try:
+        got = run(bh.Runtime(ex), _prog(x))
+    finally:
+        ex.close()
     want = scan1d_cumsum(x)
     assert np.asarray(got[0]).tobytes() == want.tobytes()
     assert np.asarray(got[1]).tobytes() == (want - x).tobytes()
-    ex = _with(monkeypatch, scan_single_pass="false", cache_dir="NONE")
-    try:
-        three = run(bh.Runtime(ex), _prog(x))
-    finally:
-        ex.close()
     for a, b in zip(got, three):
         assert np.asarray(a).tobytes() == np.asarray(b).tobytes()
 
@@ -48,7 +49,7 @@ def test_fallback_when_waits_give_up(monkeypatch, cap):
     its first unanswered poll (the fallback runs whenever a chunk found a predecessor not done)."""
     n = 3_000_017
     x = np.random.default_rng(5).standard_normal(n)
-    ex = _with(monkeypatch, scan_spin_cap=cap, cache_dir="NONE")
+    ex = _with(monkeypatch, scan_single_pass="true", scan_spin_cap=cap, cache_dir="NONE")
     try:
         rt = bh.Runtime(ex)
         for _ in range(3):  # the reset after a fallback leaves the next launch clean
@@ -60,9 +61,10 @@ def test_fallback_when_waits_give_up(monkeypatch, cap):
         ex.close()
 
 
-def test_repeated_and_graph_replayed_launches(gpu_executor):
+def test_repeated_and_graph_replayed_launches(monkeypatch):
     n = 5_000_000
     x = np.random.default_rng(9).standard_normal(n)
+    gpu_executor = _with(monkeypatch, scan_single_pass="true", cache_dir="NONE")
     rt = bh.Runtime(gpu_executor)
     a = bh.array(rt, x)
     rt.flush()
@@ -77,3 +79,5 @@ def test_repeated_and_graph_replayed_launches(gpu_executor):
                 assert gpu_executor.peek(c.base).tobytes() == want, mode
         finally:
             gpu_executor.message("CUDA: batch off")
+    del ir, c, a
+    gpu_executor.close()
