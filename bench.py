@@ -36,10 +36,19 @@ METRIC = "flush wall-time & HBM GB/s (%peak): batched+learned vs plain ve/cuda; 
 BS_OPTIONS = 10_000_000
 BS_ITERS = 10
 # DRAM bytes (read + written) per option of one Black-Scholes kernel launch, from an ncu capture
-# of a 6,000,000-option launch (dram__bytes_read.sum 144.08 MB + dram__bytes_write.sum 3.48 MB;
+# of a 6,000,000-option launch (dram__bytes_read.sum 144.08 MB + dram__bytes_write.sum 4.84 MB;
 # inputs of 144 MB, larger than L2): one pass over the three inputs plus the tile partials, so
 # the traffic grows in proportion to the options and is scaled to the launch's option count.
-BS_TRAFFIC_PER_OPTION = (144_082_176 + 3_477_504) / 6_000_000
+BS_TRAFFIC_PER_OPTION = (144_081_152 + 4_843_776) / 6_000_000
+# FP64 instructions per option of the same launch: sm__inst_executed_pipe_fp64.sum (28,608,514
+# warp instructions) x 32 lanes / 6,000,000 options. The same capture shows the FP64 pipe
+# 52.1 % busy over the kernel's active cycles (sm__inst_executed_pipe_fp64 pct_of_peak_sustained_active).
+BS_FP64_PER_OPTION = 28_608_514 * 32 / 6_000_000
+BS_FP64_PIPE_NCU = 0.521
+# FP64 lanes per SM per clock on B200: the capture's 193,301 FP64 warp instructions per SM at
+# 52.12 % of peak over 185,430 active cycles give 2.0 warp instructions (64 lanes) per cycle.
+FP64_LANES_PER_SM = 64
+SM_COUNT = 148
 
 
 # Warm-up executions of every extra workload before its timed ones: enough for the autotuner to
@@ -244,6 +253,16 @@ def run_ours(args, world, rank, local):
                 "peak_kind": peak_kind,
                 "kernel": "bh_grid_reduce (Black-Scholes flush)", "kernel_ms": round(avg_kernel_ms, 5),
                 "algorithmic_bytes_per_launch": bs_bytes(n)}
+    # The kernel's real ceiling is the FP64 pipe, not HBM: FP64 instructions per launch over the
+    # kernel time, against 64 lanes x 148 SMs at the SM clock sampled during the timed region.
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    fp64_achieved = BS_FP64_PER_OPTION * n / (avg_kernel_ms / 1e3) / 1e9
+    fp64_peak = FP64_LANES_PER_SM * SM_COUNT * mhz / 1e3
+    roofline["fp64"] = {"unit": "G FP64 lane-instructions/s", "per_option": round(BS_FP64_PER_OPTION, 1),
+                        "achieved": round(fp64_achieved, 1), "peak": round(fp64_peak, 1),
+                        "frac": round(fp64_achieved / fp64_peak, 4), "sm_mhz": mhz,
+                        "ncu_pipe_active_6e6": BS_FP64_PIPE_NCU,
+                        "source": "per-option count and pipe share from an ncu capture of a 6e6-option launch"}
     del irs, outs, inputs
 
     # ---- end to end through the C ABI with page-locked host buffers ---------------------

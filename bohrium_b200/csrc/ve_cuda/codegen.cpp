@@ -2539,6 +2539,11 @@ int grid_tiles_per_item(int64_t ntiles, const LoopB &L) {
             ++heavy;
     }
     if (n > 24 || heavy > 0) return 1;
+    // Small kernels (at most 64 tiles) take 4 tiles per item too: launched alone they are
+    // latency-bound either way, and in a grouped launch (many small arrays through the same
+    // kernel) every work item then keeps 4 tiles of loads in flight and pays one block reduction
+    // and one counter update for the 4.
+    if (ntiles <= 64) return 4;
     const int64_t resident = 148 * 4;
     if (ntiles >= 4 * 4 * resident) return 4;
     if (ntiles >= 2 * 2 * resident) return 2;
@@ -2685,77 +2690,124 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
             if (seen.insert(ViewKey(v)).second) wouts.push_back(v);
         }
     }
-    for (int path = 0; path < 2; ++path) {
-        body << (path == 0 ? "    if ((tile0 + " + to_string(K) + ") * " + to_string(kReduceTile) + " <= " + n0 + ") {\n"
-                           : "    } else {\n");
+    // Code pieces of the two paths. `k` is the (unrolled) tile index in the generated code.
+    auto emit_vec_check = [&](Emitter &eb) {
+        // Word alignment of every word-moved view: the same for every group of 4 elements of
+        // every tile, since a tile and a half-tile are whole multiples of 16 bytes.
+        body << "        bool vec = true;\n";
+        body << "        {\n";
+        body << "            const bh_i64 i0 = tile0 * " << kReduceTile << " + threadIdx.x * 4;\n";
+        for (size_t v = 0; v < pre.size(); ++v) {
+            if (!vec_pre[v]) continue;
+            const int bytes = min(16, 4 * static_cast<int>(bh_type_size(pre[v].base->dtype())));
+            body << "            vec = vec && (((unsigned long long)&" << eb.array_ref(pre[v]) << ") & " << bytes - 1
+                 << "ull) == 0;\n";
+        }
+        for (const bh_view &v : wouts) {
+            const int bytes = min(16, 4 * static_cast<int>(bh_type_size(v.base->dtype())));
+            body << "            vec = vec && (((unsigned long long)&" << eb.array_ref(v) << ") & " << bytes - 1
+                 << "ull) == 0;\n";
+        }
+        body << "        }\n";
+    };
+    auto emit_pl_decls = [&]() {
+        for (size_t v = 0; v < pre.size(); ++v)
+            body << "        " << cuda_type(pre[v].base->dtype()) << " pl" << v << "[" << K * kReduceV << "];\n";
+    };
+    // The read-only inputs of tile k's 8 elements per thread into pl*[k * 8 ...].
+    auto emit_preload_tile = [&](Emitter &eb, int ind) {
+        const string sp(static_cast<size_t>(ind), ' ');
+        if (vectorized) {
+            // Two words of 4 elements per view and tile: elements 4t..4t+3 and 1024+4t..1024+4t+3.
+            body << "#pragma unroll\n";
+            body << sp << "for (int g = 0; g < 2; ++g) {\n";
+            body << sp << "    const bh_i64 i0 = (tile0 + k) * " << kReduceTile << " + g * " << kReduceTile / 2
+                 << " + threadIdx.x * 4;\n";
+            for (size_t v = 0; v < pre.size(); ++v) {
+                const string dst = "&pl" + to_string(v) + "[k * " + to_string(kReduceV) + " + g * 4]";
+                const int bytes = 4 * static_cast<int>(bh_type_size(pre[v].base->dtype()));
+                if (vec_pre[v]) {
+                    body << sp << "    if (vec) { " << word_copy(dst, "&" + eb.array_ref(pre[v]), bytes) << "} else {\n";
+                } else {
+                    body << sp << "    {\n";
+                }
+                body << "#pragma unroll\n";
+                body << sp << "        for (int e = 0; e < 4; ++e) {\n";
+                body << sp << "            const bh_i64 i0e = i0 + e;\n";
+                body << sp << "            pl" << v << "[k * " << kReduceV << " + g * 4 + e] = "
+                     << regex_replace(eb.array_ref(pre[v]), regex("\\bi0\\b"), "i0e") << ";\n";
+                body << sp << "        }\n";
+                body << sp << "    }\n";
+            }
+            body << sp << "}\n";
+        } else {
+            body << "#pragma unroll\n";
+            body << sp << "for (int j = 0; j < " << kReduceV << "; ++j) {\n";
+            body << sp << "    const bh_i64 i0 = " << elem_index << ";\n";
+            for (size_t v = 0; v < pre.size(); ++v)
+                body << sp << "    pl" << v << "[k * " << kReduceV << " + j] = " << eb.array_ref(pre[v]) << ";\n";
+            body << sp << "}\n";
+        }
+    };
+    // Tile k's 8 elements per thread without bounds checks (inputs from pl*, written words through
+    // so*), then the written words.
+    auto emit_full_tile = [&](Emitter &eb, Scope &scope, int ind) {
+        const string sp(static_cast<size_t>(ind), ' ');
+        if (vectorized)
+            for (size_t m = 0; m < wouts.size(); ++m)
+                body << sp << cuda_type(wouts[m].base->dtype()) << " so" << m << "[" << kReduceV << "];\n";
+        body << "#pragma unroll\n";
+        body << sp << "for (int j = 0; j < " << kReduceV << "; ++j) {\n";
+        body << sp << "    const bh_i64 i0 = " << elem_index << ";\n";
+        eb.write_body(L, scope, ind + 4);
+        body << sp << "}\n";
+        if (vectorized) {
+            // The written arrays' words: 4 elements at 4t and 4 at 1024 + 4t.
+            body << "#pragma unroll\n";
+            body << sp << "for (int g = 0; g < 2; ++g) {\n";
+            body << sp << "    const bh_i64 i0 = (tile0 + k) * " << kReduceTile << " + g * " << kReduceTile / 2
+                 << " + threadIdx.x * 4;\n";
+            for (size_t m = 0; m < wouts.size(); ++m) {
+                const int bytes = 4 * static_cast<int>(bh_type_size(wouts[m].base->dtype()));
+                body << sp << "    if (vec) { " << word_copy("&" + eb.array_ref(wouts[m]), "&so" + to_string(m) + "[g * 4]", bytes)
+                     << "} else {\n";
+                body << "#pragma unroll\n";
+                body << sp << "        for (int e = 0; e < 4; ++e) {\n";
+                body << sp << "            const bh_i64 i0e = i0 + e;\n";
+                body << sp << "            " << regex_replace(eb.array_ref(wouts[m]), regex("\\bi0\\b"), "i0e")
+                     << " = so" << m << "[g * 4 + e];\n";
+                body << sp << "        }\n";
+                body << sp << "    }\n";
+            }
+            body << sp << "}\n";
+        }
+    };
+    auto full_tile_scope = [&](Scope &scope) {
+        for (size_t v = 0; v < pre.size(); ++v)
+            scope.repl[ViewKey(pre[v])] = "pl" + to_string(v) + "[k * " + to_string(kReduceV) + " + j]";
+        if (vectorized)
+            for (size_t m = 0; m < wouts.size(); ++m) scope.repl[ViewKey(wouts[m])] = "so" + to_string(m) + "[j]";
+    };
+    // Path 0: all K tiles of the item are full. Every input of all K x 8 elements of the thread is
+    // loaded first, then the tiles are computed.
+    {
+        body << "    if ((tile0 + " << K << ") * " << kReduceTile << " <= " << n0 << ") {\n";
         Scope scope;
         Emitter eb(sym, body, opt);
         eb.external_acc = acc_k;
-        if (path == 0 && vectorized) {
-            // Word alignment of every word-moved view (the same for every group of 4 elements).
-            body << "        bool vec = true;\n";
-            body << "        {\n";
-            body << "            const bh_i64 i0 = tile0 * " << kReduceTile << " + threadIdx.x * 4;\n";
-            for (size_t v = 0; v < pre.size(); ++v) {
-                if (!vec_pre[v]) continue;
-                const int bytes = min(16, 4 * static_cast<int>(bh_type_size(pre[v].base->dtype())));
-                body << "            vec = vec && (((unsigned long long)&" << eb.array_ref(pre[v]) << ") & " << bytes - 1
-                     << "ull) == 0;\n";
-            }
-            for (const bh_view &v : wouts) {
-                const int bytes = min(16, 4 * static_cast<int>(bh_type_size(v.base->dtype())));
-                body << "            vec = vec && (((unsigned long long)&" << eb.array_ref(v) << ") & " << bytes - 1
-                     << "ull) == 0;\n";
-            }
-            body << "        }\n";
-        }
-        if (path == 0 && !pre.empty()) {
-            for (size_t v = 0; v < pre.size(); ++v)
-                body << "        " << cuda_type(pre[v].base->dtype()) << " pl" << v << "[" << K * kReduceV << "];\n";
+        if (vectorized) emit_vec_check(eb);
+        if (!pre.empty()) {
+            emit_pl_decls();
             body << "#pragma unroll\n";
             body << "        for (int k = 0; k < " << K << "; ++k) {\n";
-            if (vectorized) {
-                // Two words of 4 elements per view and tile: elements 4t..4t+3 and 1024+4t..1024+4t+3.
-                body << "#pragma unroll\n";
-                body << "            for (int g = 0; g < 2; ++g) {\n";
-                body << "                const bh_i64 i0 = (tile0 + k) * " << kReduceTile << " + g * " << kReduceTile / 2
-                     << " + threadIdx.x * 4;\n";
-                for (size_t v = 0; v < pre.size(); ++v) {
-                    const string dst = "&pl" + to_string(v) + "[k * " + to_string(kReduceV) + " + g * 4]";
-                    const int bytes = 4 * static_cast<int>(bh_type_size(pre[v].base->dtype()));
-                    if (vec_pre[v]) {
-                        body << "                if (vec) { " << word_copy(dst, "&" + eb.array_ref(pre[v]), bytes) << "} else {\n";
-                    } else {
-                        body << "                {\n";
-                    }
-                    body << "#pragma unroll\n";
-                    body << "                    for (int e = 0; e < 4; ++e) {\n";
-                    body << "                        const bh_i64 i0e = i0 + e;\n";
-                    body << "                        pl" << v << "[k * " << kReduceV << " + g * 4 + e] = "
-                         << regex_replace(eb.array_ref(pre[v]), regex("\\bi0\\b"), "i0e") << ";\n";
-                    body << "                    }\n";
-                    body << "                }\n";
-                }
-                body << "            }\n";
-            } else {
-                body << "#pragma unroll\n";
-                body << "            for (int j = 0; j < " << kReduceV << "; ++j) {\n";
-                body << "                const bh_i64 i0 = " << elem_index << ";\n";
-                for (size_t v = 0; v < pre.size(); ++v)
-                    body << "                pl" << v << "[k * " << kReduceV << " + j] = " << eb.array_ref(pre[v]) << ";\n";
-                body << "            }\n";
-            }
+            emit_preload_tile(eb, 12);
             body << "        }\n";
-            for (size_t v = 0; v < pre.size(); ++v)
-                scope.repl[ViewKey(pre[v])] = "pl" + to_string(v) + "[k * " + to_string(kReduceV) + " + j]";
         }
-        if (path == 0 && vectorized)
-            for (size_t m = 0; m < wouts.size(); ++m) scope.repl[ViewKey(wouts[m])] = "so" + to_string(m) + "[j]";
+        full_tile_scope(scope);
         // k always runs to the constant K (unrolled), so the accumulator slots stay registers.
         body << "#pragma unroll\n";
         body << "        for (int k = 0; k < " << K << "; ++k) {\n";
-        if (path == 1) body << "            if (k >= ktiles) break;\n";
-        if (path == 0 && heavy && opt.interleave == 2) {
+        if (heavy && opt.interleave == 2) {
             // Two elements per step, statement by statement (elements j and j + 1; reductions
             // still fold j before j + 1): independent chains side by side for the scheduler.
             body << "#pragma unroll\n";
@@ -2768,38 +2820,43 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
             e1.write_body(L, scope, 16);
             body << interleave_second_element(one.str());
             body << "            }\n";
-            body << "        }\n";
-            continue;
+        } else {
+            emit_full_tile(eb, scope, 12);
         }
-        if (path == 0 && vectorized)
-            for (size_t m = 0; m < wouts.size(); ++m)
-                body << "            " << cuda_type(wouts[m].base->dtype()) << " so" << m << "[" << kReduceV << "];\n";
-        if (path == 0) body << "#pragma unroll\n";
-        body << "            for (int j = 0; j < " << kReduceV << "; ++j) {\n";
-        body << "                const bh_i64 i0 = " << elem_index << ";\n";
-        if (path == 1) body << "                if (i0 >= " << n0 << ") break;\n";
-        eb.write_body(L, scope, 16);
-        body << "            }\n";
-        if (path == 0 && vectorized) {
-            // The written arrays' words: 4 elements at 4t and 4 at 1024 + 4t.
-            body << "#pragma unroll\n";
-            body << "            for (int g = 0; g < 2; ++g) {\n";
-            body << "                const bh_i64 i0 = (tile0 + k) * " << kReduceTile << " + g * " << kReduceTile / 2
-                 << " + threadIdx.x * 4;\n";
-            for (size_t m = 0; m < wouts.size(); ++m) {
-                const int bytes = 4 * static_cast<int>(bh_type_size(wouts[m].base->dtype()));
-                body << "                if (vec) { " << word_copy("&" + eb.array_ref(wouts[m]), "&so" + to_string(m) + "[g * 4]", bytes)
-                     << "} else {\n";
-                body << "#pragma unroll\n";
-                body << "                    for (int e = 0; e < 4; ++e) {\n";
-                body << "                        const bh_i64 i0e = i0 + e;\n";
-                body << "                        " << regex_replace(eb.array_ref(wouts[m]), regex("\\bi0\\b"), "i0e")
-                     << " = so" << m << "[g * 4 + e];\n";
-                body << "                    }\n";
-                body << "                }\n";
-            }
+        body << "        }\n";
+    }
+    // Path 1: the last work item. Its full tiles (kfull of them) take the same code as path 0,
+    // one tile at a time; the partial tile checks every index. Both fold elements j = 0..7 of
+    // tile k into slot k in order, as path 0 does.
+    {
+        body << "    } else {\n";
+        Emitter eb(sym, body, opt);
+        eb.external_acc = acc_k;
+        if (K > 1) {
+            body << "        const bh_i64 nfull = " << n0 << " / " << kReduceTile << " - tile0;\n";
+            body << "        const int kfull = (int)(nfull < 0 ? 0 : (nfull < ktiles ? nfull : ktiles));\n";
+            if (vectorized) emit_vec_check(eb);
+            if (!pre.empty()) emit_pl_decls();
+        }
+        body << "#pragma unroll\n";
+        body << "        for (int k = 0; k < " << K << "; ++k) {\n";
+        body << "            if (k >= ktiles) break;\n";
+        int ind = 12;
+        if (K > 1) {
+            body << "            if (k < kfull) {\n";
+            Scope fscope;
+            full_tile_scope(fscope);
+            if (!pre.empty()) emit_preload_tile(eb, 16);
+            emit_full_tile(eb, fscope, 16);
+            body << "                continue;\n";
             body << "            }\n";
         }
+        Scope scope;
+        body << string(static_cast<size_t>(ind), ' ') << "for (int j = 0; j < " << kReduceV << "; ++j) {\n";
+        body << string(static_cast<size_t>(ind), ' ') << "    const bh_i64 i0 = " << elem_index << ";\n";
+        body << string(static_cast<size_t>(ind), ' ') << "    if (i0 >= " << n0 << ") break;\n";
+        eb.write_body(L, scope, ind + 4);
+        body << string(static_cast<size_t>(ind), ' ') << "}\n";
         body << "        }\n";
     }
     body << "    }\n";
@@ -2980,17 +3037,43 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
     const string T = cuda_type(t);
     const bh_opcode rop = scan_reduce_op(acc->opcode);
     const string ident = constant_literal(jitk::sweep_identity(rop, t));
+    // Windowed (scan_windows, off by default): one group of chunks at a time, unit A then unit C,
+    // so that the re-scan finds the group's inputs still in L2 (a group is 2048 chunks, 4M
+    // elements: 32 MB of float64) and each input element crosses HBM once. On a B200 it measured
+    // slower than the whole-length units (0.52 against 0.28 ms for 5e7 float64: two launches and
+    // a group scan on every CTA's critical path per 32 MB window). Every CTA of the windowed unit C repeats
+    // unit B's scan of its group's chunk totals (16 KB, read from L2) and takes its own chunk's
+    // carry from it; the CTA of the group's first chunk stores the group's total and carry, which
+    // the next group's launch reads. The operations and their association are those of the three
+    // units, so the results are bit-identical.
+    const bool windowed = opt.scan_windows;
+    struct Step {
+        int phase;
+        int64_t first, work;  // first work item (chunk, or group for unit B) and item count
+    };
+    vector<Step> steps;
+    if (windowed) {
+        for (int64_t g = 0; g < ngroups; ++g) {
+            const int64_t first = g * kScanTile, cnt = min<int64_t>(kScanTile, nchunks - first);
+            steps.push_back({0, first, cnt});
+            steps.push_back({2, first, cnt});
+        }
+    } else {
+        steps = {{0, 0, nchunks}, {1, 0, ngroups}, {2, 0, nchunks}};
+    }
     vector<LaunchUnit> units;
-    for (int phase = 0; phase < 3; ++phase) {
+    for (const Step &st : steps) {
+        const int phase = st.phase;
         LaunchUnit u;
         u.sched = Sched::SCAN1D;
         u.cols = n;
-        u.chunks = phase == 1 ? ngroups : nchunks;  // work items
+        u.chunks = st.work;  // work items
         Symbols sym = build_symbols({&holder}, {});
         ParamLayout pl;
         add_common_fields(sym, pl, opt);
         pl.add(work_field(nchunks), "bh_i64", "nchunks");
-        pl.add(work_field(phase == 1 ? ngroups : nchunks), "bh_i64", "work");
+        pl.add(work_field(st.work), "bh_i64", "work");
+        pl.add(work_field(st.first), "bh_i64", "first");
         ParamField fs{ParamField::SCRATCH};
         pl.add(fs, "unsigned char*", "scratch");
         if (phase == 1) {
@@ -3001,7 +3084,15 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
         stringstream body;
         Emitter em(sym, body, opt);
         body << block_scan_fn(T, "bh_block_scan", rop, ident);
-        body << "__device__ void bh_work(const P &p, bh_i64 c) {\n";
+        body << "__device__ void bh_work(const P &p, bh_i64 w) {\n";
+        if (phase == 2 && !windowed) {
+            // The re-scan walks the chunks from the last one down: unit A read them first to
+            // last, so the ones it read last are still in L2 when the re-scan starts. Chunks are
+            // independent here (each has its carry), so the order changes no result.
+            body << "    const bh_i64 c = p.nchunks - 1 - (p.first + w);\n";
+        } else {
+            body << "    const bh_i64 c = p.first + w;\n";
+        }
         body << pointer_locals(sym);
         body << "    __shared__ " << T << " sm[" << 2 * (kThreads / 32) + 1 << "];\n";
         body << "    " << T << "* totals = (" << T << "*)p.scratch;\n";
@@ -3030,7 +3121,7 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
             // and stores the group total; the CTA that finishes last folds the group totals in
             // group order into the carry of every group.
             body << "    " << T << "* gtot = carries + p.nchunks;\n";
-            body << "    " << T << "* grun = gtot + p.work;\n";
+            body << "    " << T << "* grun = gtot + (p.nchunks + " << kScanTile - 1 << ") / " << kScanTile << ";\n";
             body << "    __shared__ bool am_last;\n";
             body << "    const bh_i64 base = c * " << kScanTile << ";\n";
             body << "    " << T << " v[" << kScanPerThread << "];\n";
@@ -3130,10 +3221,49 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
                 body << "    if (threadIdx.x == 0) totals[c] = total;\n";
                 body << "}\n" << kWrappers;
             } else {
-                body << "    const " << T << "* grun = carries + p.nchunks + (p.nchunks + " << kScanTile - 1 << ") / "
-                     << kScanTile << ";\n";
-                body << "    const " << T << " carry = " << reduce_expr(rop, "grun[c / " + to_string(kScanTile) + "]", "carries[c]")
-                     << ";\n";
+                if (!windowed) {
+                    body << "    const " << T << "* grun = carries + p.nchunks + (p.nchunks + " << kScanTile - 1 << ") / "
+                         << kScanTile << ";\n";
+                    body << "    const " << T << " carry = " << reduce_expr(rop, "grun[c / " + to_string(kScanTile) + "]", "carries[c]")
+                         << ";\n";
+                } else {
+                    // Unit B's steps for this chunk's group: thread t folds chunk totals 8t..8t+7 of
+                    // the group (v: its exclusive running prefixes), a block scan of the thread sums,
+                    // and the group's carry from the previous group's carry and total.
+                    body << "    " << T << "* gtot = carries + p.nchunks;\n";
+                    body << "    " << T << "* grun = gtot + (p.nchunks + " << kScanTile - 1 << ") / " << kScanTile << ";\n";
+                    body << "    __shared__ " << T << " chunk_carry;\n";
+                    body << "    const bh_i64 g = c / " << kScanTile << ", gbase = g * " << kScanTile << ";\n";
+                    body << "    " << T << " gv[" << kScanPerThread << "];\n";
+                    body << "    " << T << " gs = " << ident << ";\n";
+                    body << "#pragma unroll\n";
+                    body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
+                    body << "        const bh_i64 j = gbase + threadIdx.x * " << kScanPerThread << " + k;\n";
+                    body << "        gv[k] = gs;\n";
+                    body << "        if (j < p.nchunks) { const " << T << " x = totals[j]; gs = " << reduce_expr(rop, "gs", "x")
+                         << "; }\n";
+                    body << "    }\n";
+                    body << "    " << T << " gtotal;\n";
+                    body << "    const " << T << " ge = bh_block_scan(gs, gtotal, sm);\n";
+                    body << "    const " << T << " run = g == 0 ? " << ident << " : " << reduce_expr(rop, "grun[g - 1]", "gtot[g - 1]")
+                         << ";\n";
+                    body << "    {\n";
+                    body << "        const int own = (int)(c - gbase);\n";
+                    body << "        if ((int)threadIdx.x == own / " << kScanPerThread << ") {\n";
+                    body << "            " << T << " v = gv[0];\n";
+                    body << "#pragma unroll\n";
+                    body << "            for (int k = 1; k < " << kScanPerThread << "; ++k) if (k == own % " << kScanPerThread
+                         << ") v = gv[k];\n";
+                    body << "            chunk_carry = " << reduce_expr(rop, "run", "(" + reduce_expr(rop, "ge", "v") + ")") << ";\n";
+                    body << "        }\n";
+                    body << "        if (c == gbase && threadIdx.x == 0) {\n";
+                    body << "            gtot[g] = gtotal;\n";
+                    body << "            grun[g] = run;\n";
+                    body << "        }\n";
+                    body << "    }\n";
+                    body << "    __syncthreads();\n";
+                    body << "    const " << T << " carry = chunk_carry;\n";
+                }
                 body << "    " << T << " r = " << ident << ";\n";
                 body << "#pragma unroll\n";
                 body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
@@ -3170,8 +3300,12 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
         u.scratch_bytes_per_tile = 0;
         // chunk totals, chunk carries, group totals, group carries
         u.scan_bytes = 2 * (nchunks + ngroups) * static_cast<int64_t>(bh_type_size(t));
-        u.algorithmic_bytes = phase == 2 ? unit_bytes(sym, vector<const Block *>{&holder}) : 0;
-        u.elements = phase == 1 ? nchunks : n;
+        // The whole scan's bytes go to its last unit; a window's units share them by elements.
+        const int64_t all_bytes = phase == 2 ? unit_bytes(sym, vector<const Block *>{&holder}) : 0;
+        const int64_t elems = phase == 1 ? st.work : min<int64_t>(n, (st.first + st.work) * kScanTile) - st.first * kScanTile;
+        u.algorithmic_bytes = windowed ? static_cast<int64_t>(static_cast<double>(all_bytes) * elems / max<int64_t>(n, 1))
+                                       : all_bytes;
+        u.elements = elems;
         if (phase == 2) u.red_orders.emplace_back(acc->origin_id, "scan:" + to_string(kScanTile) + ":" + to_string(n));
         finish_source(u, pl.decl.str(), body.str(), opt);
         units.push_back(std::move(u));

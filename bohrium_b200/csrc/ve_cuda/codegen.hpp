@@ -30,6 +30,9 @@
 //   SCAN1D        a 1-D nest with one accumulate (cumulative sum/product) among elementwise
 //                 instructions: three units -- chunk totals, one-CTA exclusive scan of the totals,
 //                 re-scan with the carry -- each with a fixed block scan (order set by the length).
+//                 The re-scan walks the chunks last to first (the ones A read last are in L2).
+//                 With scan_windows, A and C run one group of 2048 chunks at a time (C repeating
+//                 B's steps for its group), so the re-scan reads the group's inputs from L2.
 //   SERIAL        anything else: one thread runs the nest in program order (always correct).
 //   TILE2D        a 2-D map that reads arrays through transposed views (unit stride along the outer
 //                 rank): tiles of (128 bytes / element) rows x 64 columns; each transposed view's
@@ -151,6 +154,7 @@ struct CodegenOptions {
     bool tile2d = true;         // TILE2D for maps over transposed views (else FLAT)
     bool vector_access = true;  // FLAT: 4 consecutive elements per thread, moved as 128-bit words
     bool scan_single_pass = false; // SCAN1D as one pass with look-back (else three units; see lower_scan1d_single)
+    bool scan_windows = false;     // SCAN1D units A and C one group of chunks at a time (see lower_scan1d)
     int64_t scan_spin_cap = int64_t{1} << 22; // polls per look-back wait (negative: give up at once)
 };
 

@@ -1,6 +1,7 @@
 // Device-free inspection of the engine's lowering: fuse a BhIR, generate the kernel sources and
 // optionally compile them with NVRTC for sm_100a. Used by the CPU test-suite to check every code
 // path up to the launch on a machine without a GPU.
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <set>
@@ -28,7 +29,14 @@ string json_escape(const string &s) {
             case '\\': r += "\\\\"; break;
             case '\n': r += "\\n"; break;
             case '\t': r += "\\t"; break;
-            default: r += c;
+            default:
+                if (static_cast<unsigned char>(c) < 0x20) {
+                    char buf[8];
+                    snprintf(buf, sizeof buf, "\\u%04x", static_cast<unsigned>(static_cast<unsigned char>(c)));
+                    r += buf;
+                } else {
+                    r += c;
+                }
         }
     }
     return r;
@@ -100,6 +108,7 @@ extern "C" const char *bh_ve_cuda_dry_run(bhb_ir *handle, int compile, const cha
         if (const char *v = getenv("BH_CUDA_TILE2D")) opt.tile2d = string(v) == "true" || string(v) == "1";
         if (const char *v = getenv("BH_CUDA_VECTOR_ACCESS")) opt.vector_access = string(v) == "true" || string(v) == "1";
         if (const char *v = getenv("BH_CUDA_SCAN_SINGLE_PASS")) opt.scan_single_pass = string(v) == "true" || string(v) == "1";
+        if (const char *v = getenv("BH_CUDA_SCAN_WINDOWS")) opt.scan_windows = string(v) == "true" || string(v) == "1";
         vector<vector<cuda::LaunchUnit>> lowered(kernels.size());
         for (size_t k = 0; k < kernels.size(); ++k)
             if (!kernels[k].isSystemOnly()) lowered[k] = cuda::lower_kernel(kernels[k], opt);

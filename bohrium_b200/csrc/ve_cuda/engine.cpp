@@ -113,6 +113,7 @@ EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
     cg_opt.tile2d = cfg.defaultGet<bool>("tile2d", true);
     cg_opt.vector_access = cfg.defaultGet<bool>("vector_access", true);
     cg_opt.scan_single_pass = cfg.defaultGet<bool>("scan_single_pass", false);
+    cg_opt.scan_windows = cfg.defaultGet<bool>("scan_windows", false);
     cg_opt.scan_spin_cap = cfg.defaultGet<int64_t>("scan_spin_cap", int64_t{1} << 22);
     // The GPU reduces over the outermost axis natively, so sweeps may fuse with maps at rank 0.
     fusion_config = jitk::FusionConfig(cfg, false);
@@ -168,6 +169,10 @@ EngineCUDA::~EngineCUDA() {
     try {
         if (_copy_stream) cudaStreamSynchronize(static_cast<cudaStream_t>(_copy_stream));
         cudaStreamSynchronize(static_cast<cudaStream_t>(_stream));
+        // Replays own CUDA graphs and device memory, and a graph's clean-up synchronises the
+        // engine's stream: release them while that stream still exists (members are destroyed
+        // only after this body has destroyed it).
+        replays.clear();
         for (auto &kv : buffers) {
             if (kv.second.arrival) cudaEventDestroy(static_cast<cudaEvent_t>(kv.second.arrival));
             if (kv.second.ptr) cudaFree(kv.second.ptr);
@@ -905,8 +910,12 @@ int EngineCUDA::launch_raw(void *fn, int64_t grid, void **args) {
                                                 args, nullptr));
 }
 
+EngineCUDA::PackCache::~PackCache() {
+    if (dev) cudaFree(dev);  // waits for the launches that read it
+}
+
 void EngineCUDA::launch_batched(const vector<const PlanUnit *> &group, const vector<bh_base *> &bases,
-                                const vector<bh_instruction *> &instrs) {
+                                const vector<bh_instruction *> &instrs, PackCache *cache) {
     const PlanUnit &proto = *group[0];
     const size_t psize = proto.unit.fields.size() * 8;
     const size_t n = group.size();
@@ -924,28 +933,61 @@ void EngineCUDA::launch_batched(const vector<const PlanUnit *> &group, const vec
     // Items (parameter structs) followed by the prefix sums of their work counts.
     const size_t items_bytes = (psize * n + 15) / 16 * 16;
     const size_t bytes = items_bytes + (n + 1) * sizeof(int64_t);
-    uint8_t *host = staging_alloc(bytes);
-    int64_t *prefix = reinterpret_cast<int64_t *>(host + items_bytes);
+    uint8_t *dev = nullptr;
     int64_t total = 0;
-    packing_grouped = true;  // tensor maps need the plain kernel's parameter space
-    for (size_t k = 0; k < n; ++k) {
-        pack_params(*group[k], bases, instrs, scratch_off[k], counter_off[k], host + k * psize);
-        prefix[k] = total;
-        total += group[k]->unit.work_items();
+    if (cache && cache->dev && cache->n == n && cache->bytes == bytes && cache->epoch == buffer_epoch &&
+        cache->scratch == scratch && cache->counters == counters && cache->scan_arena == scan_arena) {
+        // The same items as last time, already on the device.
+        dev = cache->dev;
+        total = cache->total;
+        ++_stats.pack_reuses;
+    } else {
+        uint8_t *host = staging_alloc(bytes);
+        int64_t *prefix = reinterpret_cast<int64_t *>(host + items_bytes);
+        packing_grouped = true;  // tensor maps need the plain kernel's parameter space
+        for (size_t k = 0; k < n; ++k) {
+            pack_params(*group[k], bases, instrs, scratch_off[k], counter_off[k], host + k * psize);
+            prefix[k] = total;
+            total += group[k]->unit.work_items();
+        }
+        packing_grouped = false;
+        prefix[n] = total;
+        if (total == 0) return;
+        if (cache) {
+            if (cache->capacity < bytes) {
+                if (cache->dev) {
+                    synchronize();
+                    check(cudaFree(cache->dev), "cudaFree(pack cache)");
+                    cache->dev = nullptr;
+                }
+                void *p = nullptr;
+                check(cudaMalloc(&p, bytes), "cudaMalloc(pack cache)");
+                cache->dev = static_cast<uint8_t *>(p);
+                cache->capacity = bytes;
+            }
+            dev = cache->dev;
+            cache->n = n;
+            cache->bytes = bytes;
+            cache->items_bytes = items_bytes;
+            cache->total = total;
+            cache->epoch = buffer_epoch;  // after any buffer the packing allocated
+            cache->scratch = scratch;
+            cache->counters = counters;
+            cache->scan_arena = scan_arena;
+        } else {
+            dev = device_staging(bytes);
+        }
+        check(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, static_cast<cudaStream_t>(_stream)),
+              "cudaMemcpyAsync(batch items)");
+        if (!staging_event) {
+            cudaEvent_t e;
+            check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+            staging_event = e;
+        }
+        check(cudaEventRecord(static_cast<cudaEvent_t>(staging_event), static_cast<cudaStream_t>(_stream)),
+              "cudaEventRecord(staging)");
     }
-    packing_grouped = false;
-    prefix[n] = total;
     if (total == 0) return;
-    uint8_t *dev = device_staging(bytes);
-    check(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, static_cast<cudaStream_t>(_stream)),
-          "cudaMemcpyAsync(batch items)");
-    if (!staging_event) {
-        cudaEvent_t e;
-        check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
-        staging_event = e;
-    }
-    check(cudaEventRecord(static_cast<cudaEvent_t>(staging_event), static_cast<cudaStream_t>(_stream)),
-          "cudaEventRecord(staging)");
     void *items_ptr = dev;
     void *prefix_ptr = dev + items_bytes;
     int nitems = static_cast<int>(n);
@@ -1230,6 +1272,24 @@ EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const
         _stats.time_codegen += seconds_since(tc);
         precompile(all);
     }
+    // Register temporaries: arrays this flush creates that no unit addresses in memory. They never
+    // get a buffer or host data, so their writes and frees need no bookkeeping and make no
+    // dependencies between kernels.
+    vector<char> in_memory(base_ids.size(), 0), created(base_ids.size(), 0);
+    for (const vector<LaunchUnit> &units : lowered)
+        for (const LaunchUnit &u : units)
+            for (const ParamField &f : u.fields)
+                if ((f.kind == ParamField::PTR || f.kind == ParamField::TMAP) && f.base != nullptr) {
+                    const int b = idx(f.base);
+                    if (b >= 0) in_memory[static_cast<size_t>(b)] = 1;
+                }
+    for (const LoopB &kernel : kernels)
+        for (const InstrPtr &instr : all_instr(kernel))
+            if (instr->constructor && !instr->operand.empty() && !instr->operand[0].isConstant()) {
+                const int b = idx(instr->operand[0].base);
+                if (b >= 0) created[static_cast<size_t>(b)] = 1;
+            }
+    auto register_temp = [&](int b) { return created[static_cast<size_t>(b)] && !in_memory[static_cast<size_t>(b)]; };
     for (size_t kidx = 0; kidx < kernels.size(); ++kidx) {
         if (folded_into[kidx] >= 0) continue;  // runs in the tail of an earlier kernel
         const LoopB &kernel = kernels[kidx];
@@ -1265,7 +1325,7 @@ EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const
                     const bh_view &v = instr->operand[o];
                     if (v.isConstant()) continue;
                     const int b = idx(v.base);
-                    if (b < 0) continue;
+                    if (b < 0 || register_temp(b)) continue;
                     if (o == 0) {
                         writes.insert(b);
                     } else {
@@ -1275,7 +1335,7 @@ EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const
             }
             for (bh_base *f : part->getAllFrees()) {
                 const int b = idx(f);
-                if (b >= 0) {
+                if (b >= 0 && !register_temp(b)) {
                     pk.frees.push_back(b);
                     writes.insert(b);
                 }
@@ -1316,19 +1376,25 @@ EngineCUDA::FlushPlan EngineCUDA::build_plan(const vector<LoopB> &kernels, const
     return plan;
 }
 
-void EngineCUDA::run_plan(const FlushPlan &plan, const vector<bh_base *> &bases, const vector<bh_instruction *> &instrs) {
+void EngineCUDA::run_plan(const FlushPlan &plan, const vector<bh_base *> &bases, const vector<bh_instruction *> &instrs,
+                          Replay *replay) {
     if (plan.scan_bytes > 0) ensure_scan_arena(plan.scan_bytes);
     if (record) {
         record_kernel_times(plan, bases, instrs);
         return;
     }
+    // A replay whose writes are all still in host_stale (nothing was removed from it since its
+    // last run) need not insert them again.
+    const bool stale_known = replay != nullptr && replay->stale_after == stale_epoch;
     if (batch_mode == "off" || plan.kernels.size() < 2) {
         for (const PlanKernel &pk : plan.kernels) {
             ++_stats.kernels;
             for (const PlanUnit &pu : pk.units) launch_plain(pu, bases, instrs);
-            for (int w : pk.writes) host_stale.insert(bases[static_cast<size_t>(w)]);
+            if (!stale_known)
+                for (int w : pk.writes) host_stale.insert(bases[static_cast<size_t>(w)]);
             for (int f : pk.frees) free_base(bases[static_cast<size_t>(f)]);
         }
+        if (replay) replay->stale_after = stale_epoch;
         return;
     }
     // Grouped execution: level by level, units of the same compiled kernel run as one launch.
@@ -1351,14 +1417,22 @@ void EngineCUDA::run_plan(const FlushPlan &plan, const vector<bh_base *> &bases,
             if (g.size() == 1 || g[0]->unit.no_batch) {
                 for (const PlanUnit *pu : g) launch_plain(*pu, bases, instrs);
             } else {
-                launch_batched(g, bases, instrs);
+                PackCache *pc = nullptr;
+                if (replay) {
+                    unique_ptr<PackCache> &slot = replay->packs[{lv, c}];
+                    if (!slot) slot.reset(new PackCache());
+                    pc = slot.get();
+                }
+                launch_batched(g, bases, instrs, pc);
             }
         }
         for (const PlanKernel *pk : kernels_by_end[lv]) {
-            for (int w : pk->writes) host_stale.insert(bases[static_cast<size_t>(w)]);
+            if (!stale_known)
+                for (int w : pk->writes) host_stale.insert(bases[static_cast<size_t>(w)]);
             for (int f : pk->frees) free_base(bases[static_cast<size_t>(f)]);
         }
     }
+    if (replay) replay->stale_after = stale_epoch;
 }
 
 void EngineCUDA::handleExecution(BhIR *bhir) {
@@ -1370,9 +1444,11 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
         // A graph replay whose arrays and host copies are untouched since its last launch needs
         // no checks at all.
         const bool graph_mode = batch_mode == "graph" && !prof && !record;
-        const bool unchanged = rit != replays.end() && graph_mode && rit->second.graph &&
-                               rit->second.checked_epoch == buffer_epoch;
-        if (rit != replays.end() && (unchanged || replay_valid(rit->second))) {
+        // No buffer or host pointer changed since a replay that changed none itself: its checks
+        // would find what they found then.
+        const bool same_state = rit != replays.end() && rit->second.checked_epoch == buffer_epoch;
+        const bool unchanged = same_state && graph_mode && rit->second.graph;
+        if (rit != replays.end() && (same_state || replay_valid(rit->second))) {
             Replay &r = rit->second;
             for (bh_base *b : r.dead) free_base(b);
             const auto t1 = chrono::steady_clock::now();
@@ -1398,7 +1474,9 @@ void EngineCUDA::handleExecution(BhIR *bhir) {
             staging_used = 0;
             ++_stats.plan_cache_hits;
             ++_stats.replays;
-            run_plan(*r.plan, r.base_ids, r.instrs);
+            const uint64_t epoch0 = buffer_epoch;
+            run_plan(*r.plan, r.base_ids, r.instrs, &r);
+            r.checked_epoch = buffer_epoch == epoch0 ? buffer_epoch : 0;
             _stats.time_launch += seconds_since(t1);
             copyToHost(bhir->_syncs, false);
             check_error_record();
@@ -1698,7 +1776,7 @@ string EngineCUDA::statistics() const {
        << "\nkernel_cache_misses: " << _stats.kernel_cache_misses << "\ndisk_cache_hits: " << _stats.disk_cache_hits
        << "\ndisk_cache_rejected: " << _stats.disk_cache_rejected
        << "\nfma_contractions: " << _stats.fma_contractions << "\neager_uploads: " << _stats.eager_uploads
-       << "\ntma_units: " << _stats.tma_units
+       << "\ntma_units: " << _stats.tma_units << "\npack_reuses: " << _stats.pack_reuses
        << "\nbytes_h2d: " << _stats.bytes_h2d << "\nbytes_d2h: " << _stats.bytes_d2h
        << "\ntime_fusion: " << _stats.time_fusion << "\ntime_codegen: " << _stats.time_codegen
        << "\ntime_compile: " << _stats.time_compile << "\nparallel_compiles: " << _stats.parallel_compiles

@@ -47,7 +47,7 @@ struct Stats {
     uint64_t fuse_cache_hits = 0, fuse_cache_misses = 0;
     uint64_t plan_cache_hits = 0, plan_cache_misses = 0, replays = 0;
     uint64_t kernel_cache_hits = 0, kernel_cache_misses = 0, disk_cache_hits = 0, disk_cache_rejected = 0;
-    uint64_t fma_contractions = 0, eager_uploads = 0, tma_units = 0;
+    uint64_t fma_contractions = 0, eager_uploads = 0, tma_units = 0, pack_reuses = 0;
     uint64_t bytes_h2d = 0, bytes_d2h = 0;
     uint64_t serial_units = 0;
     // learned fusion: structures tried with both plans, kept learned / kept greedy, learned plan
@@ -294,6 +294,20 @@ private:
         uint64_t stale_epoch = 0; // host_stale already holds `written` while stale_epoch matches
         ~ReplayGraph();
     };
+    // The parameter blocks of one grouped launch of a replay, kept on the device: a later replay
+    // launches them again without packing or copying while no buffer changed (buffer_epoch) and
+    // the scratch, counter and scan arenas are where they were.
+    struct PackCache {
+        uint64_t epoch = 0;
+        const void *scratch = nullptr, *counters = nullptr, *scan_arena = nullptr;
+        uint8_t *dev = nullptr;  // items, then the prefix sums of their work counts
+        size_t capacity = 0, bytes = 0, items_bytes = 0, n = 0;
+        int64_t total = 0;
+        PackCache() = default;
+        PackCache(const PackCache &) = delete;
+        PackCache &operator=(const PackCache &) = delete;
+        ~PackCache();
+    };
     struct Replay {
         const FlushPlan *plan = nullptr;
         std::vector<bh_base *> base_ids, dead;
@@ -305,7 +319,9 @@ private:
         std::unique_ptr<ReplayGraph> graph;
         bool graph_failed = false;
         int valid_runs = 0;
-        uint64_t checked_epoch = 0; // buffer_epoch after the last graph replay
+        uint64_t checked_epoch = 0; // buffer_epoch after the last replay that changed no buffer
+        uint64_t stale_after = 0;   // stale_epoch after the last replay (its writes are in host_stale)
+        std::map<std::pair<size_t, const Compiled *>, std::unique_ptr<PackCache>> packs; // by level, kernel
     };
     // Bumped on every change of a device buffer or a host data pointer, and on every removal from
     // host_stale; a graph replay that sees both unchanged skips its checks.
@@ -341,12 +357,13 @@ private:
     void record_kernel_times(const FlushPlan &plan, const std::vector<bh_base *> &bases,
                              const std::vector<bh_instruction *> &instrs);
     FlushPlan build_plan(const std::vector<jitk::LoopB> &kernels, const std::vector<bh_base *> &base_ids);
-    void run_plan(const FlushPlan &plan, const std::vector<bh_base *> &bases, const std::vector<bh_instruction *> &instrs);
+    void run_plan(const FlushPlan &plan, const std::vector<bh_base *> &bases, const std::vector<bh_instruction *> &instrs,
+                  Replay *replay = nullptr);
     void pack_params(const PlanUnit &pu, const std::vector<bh_base *> &bases, const std::vector<bh_instruction *> &instrs,
                      int64_t scratch_off, int64_t counter_idx, uint8_t *out);
     void launch_plain(const PlanUnit &pu, const std::vector<bh_base *> &bases, const std::vector<bh_instruction *> &instrs);
     void launch_batched(const std::vector<const PlanUnit *> &group, const std::vector<bh_base *> &bases,
-                        const std::vector<bh_instruction *> &instrs);
+                        const std::vector<bh_instruction *> &instrs, PackCache *cache = nullptr);
     void record_begin(UnitRecord &r, void *&e0);
     void record_end(UnitRecord &r, void *e0);
     // While set, every launch is bracketed by a pair of events from this pool (device busy time

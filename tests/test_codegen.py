@@ -150,14 +150,24 @@ def test_row_reductions_of_contiguous_rows_use_lanes():
     assert "lane_reduce" not in [u["sched"] for u in units]
 
 
-def test_one_dimensional_accumulate_lowers_to_three_scan_units_or_one_pass(monkeypatch):
-    """By default a 1-D accumulate is the three units (chunk totals, carries, re-scan); with
+def test_one_dimensional_accumulate_lowers_to_scan_units_or_one_pass(monkeypatch):
+    """By default a 1-D accumulate is the three units (chunk totals, carries, re-scan walking the
+    chunks last to first) over the whole length; with scan_windows on it is units A and C (the
+    re-scan repeating unit B's scan of the group's totals) per group of 2048 chunks; with
     scan_single_pass on it is one unit (look-back with bounded waits and a fallback)."""
     def prog(rt):
         a = bh.empty(rt, (100000,), np.float64)
         return [bh.accumulate("ADD_ACCUMULATE", a * 2.0 + 1.0, 0) * 3.0]
     res, units = plan(prog)
     assert [u["sched"] for u in units] == ["scan1d", "scan1d", "scan1d"], [u["sched"] for u in units]
+    assert all("chunk_carry" not in u["source"] for u in units)
+    assert "const bh_i64 c = p.nchunks - 1 - (p.first + w);" in units[2]["source"]
+    assert "const bh_i64 c = p.first + w;" in units[0]["source"]
+    monkeypatch.setenv("BH_CUDA_SCAN_WINDOWS", "true")
+    res, units = plan(prog)
+    assert [u["sched"] for u in units] == ["scan1d", "scan1d"], [u["sched"] for u in units]
+    assert "chunk_carry" in units[1]["source"] and "chunk_carry" not in units[0]["source"]
+    monkeypatch.delenv("BH_CUDA_SCAN_WINDOWS")
     monkeypatch.setenv("BH_CUDA_SCAN_SINGLE_PASS", "true")
     res, units = plan(prog)
     assert [u["sched"] for u in units] == ["scan1d"], [u["sched"] for u in units]
@@ -200,6 +210,27 @@ def test_scan_units_stage_elements_at_coalesced_positions(dtype):
             assert "const int q = k * 256 + (int)threadIdx.x;" in src
             assert "stage[q + (q >> 3)] = x;" in src
         assert "= stage[q + (q >> 3)];" in units[2]["source"]
+
+
+def test_scan_windows_are_groups_of_chunks_sharing_two_kernels(monkeypatch):
+    """A scan over 2.5 groups of chunks (2048 chunks of 2048 elements each) is units A and C for
+    each group in turn: the same two compiled kernels, with the group's first chunk and chunk
+    count as parameters; a window's algorithmic bytes are its share of the scan's."""
+    n = 2048 * 2048 * 2 + 2048 * 1024 + 5
+
+    def prog(rt):
+        a = bh.empty(rt, (n,), np.float64)
+        return [bh.accumulate("ADD_ACCUMULATE", a, 0)]
+    monkeypatch.setenv("BH_CUDA_SCAN_WINDOWS", "true")
+    _, units = plan(prog, compile=False)
+    assert [u["sched"] for u in units] == ["scan1d"] * 6
+    names = [u["name"] for u in units]
+    assert names[0] == names[2] == names[4] and names[1] == names[3] == names[5] and names[0] != names[1]
+    monkeypatch.setenv("BH_CUDA_SCAN_WINDOWS", "false")
+    _, whole = plan(prog, compile=False)
+    assert [u["work"] for u in whole] == [5121, 3, 5121]
+    assert sum(u["bytes"] for u in units) == pytest.approx(whole[2]["bytes"], rel=1e-6)
+    assert [u["work"] for u in units] == [2048, 2048, 2048, 2048, 1025, 1025]
 
 
 def test_complex_programs_compile_for_every_schedule():

@@ -498,11 +498,12 @@ def test_scan1d(gpu_rt, oracle_rt, n, dtype, name):
 
 
 @pytest.mark.parametrize("n,dtype", [(5, np.float64), (2049, np.float32), (1_000_003, np.float64),
-                                     (4_500_001, np.float32)])
+                                     (4_500_001, np.float32), (9_000_001, np.float64)])
 def test_scan1d_order_is_canonical(gpu_rt, n, dtype):
     """SCAN1D adds in one fixed order (per-thread runs of 8, block scans, carries over the chunk
-    totals, more than one group of 2048 totals at 4.5M elements): the GPU cumulative sum of a
-    fused input equals the exact order model bit for bit."""
+    totals, more than one group of 2048 totals from 4.2M elements, each group's carry from the
+    previous group's): the GPU cumulative sum of a fused input equals the exact order model bit
+    for bit."""
     from tests.harness import scan1d_cumsum
     x = np.random.default_rng(n).standard_normal(n).astype(dtype)
 
@@ -511,6 +512,34 @@ def test_scan1d_order_is_canonical(gpu_rt, n, dtype):
     (got,) = run(gpu_rt, prog)
     want = scan1d_cumsum(x)
     assert np.asarray(got).tobytes() == want.tobytes()
+
+
+@pytest.mark.parametrize("name", ["ADD_ACCUMULATE", "MULTIPLY_ACCUMULATE"])
+def test_scan1d_windows_equal_the_whole_length_units(gpu_rt, monkeypatch, name):
+    """With scan_windows on, units A and C run one group of chunks at a time (C repeating unit
+    B's scan of its group); by default the three units run over the whole length (the re-scan
+    last chunk first). Both give the same bits, for sums and products, over three groups and a
+    partial one."""
+    n = 3 * 2048 * 2048 + 12345
+    rng = np.random.default_rng(17)
+    x = (1.0 + 1e-7 * rng.standard_normal(n)) if name == "MULTIPLY_ACCUMULATE" else rng.standard_normal(n)
+
+    def prog(rt):
+        a = bh.array(rt, x)
+        c = bh.accumulate(name, a * 1.0 + 0.0, 0)
+        return [c, c * 2.0]
+    whole = run(gpu_rt, prog)
+    monkeypatch.setenv("BH_CUDA_SCAN_WINDOWS", "true")
+    ex = bh.NativeExecutor(stack="cuda")
+    try:
+        windowed = run(bh.Runtime(ex), prog)
+    finally:
+        ex.close()
+    for a, b in zip(windowed, whole):
+        assert np.asarray(a).tobytes() == np.asarray(b).tobytes()
+    if name == "ADD_ACCUMULATE":
+        from tests.harness import scan1d_cumsum
+        assert np.asarray(windowed[0]).tobytes() == scan1d_cumsum(x).tobytes()
 
 
 @pytest.mark.parametrize("dtype", [np.float64, np.int64])
