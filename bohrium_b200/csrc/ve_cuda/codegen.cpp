@@ -60,6 +60,14 @@ int64_t LaunchUnit::work_items() const {
     return 1;
 }
 
+int64_t LaunchUnit::grouped_work_items() const {
+    if (sched == Sched::GRID_REDUCE && batch_chunks > 0 && batch_chunks != chunks) {
+        const int64_t tiles = (cols + kReduceTile - 1) / kReduceTile;
+        return (tiles + batch_chunks - 1) / batch_chunks;
+    }
+    return work_items();
+}
+
 int64_t LaunchUnit::scratch_bytes() const {
     if (sched == Sched::GRID_REDUCE) return (cols + kReduceTile - 1) / kReduceTile * scratch_bytes_per_tile;
     if (sched == Sched::SPLIT_REDUCE) return slot_bytes * static_cast<int64_t>(nred) * chunks * rows * cols;
@@ -379,6 +387,12 @@ __device__ __forceinline__ bool bh_mbar_wait(unsigned long long *bar, unsigned p
     for (int i = 0; i < (1 << 20); ++i)
         if (bh_mbar_try_wait(bar, parity)) return true;
     return false;
+}
+// One contiguous global -> shared copy by the TMA engine (16-byte aligned addresses, a multiple
+// of 16 bytes), counted on `bar`; no cluster multicast.
+__device__ __forceinline__ void bh_bulk_row(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(bh_saddr(dst)), "l"(src), "r"(bytes), "r"(bh_saddr(bar)) : "memory");
 }
 __device__ __forceinline__ void bh_tma_2d(void *dst, const bh_tmap *map, int x, int y, unsigned long long *bar) {
     asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
@@ -1113,16 +1127,22 @@ extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME___batch(const P*
             have_lo = prefix[lo];
             have_hi = prefix[lo + 1];
         }
-        bh_work(sp, g - have_lo);
+        bh_batch_work(sp, g - have_lo);
     }
     (void)have;
 }
 )CUDA";
-const string kWrappers = string(R"CUDA(
+// What one CTA of a plain launch does, and the device code of one work item of a grouped launch
+// (the same as a plain launch's unless a unit defines its own).
+const char *kMainWrapper = R"CUDA(
 __device__ __forceinline__ void bh_main(const P &p) {
     for (bh_i64 w = blockIdx.x; w < p.work; w += gridDim.x) bh_work(p, w);
 }
-)CUDA") + kKernels;
+)CUDA";
+const char *kBatchWork = R"CUDA(
+__device__ __forceinline__ void bh_batch_work(const P &p, bh_i64 w) { bh_work(p, w); }
+)CUDA";
+const string kWrappers = string(kMainWrapper) + kBatchWork + kKernels;
 
 void finish_source(LaunchUnit &u, const string &params_decl, const string &body, const CodegenOptions &opt) {
     u.params_decl = params_decl;
@@ -1136,7 +1156,7 @@ void finish_source(LaunchUnit &u, const string &params_decl, const string &body,
     src << kPrelude;
     auto uses = [&](const char *name) { return params_decl.find(name) != string::npos || body.find(name) != string::npos; };
     if (uses("bh_c64") || uses("bh_c128")) src << kComplexPrelude;
-    if (uses("bh_tmap")) src << kTmaPrelude;
+    if (uses("bh_tmap") || uses("bh_mbar")) src << kTmaPrelude;
     if (opt.bounds_check) src << bounds_check_helper();
     src << "struct P {\n" << params_decl << "};\n";
     src << body;
@@ -1770,7 +1790,7 @@ bool lower_tile2d(const LoopB &loop, const CodegenOptions &opt, LaunchUnit &u) {
     }
 }
 )CUDA";
-    body << kKernels;
+    body << kBatchWork << kKernels;
     u.fields = pl.fields;
     u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
     u.elements = u.rows * u.cols;
@@ -2153,6 +2173,13 @@ LaunchUnit lower_lane_reduce(const LoopB &loop, unsigned P, const CodegenOptions
             ParamField fe{ParamField::I64};
             fe.i64 = v0->base->nelem();
             pl.add(fe, "bh_i64", "stage_nelem");
+            if (opt.stage_bulk) {
+                ParamField fok{ParamField::TMA_OK};  // bulk copies allowed (not in grouped launches)
+                pl.add(fok, "bh_i64", "tma_ok");
+                ParamField ferr{ParamField::SCRATCH};
+                ferr.i64 = -1;  // the engine's error record
+                pl.add(ferr, "unsigned long long*", "err");
+            }
             body << "// bh_dynamic_shared_bytes: " << smem << "\n";
             body << kStagePrelude;
             // Launch-time check: the layout the staging assumes holds for these parameters, and
@@ -2172,7 +2199,25 @@ LaunchUnit lower_lane_reduce(const LoopB &loop, unsigned P, const CodegenOptions
                  << g.mmin << "LL) + " << nrow << ";\n";
             body << "    return first >= 0 && last <= p.stage_nelem;\n";
             body << "}\n";
-            body << "__device__ void bh_work_staged(const P &p, bh_i64 lo, bh_i64 hi) {\n";
+            // The bulk form copies each row from the 16-byte boundary at or below its first element
+            // to the 16-byte boundary at or above its end: that span must lie inside the base.
+            body << "__device__ __forceinline__ bool bh_bulk_ok(const P &p, bh_i64 lo, bh_i64 hi) {\n";
+            body << "    const bh_i64 S0 = " << S0 << ";\n";
+            body << "    if (((unsigned long long)p.a" << pid << " & 15ULL) != 0) return false;\n";
+            body << "    const bh_i64 first = p.v" << vid0 << "_o + (lo + (" << g.kmin << "LL)) * S0 + (" << g.mmin << "LL);\n";
+            body << "    const bh_i64 pre = first % " << CE << ";\n";
+            body << "    const bh_i64 span = (pre + " << nrow << " + " << CE - 1 << ") / " << CE << " * " << CE << ";\n";
+            body << "    const bh_i64 last = p.v" << vid0 << "_o + (hi - 1 + (" << g.kmin + g.kspan << "LL)) * S0 + (" << g.mmin
+                 << "LL) - pre + span;\n";
+            body << "    return span <= " << RS << " && last <= p.stage_nelem;\n";
+            body << "}\n";
+            // Two forms of the staged walk: `bulk` fills each ring row with one cp.async.bulk copy
+            // (the TMA engine, issued by one thread, completion counted on the row slot's
+            // mbarrier; waits bounded), the other with 16-byte cp.async copies by every thread
+            // (commit groups). Grouped launches (no error-record check) take the cp.async form.
+            auto emit_staged = [&](bool bulk) {
+            const string fname = bulk ? "bh_work_bulk" : "bh_work_staged";
+            body << "__device__ void " << fname << "(const P &p, bh_i64 lo, bh_i64 hi) {\n";
             body << "    extern __shared__ __align__(16) unsigned char bh_dyn[];\n";
             body << "    " << T << "* ring = (" << T << "*)bh_dyn;\n";
             body << pointer_locals(sym);
@@ -2184,21 +2229,61 @@ LaunchUnit lower_lane_reduce(const LoopB &loop, unsigned P, const CodegenOptions
                  << g.mmin << "LL));\n";
             body << "    const int pre = (int)(((unsigned long long)(rows0 + lo * S0) & 15ULL) / " << es << ");\n";
             body << "    const bh_i64 rend = hi + " << g.kspan << ";\n";
-            body << "    for (int b = 0; b < " << NB << "; ++b) {\n";
-            body << "        const bh_i64 r = lo + b;\n";
-            body << "        if (r < rend) bh_stage_row(ring + (r % " << NB << ") * " << RS << ", rows0 + r * S0, (bh_i64)"
-                 << nrow << ", pre);\n";
-            body << "        bh_cp_commit();\n";
-            body << "    }\n";
+            if (bulk) {
+                // Row r (relative index r - lo) lives in slot (r - lo) % NB; its copy is the
+                // ((r - lo) / NB)-th completion of that slot's barrier.
+                body << "    const unsigned row_bytes = (unsigned)(((pre + " << nrow << ") * " << es << " + 15) / 16 * 16);\n";
+                body << "    __shared__ alignas(8) unsigned long long bar[" << NB << "];\n";
+                body << "    __shared__ int fail;\n";
+                body << "    if (threadIdx.x == 0) {\n";
+                body << "        for (int b = 0; b < " << NB << "; ++b) bh_mbar_init(&bar[b], 1u);\n";
+                body << "        bh_mbar_fence_init();\n";
+                body << "        fail = 0;\n";
+                body << "    }\n";
+                body << "    __syncthreads();\n";
+                body << "    bh_i64 issued = lo, waited = lo;  // rows [lo, issued) copied, [lo, waited) arrived (thread 0)\n";
+                body << "    if (threadIdx.x == 0) {\n";
+                body << "        for (; issued < rend && issued < lo + " << NB << "; ++issued) {\n";
+                body << "            const int b = (int)(issued - lo);\n";
+                body << "            bh_mbar_expect_tx(&bar[b], row_bytes);\n";
+                body << "            bh_bulk_row(ring + b * " << RS << ", (const char *)(rows0 + issued * S0) - pre * " << es
+                     << ", row_bytes, &bar[b]);\n";
+                body << "        }\n";
+                body << "    }\n";
+            } else {
+                body << "    for (int b = 0; b < " << NB << "; ++b) {\n";
+                body << "        const bh_i64 r = lo + b;\n";
+                body << "        if (r < rend) bh_stage_row(ring + (r % " << NB << ") * " << RS << ", rows0 + r * S0, (bh_i64)"
+                     << nrow << ", pre);\n";
+                body << "        bh_cp_commit();\n";
+                body << "    }\n";
+            }
             body << "    for (bh_i64 pt = lo; pt < hi; ++pt) {\n";
-            body << "        bh_cp_wait<" << kStagePrefetch << ">();  // all but the newest prefetched rows have landed\n";
-            body << "        __syncthreads();\n";
+            if (bulk) {
+                // Rows pt .. pt + kspan are read; all but the newest arrived by earlier points.
+                body << "        for (bh_i64 r = (pt == lo ? lo : pt + " << g.kspan << "); r <= pt + " << g.kspan << "; ++r) {\n";
+                body << "            const int b = (int)((r - lo) % " << NB << ");\n";
+                body << "            if (!bh_mbar_wait(&bar[b], (unsigned)(((r - lo) / " << NB << ") & 1))) fail = 1;\n";
+                body << "            else if (threadIdx.x == 0) waited = r + 1;\n";
+                body << "        }\n";
+                body << "        __syncthreads();\n";
+                body << "        if (fail) break;\n";
+            } else {
+                body << "        bh_cp_wait<" << kStagePrefetch << ">();  // all but the newest prefetched rows have landed\n";
+                body << "        __syncthreads();\n";
+            }
             body << "        const bh_i64 i0 = pt;\n";
             for (size_t k = 0; k < reds.size(); ++k)
                 body << "        " << ctypes[k] << " pacc" << k << " = " << idents[k] << ";\n";
-            for (size_t k = 0; k < g.m.size(); ++k)
-                body << "        const " << T << "* sr" << k << " = ring + ((pt + " << g.m[k].dk - g.kmin << ") % " << NB
-                     << ") * " << RS << " + pre + " << g.m[k].dm - g.mmin << ";\n";
+            for (size_t k = 0; k < g.m.size(); ++k) {
+                if (bulk) {
+                    body << "        const " << T << "* sr" << k << " = ring + ((pt - lo + " << g.m[k].dk - g.kmin << ") % " << NB
+                         << ") * " << RS << " + pre + " << g.m[k].dm - g.mmin << ";\n";
+                } else {
+                    body << "        const " << T << "* sr" << k << " = ring + ((pt + " << g.m[k].dk - g.kmin << ") % " << NB
+                         << ") * " << RS << " + pre + " << g.m[k].dm - g.mmin << ";\n";
+                }
+            }
             {
                 Scope scope;
                 declare_chain_temps(em, sym, scope, chain, P, body, 8);
@@ -2221,9 +2306,19 @@ LaunchUnit lower_lane_reduce(const LoopB &loop, unsigned P, const CodegenOptions
             }
             body << "        __syncthreads();  // also: every thread is done with the oldest row's buffer\n";
             body << "        const bh_i64 rnext = pt + " << NB << ";\n";
-            body << "        if (rnext < rend) bh_stage_row(ring + (rnext % " << NB << ") * " << RS
-                 << ", rows0 + rnext * S0, (bh_i64)" << nrow << ", pre);\n";
-            body << "        bh_cp_commit();\n";
+            if (bulk) {
+                body << "        if (threadIdx.x == 0 && rnext < rend) {\n";
+                body << "            const int b = (int)((rnext - lo) % " << NB << ");\n";
+                body << "            bh_mbar_expect_tx(&bar[b], row_bytes);\n";
+                body << "            bh_bulk_row(ring + b * " << RS << ", (const char *)(rows0 + rnext * S0) - pre * " << es
+                     << ", row_bytes, &bar[b]);\n";
+                body << "            issued = rnext + 1;\n";
+                body << "        }\n";
+            } else {
+                body << "        if (rnext < rend) bh_stage_row(ring + (rnext % " << NB << ") * " << RS
+                     << ", rows0 + rnext * S0, (bh_i64)" << nrow << ", pre);\n";
+                body << "        bh_cp_commit();\n";
+            }
             body << "        if (lane == 0) {\n";
             for (size_t k = 0; k < reds.size(); ++k) {
                 body << "            pacc" << k << " = wsum" << k << "[pt & 1][0];\n";
@@ -2256,8 +2351,21 @@ LaunchUnit lower_lane_reduce(const LoopB &loop, unsigned P, const CodegenOptions
             }
             body << "        }\n";
             body << "    }\n";
-            body << "    bh_cp_wait0();  // no copy in flight when the CTA leaves\n";
+            if (bulk) {
+                body << "    if (fail && threadIdx.x == 0) {\n";
+                body << "        // A row copy never completed: record it, and let the copies still in flight into\n";
+                body << "        // the ring land (bounded) before the CTA leaves.\n";
+                body << "        atomicCAS(p.err, 0ull, 0xC000000000000000ull | (unsigned long long)blockIdx.x);\n";
+                body << "        for (bh_i64 r = waited; r < issued; ++r)\n";
+                body << "            bh_mbar_wait(&bar[(r - lo) % " << NB << "], (unsigned)(((r - lo) / " << NB << ") & 1));\n";
+                body << "    }\n";
+            } else {
+                body << "    bh_cp_wait0();  // no copy in flight when the CTA leaves\n";
+            }
             body << "}\n";
+            };
+            emit_staged(false);
+            if (opt.stage_bulk) emit_staged(true);
             string wrappers = kWrappers;
             const string loop = "    for (bh_i64 w = blockIdx.x; w < p.work; w += gridDim.x) bh_work(p, w);\n";
             const size_t at = wrappers.find(loop);
@@ -2266,8 +2374,10 @@ LaunchUnit lower_lane_reduce(const LoopB &loop, unsigned P, const CodegenOptions
                              "    // a contiguous range of points (rows) per CTA\n"
                              "    const bh_i64 lo = (bh_i64)blockIdx.x * p.work / gridDim.x;\n"
                              "    const bh_i64 hi = ((bh_i64)blockIdx.x + 1) * p.work / gridDim.x;\n"
-                             "    if (lo < hi && bh_stage_ok(p, lo, hi)) {\n"
-                             "        bh_work_staged(p, lo, hi);\n"
+                             "    if (lo < hi && bh_stage_ok(p, lo, hi)) {\n" +
+                             string(opt.stage_bulk ? "        if (p.tma_ok && bh_bulk_ok(p, lo, hi)) bh_work_bulk(p, lo, hi);\n"
+                                                     "        else bh_work_staged(p, lo, hi);\n"
+                                                   : "        bh_work_staged(p, lo, hi);\n") +
                              "    } else {\n"
                              "        for (bh_i64 w = lo; w < hi; ++w) bh_work(p, w);\n"
                              "    }\n");
@@ -2539,15 +2649,20 @@ int grid_tiles_per_item(int64_t ntiles, const LoopB &L) {
             ++heavy;
     }
     if (n > 24 || heavy > 0) return 1;
-    // Small kernels (at most 64 tiles) take 4 tiles per item too: launched alone they are
-    // latency-bound either way, and in a grouped launch (many small arrays through the same
-    // kernel) every work item then keeps 4 tiles of loads in flight and pays one block reduction
-    // and one counter update for the 4.
-    if (ntiles <= 64) return 4;
     const int64_t resident = 148 * 4;
     if (ntiles >= 4 * 4 * resident) return 4;
     if (ntiles >= 2 * 2 * resident) return 2;
     return 1;
+}
+
+// Tiles per work item in a grouped launch: small light kernels (at most 64 tiles) take 4, so that
+// in a launch of many small arrays through the same kernel every work item keeps 4 tiles of loads
+// in flight and pays one block reduction and one counter update for the 4. Launched alone they
+// keep 1 tile per item (more CTAs: a launch of a few tiles is latency-bound).
+int grid_tiles_per_item_grouped(int64_t ntiles, const LoopB &L) {
+    const int plain = grid_tiles_per_item(ntiles, L);
+    if (plain == 1 && ntiles <= 64 && grid_tiles_per_item(int64_t{1} << 40, L) == 4) return 4;
+    return plain;
 }
 
 // Block reduction of K values per thread at once (one shared-memory round for all K): the same
@@ -2581,7 +2696,8 @@ string block_reduce_k_fn(const string &ctype, const string &fname, bh_opcode op,
     return ss.str();
 }
 
-LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identities, const CodegenOptions &opt) {
+LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identities, const CodegenOptions &opt,
+                             int forceK = 0) {
     LaunchUnit u;
     u.sched = Sched::GRID_REDUCE;
     u.V = kReduceV;
@@ -2595,7 +2711,28 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
     u.nred = static_cast<int>(reds.size());
     u.cols = L.size;
     const int64_t ntiles = (L.size + kReduceTile - 1) / kReduceTile;
-    const int K = grid_tiles_per_item(ntiles, L);
+    // Tiles per work item: Kp for plain launches, Kg for grouped ones. When they differ the unit's
+    // source holds the device code twice, compiled for each (bh_work and bh_batch_work); results
+    // do not depend on it (every tile keeps its own partial).
+    const int Kp = grid_tiles_per_item(ntiles, L), Kg = grid_tiles_per_item_grouped(ntiles, L);
+    if (forceK == 0 && Kp != Kg) {
+        LaunchUnit up = lower_grid_reduce(loop, identities, opt, Kp);
+        const LaunchUnit ug = lower_grid_reduce(loop, identities, opt, Kg);
+        if (up.body_core.empty() || ug.body_core.empty()) throw runtime_error("lower_grid_reduce(): no body core");
+        stringstream both;
+        both << "namespace bh_kp {\n" << up.body_core << "} // namespace bh_kp\n";
+        both << "namespace bh_kg {\n" << ug.body_core << "} // namespace bh_kg\n";
+        both << "__device__ __forceinline__ void bh_work(const P &p, bh_i64 w) { bh_kp::bh_work(p, w); }\n";
+        both << "__device__ __forceinline__ void bh_batch_work(const P &p, bh_i64 w) { bh_kg::bh_work(p, w); }\n";
+        if (up.tail_capable) both << "__device__ __forceinline__ void bh_tail(const P &p) { bh_kp::bh_tail(p); }\n";
+        both << kMainWrapper << kKernels;
+        LaunchUnit u2 = up;
+        u2.batch_chunks = Kg;
+        finish_source(u2, up.params_decl, both.str(), opt);
+        return u2;
+    }
+    const int K = forceK > 0 ? forceK : Kp;
+    const string KT = to_string(K);
     u.chunks = K;
     ParamLayout pl;
     add_common_fields(sym, pl, opt);
@@ -2648,8 +2785,8 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
         body << "#pragma unroll\n";
         body << "    for (int k = 0; k < " << K << "; ++k) " << accs[k] << "[k] = " << idents[k] << ";\n";
     }
-    body << "    const bh_i64 tile0 = w * " << K << ";\n";
-    body << "    const int ktiles = (int)min((bh_i64)" << K << ", p.ntiles - tile0);\n";
+    body << "    const bh_i64 tile0 = w * " << KT << ";\n";
+    body << "    const int ktiles = (int)min((bh_i64)" << KT << ", p.ntiles - tile0);\n";
     // Full items (K full tiles) run without bounds checks, after loading the read-only inputs of
     // all K x 8 elements of the thread; the last item checks every index. Tile k accumulates into
     // slot k, elements j = 0..7 in order, in both paths.
@@ -2791,7 +2928,7 @@ LaunchUnit lower_grid_reduce(const LoopB &loop, const vector<InstrPtr> &identiti
     // Path 0: all K tiles of the item are full. Every input of all K x 8 elements of the thread is
     // loaded first, then the tiles are computed.
     {
-        body << "    if ((tile0 + " << K << ") * " << kReduceTile << " <= " << n0 << ") {\n";
+        body << "    if ((tile0 + " << KT << ") * " << kReduceTile << " <= " << n0 << ") {\n";
         Scope scope;
         Emitter eb(sym, body, opt);
         eb.external_acc = acc_k;
@@ -3085,14 +3222,7 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
         Emitter em(sym, body, opt);
         body << block_scan_fn(T, "bh_block_scan", rop, ident);
         body << "__device__ void bh_work(const P &p, bh_i64 w) {\n";
-        if (phase == 2 && !windowed) {
-            // The re-scan walks the chunks from the last one down: unit A read them first to
-            // last, so the ones it read last are still in L2 when the re-scan starts. Chunks are
-            // independent here (each has its carry), so the order changes no result.
-            body << "    const bh_i64 c = p.nchunks - 1 - (p.first + w);\n";
-        } else {
-            body << "    const bh_i64 c = p.first + w;\n";
-        }
+        body << "    const bh_i64 c = p.first + w;\n";
         body << pointer_locals(sym);
         body << "    __shared__ " << T << " sm[" << 2 * (kThreads / 32) + 1 << "];\n";
         body << "    " << T << "* totals = (" << T << "*)p.scratch;\n";
@@ -3680,7 +3810,7 @@ __device__ __forceinline__ bool bh_await(const unsigned *flag, const unsigned *a
     }
 }
 )CUDA";
-    body << kKernels;
+    body << kBatchWork << kKernels;
     u.fields = pl.fields;
     u.scan_bytes = (2 * nchunks + (nchunks + 7) / 8 + (nchunks + 255) / 256 + ngroups + 1) *
                    static_cast<int64_t>(bh_type_size(t));
@@ -3836,7 +3966,7 @@ extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME___batch(const P*
             have_lo = prefix[lo];
             have_hi = prefix[lo + 1];
         }
-        bh_u1::bh_work(sp.a, g - have_lo);
+        bh_u1::bh_batch_work(sp.a, g - have_lo);
         if (bh_tail_gate(sp.tail_counter, (unsigned int)(have_hi - have_lo))) bh_u2::bh_tail(sp.b);
     }
 }
@@ -3860,7 +3990,7 @@ LaunchUnit fuse_tail(const LaunchUnit &u1, const LaunchUnit &u2) {
         return false;
     };
     if (uses("bh_c64") || uses("bh_c128")) src << kComplexPrelude;
-    if (uses("bh_tmap")) src << kTmaPrelude;
+    if (uses("bh_tmap") || uses("bh_mbar")) src << kTmaPrelude;
     src << "namespace bh_u1 {\nstruct P {\n" << u1.params_decl << "};\n" << u1.body_core << "} // namespace bh_u1\n";
     src << "namespace bh_u2 {\nstruct P {\n" << u2.params_decl << "};\n" << u2.body_core << "} // namespace bh_u2\n";
     src << kTailWrappers;

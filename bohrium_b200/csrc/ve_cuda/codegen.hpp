@@ -30,7 +30,6 @@
 //   SCAN1D        a 1-D nest with one accumulate (cumulative sum/product) among elementwise
 //                 instructions: three units -- chunk totals, one-CTA exclusive scan of the totals,
 //                 re-scan with the carry -- each with a fixed block scan (order set by the length).
-//                 The re-scan walks the chunks last to first (the ones A read last are in L2).
 //                 With scan_windows, A and C run one group of 2048 chunks at a time (C repeating
 //                 B's steps for its group), so the re-scan reads the group's inputs from L2.
 //   SERIAL        anything else: one thread runs the nest in program order (always correct).
@@ -117,6 +116,7 @@ struct LaunchUnit {
     int slot_bytes = 8;         // GRID_REDUCE / SPLIT_REDUCE: bytes of one partial (16 with complex128)
     int64_t chunks = 1;         // SPLIT_REDUCE: chunks of the swept axis; LANE_REDUCE: lanes per point;
                                 // GRID_REDUCE: tiles per work item; SCAN1D: work items of the phase
+    int64_t batch_chunks = 0;   // GRID_REDUCE: tiles per work item in a grouped launch (0: chunks)
     int64_t scan_bytes = 0;     // SCAN1D: its chunk totals and carries and group totals and carries
     int64_t scan_offset = 0;    // SCAN1D: offset of scan_bytes in the scan arena (set by the plan)
     bool scan_gate = false;     // SCAN1D carry unit: one completion counter
@@ -133,6 +133,7 @@ struct LaunchUnit {
     // completion counter follows the unit's own counters.
     bool tail = false;
     int64_t work_items() const;
+    int64_t grouped_work_items() const; // work items when launched grouped (batch_chunks)
     int64_t scratch_bytes() const;   // partials in the scratch arena
     int64_t counters_needed() const; // completion counters
 
@@ -155,6 +156,7 @@ struct CodegenOptions {
     bool vector_access = true;  // FLAT: 4 consecutive elements per thread, moved as 128-bit words
     bool scan_single_pass = false; // SCAN1D as one pass with look-back (else three units; see lower_scan1d_single)
     bool scan_windows = false;     // SCAN1D units A and C one group of chunks at a time (see lower_scan1d)
+    bool stage_bulk = true;        // LANE_REDUCE stencil rows staged by TMA bulk copies (else cp.async)
     int64_t scan_spin_cap = int64_t{1} << 22; // polls per look-back wait (negative: give up at once)
 };
 

@@ -114,6 +114,7 @@ EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
     cg_opt.vector_access = cfg.defaultGet<bool>("vector_access", true);
     cg_opt.scan_single_pass = cfg.defaultGet<bool>("scan_single_pass", false);
     cg_opt.scan_windows = cfg.defaultGet<bool>("scan_windows", false);
+    cg_opt.stage_bulk = cfg.defaultGet<bool>("stage_bulk", true);
     cg_opt.scan_spin_cap = cfg.defaultGet<int64_t>("scan_spin_cap", int64_t{1} << 22);
     // The GPU reduces over the outermost axis natively, so sweeps may fuse with maps at rank 0.
     fusion_config = jitk::FusionConfig(cfg, false);
@@ -205,9 +206,9 @@ void EngineCUDA::synchronize_all() {
     check_tma_record();
 }
 
-// A TILE2D kernel whose tile loads did not complete within its bounded wait records that in the
-// error record (top bits 11) and skips the rest of its tiles. Read at synchronisation points only,
-// so that flushes stay asynchronous.
+// A kernel whose TMA copies (TILE2D tiles, bulk-staged stencil rows) did not complete within its
+// bounded wait records that in the error record (top bits 11) and skips the rest of its work. Read
+// at synchronisation points only, so that flushes stay asynchronous.
 void EngineCUDA::check_tma_record() {
     if (!tma_check_pending) return;
     tma_check_pending = false;
@@ -215,7 +216,7 @@ void EngineCUDA::check_tma_record() {
     check(cudaMemcpy(&v, err_record, sizeof(v), cudaMemcpyDeviceToHost), "cudaMemcpy(err)");
     if ((v >> 62) == 3ULL) {
         check(cudaMemset(err_record, 0, sizeof(v)), "cudaMemset(err)");
-        throw runtime_error("a TILE2D kernel gave up waiting for a TMA tile load (CTA " +
+        throw runtime_error("a kernel gave up waiting for a TMA copy (CTA " +
                             to_string(v & 0xffffffffULL) + "); its outputs are incomplete");
     }
 }
@@ -948,7 +949,7 @@ void EngineCUDA::launch_batched(const vector<const PlanUnit *> &group, const vec
         for (size_t k = 0; k < n; ++k) {
             pack_params(*group[k], bases, instrs, scratch_off[k], counter_off[k], host + k * psize);
             prefix[k] = total;
-            total += group[k]->unit.work_items();
+            total += group[k]->unit.grouped_work_items();
         }
         packing_grouped = false;
         prefix[n] = total;

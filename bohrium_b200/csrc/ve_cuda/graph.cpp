@@ -180,7 +180,7 @@ bool EngineCUDA::build_graph(Replay &r) {
                     soff += (grp[k]->unit.scratch_bytes() + 255) / 256 * 256;
                     coff += grp[k]->unit.counters_needed();
                     prefix[k] = total;
-                    total += grp[k]->unit.work_items();
+                    total += grp[k]->unit.grouped_work_items();
                 }
                 packing_grouped = false;
                 prefix[n] = total;

@@ -517,8 +517,7 @@ def test_scan1d_order_is_canonical(gpu_rt, n, dtype):
 @pytest.mark.parametrize("name", ["ADD_ACCUMULATE", "MULTIPLY_ACCUMULATE"])
 def test_scan1d_windows_equal_the_whole_length_units(gpu_rt, monkeypatch, name):
     """With scan_windows on, units A and C run one group of chunks at a time (C repeating unit
-    B's scan of its group); by default the three units run over the whole length (the re-scan
-    last chunk first). Both give the same bits, for sums and products, over three groups and a
+    B's scan of its group); by default the three units run over the whole length. Both give the same bits, for sums and products, over three groups and a
     partial one."""
     n = 3 * 2048 * 2048 + 12345
     rng = np.random.default_rng(17)
