@@ -120,6 +120,15 @@ typedef long long bh_i64;
 typedef unsigned long long bh_u64;
 struct bh_r123 { bh_u64 start, key; };
 
+// Programmatic dependent launch: a kernel launched with programmatic stream serialization may
+// start while the kernel before it in the stream finishes; it waits here, before touching memory,
+// until that kernel has completed and its writes are visible, and lets the next kernel start
+// early in turn. For a launch without the attribute both are no-ops.
+__device__ __forceinline__ void bh_grid_dependency() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ bh_u64 bh_random123(bh_u64 start, bh_u64 key, bh_u64 index) {
     const bh_u64 c = start + index;
     unsigned x0 = (unsigned)c, x1 = (unsigned)(c >> 32), k = (unsigned)key;
@@ -1100,6 +1109,7 @@ uint64_t fnv1a(const string &s) {
 // replaces its loop) and the two kernels. The kernels' text (kKernels) is the same for every unit.
 const char *kKernels = R"CUDA(
 extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME__(const __grid_constant__ P p) {
+    bh_grid_dependency();
     bh_main(p);
 }
 extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME___batch(const P* __restrict__ items,
@@ -1107,6 +1117,7 @@ extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME___batch(const P*
     // Each CTA takes a contiguous range of the work items of all items, so consecutive work items
     // of a CTA belong to the same item except at item boundaries. The parameters of the current
     // item live in shared memory and are looked up and reloaded only at those boundaries.
+    bh_grid_dependency();
     __shared__ P sp;
     int have = -1;
     bh_i64 have_lo = 0, have_hi = 0;
@@ -1494,6 +1505,9 @@ void emit_flat_vector(Symbols &sym, ostream &body, const CodegenOptions &opt, co
     body << "    }\n";
 }
 
+// Elements of a map small enough to run in another kernel's tail.
+constexpr int64_t kFlatTailElements = 4096;
+
 LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) {
     LaunchUnit u;
     u.sched = Sched::FLAT;
@@ -1534,9 +1548,18 @@ LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) 
         u.V > 1 && !(heavy_body(inner) && !opt.preload_heavy) ? preloadable_views(inner, L, sym) : vector<bh_view>{};
     const string n_inner = "p.n" + to_string(sym.loop_id.at(&inner));
     const string iv = "i" + to_string(P - 1);
+    // A small map (at most kFlatTailElements elements) can also run in the tail of the kernel
+    // before it, by the CTA that finishes that kernel last (fuse_tails): one CTA runs every work
+    // item in turn. Elementwise results do not depend on which thread computes them. (bh_tail is
+    // in every map's source, so that maps of every size share one compiled kernel.)
+    const string tail_fn = opt.bounds_check ? ""
+                                            : "__device__ void bh_tail(const P &p) {\n"
+                                              "    for (bh_i64 w = 0; w < p.work; ++w) bh_work(p, w);\n"
+                                              "}\n";
+    u.tail_capable = !opt.bounds_check && rows * u.cols <= kFlatTailElements;
     if (u.V == 4 && opt.vector_access && !opt.bounds_check) {
         emit_flat_vector(sym, body, opt, inner, chain, P, pre, per, n_inner, iv);
-        body << "}\n" << kWrappers;
+        body << "}\n" << tail_fn << kWrappers;
         u.fields = pl.fields;
         u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
         u.elements = rows * u.cols;
@@ -1562,7 +1585,7 @@ LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) 
         eb.write_body(inner, scope, 12);
         body << "        }\n";
     }
-    body << "    }\n}\n" << kWrappers;
+    body << "    }\n}\n" << tail_fn << kWrappers;
     u.fields = pl.fields;
     u.algorithmic_bytes = unit_bytes(sym, vector<const Block *>{&holder});
     u.elements = rows * u.cols;
@@ -3942,12 +3965,14 @@ __device__ __forceinline__ bool bh_tail_gate(unsigned int *counter, unsigned int
     return l;
 }
 extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME__(const __grid_constant__ P p) {
+    bh_grid_dependency();
     bh_u1::bh_main(p.a);
     if (bh_tail_gate(p.tail_counter, gridDim.x)) bh_u2::bh_tail(p.b);
 }
 extern "C" __global__ void __launch_bounds__(256) __KERNEL_NAME___batch(const P* __restrict__ items,
         const bh_i64* __restrict__ prefix, int nitems, bh_i64 total) {
     // As the plain grouped wrapper; each item's tail runs after the item's last work item.
+    bh_grid_dependency();
     __shared__ P sp;
     bh_i64 have_lo = 0, have_hi = 0;
     const bh_i64 g_lo = (bh_i64)blockIdx.x * total / gridDim.x;

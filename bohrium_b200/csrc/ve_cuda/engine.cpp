@@ -62,6 +62,7 @@ struct DeviceApi {
     CUresult (*cuModuleGetFunction)(CUfunction *, CUmodule, const char *) = nullptr;
     CUresult (*cuLaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
                                CUstream, void **, void **) = nullptr;
+    CUresult (*cuLaunchKernelEx)(const CUlaunchConfig *, CUfunction, void **, void **) = nullptr;
     CUresult (*cuOccupancyMaxActiveBlocksPerMultiprocessor)(int *, CUfunction, int, size_t) = nullptr;
     CUresult (*cuGetErrorString)(CUresult, const char **) = nullptr;
     CUresult (*cuFuncGetAttribute)(int *, CUfunction_attribute, CUfunction) = nullptr;
@@ -83,6 +84,7 @@ struct DeviceApi {
         get("cuModuleUnload", cuModuleUnload);
         get("cuModuleGetFunction", cuModuleGetFunction);
         get("cuLaunchKernel", cuLaunchKernel);
+        get("cuLaunchKernelEx", cuLaunchKernelEx);
         get("cuOccupancyMaxActiveBlocksPerMultiprocessor", cuOccupancyMaxActiveBlocksPerMultiprocessor);
         get("cuGetErrorString", cuGetErrorString);
         get("cuFuncGetAttribute", cuFuncGetAttribute);
@@ -115,6 +117,7 @@ EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
     cg_opt.scan_single_pass = cfg.defaultGet<bool>("scan_single_pass", false);
     cg_opt.scan_windows = cfg.defaultGet<bool>("scan_windows", false);
     cg_opt.stage_bulk = cfg.defaultGet<bool>("stage_bulk", true);
+    pdl = cfg.defaultGet<bool>("pdl", true);
     cg_opt.scan_spin_cap = cfg.defaultGet<int64_t>("scan_spin_cap", int64_t{1} << 22);
     // The GPU reduces over the outermost axis natively, so sweeps may fuse with maps at rank 0.
     fusion_config = jitk::FusionConfig(cfg, false);
@@ -895,14 +898,39 @@ void EngineCUDA::launch_plain(const PlanUnit &pu, const vector<bh_base *> &bases
     void *e0 = nullptr;
     record_begin(rec, e0);
     busy_begin();
-    api->ck(api->cuLaunchKernel(reinterpret_cast<CUfunction>(pu.compiled->fn), static_cast<unsigned>(grid), 1, 1,
-                                kThreads, 1, 1, shared_bytes_of(pu.compiled->fn), static_cast<CUstream>(_stream), args,
-                                nullptr),
-            "cuLaunchKernel");
+    launch_dependent(pu.compiled->fn, grid, args, "cuLaunchKernel");
     busy_end();
     record_end(rec, e0);
     ++_stats.launches;
     if (u.sched == Sched::SERIAL) ++_stats.serial_units;
+}
+
+// A launch of the engine's own kernels on its stream with programmatic stream serialization (when
+// `pdl` is on): the kernel may start while the one before it finishes, and waits in
+// bh_grid_dependency() until that one's writes are visible.
+void EngineCUDA::launch_dependent(void *fn, int64_t grid, void **args, const char *what) {
+    const unsigned smem = static_cast<unsigned>(shared_bytes_of(fn));
+    if (!pdl) {
+        api->ck(api->cuLaunchKernel(reinterpret_cast<CUfunction>(fn), static_cast<unsigned>(grid), 1, 1, kThreads, 1, 1,
+                                    smem, static_cast<CUstream>(_stream), args, nullptr),
+                what);
+        return;
+    }
+    CUlaunchAttribute attr[1];
+    memset(attr, 0, sizeof(attr));
+    attr[0].id = CU_LAUNCH_ATTRIBUTE_PROGRAMMATIC_STREAM_SERIALIZATION;
+    attr[0].value.programmaticStreamSerializationAllowed = 1;
+    CUlaunchConfig cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDimX = static_cast<unsigned>(grid);
+    cfg.gridDimY = cfg.gridDimZ = 1;
+    cfg.blockDimX = kThreads;
+    cfg.blockDimY = cfg.blockDimZ = 1;
+    cfg.sharedMemBytes = smem;
+    cfg.hStream = static_cast<CUstream>(_stream);
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    api->ck(api->cuLaunchKernelEx(&cfg, reinterpret_cast<CUfunction>(fn), args, nullptr), what);
 }
 
 int EngineCUDA::launch_raw(void *fn, int64_t grid, void **args) {
@@ -1009,9 +1037,7 @@ void EngineCUDA::launch_batched(const vector<const PlanUnit *> &group, const vec
     void *e0 = nullptr;
     record_begin(rec, e0);
     busy_begin();
-    api->ck(api->cuLaunchKernel(reinterpret_cast<CUfunction>(proto.compiled->fn_batch), static_cast<unsigned>(grid),
-                                1, 1, kThreads, 1, 1, 0, static_cast<CUstream>(_stream), args, nullptr),
-            "cuLaunchKernel(batch)");
+    launch_dependent(proto.compiled->fn_batch, grid, args, "cuLaunchKernel(batch)");
     busy_end();
     record_end(rec, e0);
     ++_stats.launches;

@@ -331,6 +331,8 @@ private:
     void graph_launch(ReplayGraph &g);
     bool build_graph(Replay &r);
     int launch_raw(void *fn, int64_t grid, void **args); // cuLaunchKernel on the engine's stream
+    void launch_dependent(void *fn, int64_t grid, void **args, const char *what); // with PDL when `pdl`
+    bool pdl = true; // programmatic dependent launch of plain and grouped launches
     std::unordered_map<uint64_t, Replay> replays;
     bool replay_valid(const Replay &r) const;
 

@@ -31,12 +31,30 @@ def test_plain_chain_is_one_grid_reduction():
 
 
 def test_black_scholes_iteration_is_one_kernel():
+    """The whole iteration is one GRID_REDUCE launch: the mean (the sum divided by n, a
+    one-element map) runs in its tail, in the CTA that finishes last."""
     def prog(rt):
         S, K, T = (bh.empty(rt, (10000,), np.float64) for _ in range(3))
         return [W.black_scholes_iteration(rt, S, K, T, 0)]
     res, units = plan(prog)
     scheds = [u["sched"] for u in units]
-    assert scheds.count("grid_reduce") == 1 and len(units) <= 2, scheds
+    assert scheds == ["grid_reduce"] and units[0]["tail"], scheds
+    assert [k["folded_into"] for k in res["kernels"] if k["folded_into"] >= 0] == [0]
+
+
+def test_small_maps_run_in_the_producers_tail_and_large_ones_do_not():
+    """A map of at most 4096 elements that reads a reduction's result runs in the reduction
+    kernel's tail; a larger one keeps its own launch. Maps of every size share one kernel source."""
+    def prog(n):
+        def p(rt):
+            a = bh.empty(rt, (1 << 20,), np.float32)
+            b = bh.empty(rt, (n,), np.float32)
+            return [b * a.sum() + 1.0]
+        return p
+    _, small = plan(prog(4096))
+    _, large = plan(prog(4097))
+    assert [u["sched"] for u in small] == ["grid_reduce"] and small[0]["tail"], [u["sched"] for u in small]
+    assert [u["sched"] for u in large] == ["grid_reduce", "flat"], [u["sched"] for u in large]
 
 
 def test_heat_step_fuses_stencil_write_and_split_partial_max():

@@ -514,6 +514,25 @@ def test_scan1d_order_is_canonical(gpu_rt, n, dtype):
     assert np.asarray(got).tobytes() == want.tobytes()
 
 
+@pytest.mark.parametrize("n,dtype", [(1, np.float64), (1000, np.float32), (4096, np.float64), (4097, np.float32)])
+def test_small_maps_after_a_reduction_match_the_oracle(gpu_rt, oracle_rt, n, dtype):
+    """A map of at most 4096 elements that reads a reduction's result runs in the reduction
+    kernel's tail (one CTA, every work item); a larger one keeps its own launch. Both against the
+    oracle."""
+    a_host = np.random.default_rng(n).random(1 << 20).astype(dtype)
+    b_host = np.random.default_rng(n + 1).random(n).astype(dtype)
+
+    def prog(rt):
+        a, b = bh.array(rt, a_host), bh.array(rt, b_host)
+        s = a.sum()
+        return [s, b * s + dtype(1), bh.sqrt(b) - s / dtype(n)]
+    g, o = both(gpu_rt, oracle_rt, prog)
+    rtol = reduce_tol(dtype)
+    assert_close(g[0], o[0], rtol, rtol, "sum")
+    for x, y in zip(g[1:], o[1:]):
+        assert_close(x, y, rtol, rtol, "map")
+
+
 @pytest.mark.parametrize("name", ["ADD_ACCUMULATE", "MULTIPLY_ACCUMULATE"])
 def test_scan1d_windows_equal_the_whole_length_units(gpu_rt, monkeypatch, name):
     """With scan_windows on, units A and C run one group of chunks at a time (C repeating unit
