@@ -144,108 +144,101 @@ void add_instr_to_block(LoopB &block, InstrPtr instr, int rank, int64_t size_of_
 
 LoopB::LoopB(int r, int64_t s, vector<Block> block_list) : rank(r), size(s), _block_list(std::move(block_list)) {}
 
+namespace {
+// `f(loop)` for `loop` and then for every loop nested in it, depth first, in block-list order.
+template <typename L, typename F>
+void visit_loops(L &loop, F &&f) {
+    f(loop);
+    for (auto &b : loop._block_list)
+        if (!b.isInstr()) visit_loops(b.getLoop(), f);
+}
+} // namespace
+
 int LoopB::replaceInstr(const InstrPtr &subject, const bh_instruction &replacement) {
-    int ret = 0;
-    for (Block &b : _block_list) {
-        if (b.isInstr()) {
-            if (*b.getInstr() == *subject) {
+    int replaced = 0;
+    visit_loops(*this, [&](LoopB &l) {
+        for (Block &b : l._block_list)
+            if (b.isInstr() && *b.getInstr() == *subject) {
                 b.setInstr(replacement);
-                ++ret;
+                ++replaced;
             }
-        } else {
-            ret += b.getLoop().replaceInstr(subject, replacement);
-        }
-    }
-    return ret;
+    });
+    return replaced;
 }
 
 bool LoopB::isInnermost() const {
-    for (const Block &b : _block_list)
-        if (!b.isInstr()) return false;
-    return true;
+    return none_of(_block_list.begin(), _block_list.end(), [](const Block &b) { return !b.isInstr(); });
 }
 
 bool LoopB::isSystemOnly() const {
-    for (const Block &b : _block_list)
-        if (!b.isSystemOnly()) return false;
-    return true;
+    return all_of(_block_list.begin(), _block_list.end(), [](const Block &b) { return b.isSystemOnly(); });
 }
 
 void LoopB::getAllSubBlocks(vector<const LoopB *> &out) const {
-    for (const Block &b : _block_list) {
-        if (!b.isInstr()) {
-            out.push_back(&b.getLoop());
-            b.getLoop().getAllSubBlocks(out);
-        }
-    }
+    visit_loops(*this, [&](const LoopB &l) {
+        if (&l != this) out.push_back(&l);
+    });
 }
 
 vector<const LoopB *> LoopB::getLocalSubBlocks() const {
-    vector<const LoopB *> ret;
+    vector<const LoopB *> children;
     for (const Block &b : _block_list)
-        if (!b.isInstr()) ret.push_back(&b.getLoop());
-    return ret;
+        if (!b.isInstr()) children.push_back(&b.getLoop());
+    return children;
 }
 
 set<const bh_base *> LoopB::getAllBases() const {
-    set<const bh_base *> ret;
+    set<const bh_base *> bases;
     for (const InstrPtr &instr : all_instr(*this))
-        for (const bh_base *b : instr_bases(*instr)) ret.insert(b);
-    return ret;
+        for (const bh_view &v : instr->getViews()) bases.insert(v.base);
+    return bases;
 }
 
 void LoopB::getAllNews(set<bh_base *> &out) const {
-    out.insert(_news.begin(), _news.end());
-    for (const Block &b : _block_list)
-        if (!b.isInstr()) b.getLoop().getAllNews(out);
+    visit_loops(*this, [&](const LoopB &l) { out.insert(l._news.begin(), l._news.end()); });
 }
 set<bh_base *> LoopB::getAllNews() const {
-    set<bh_base *> ret;
-    getAllNews(ret);
-    return ret;
+    set<bh_base *> news;
+    getAllNews(news);
+    return news;
 }
 void LoopB::getAllFrees(set<bh_base *> &out) const {
-    out.insert(_frees.begin(), _frees.end());
-    for (const Block &b : _block_list)
-        if (!b.isInstr()) b.getLoop().getAllFrees(out);
+    visit_loops(*this, [&](const LoopB &l) { out.insert(l._frees.begin(), l._frees.end()); });
 }
 set<bh_base *> LoopB::getAllFrees() const {
-    set<bh_base *> ret;
-    getAllFrees(ret);
-    return ret;
+    set<bh_base *> frees;
+    getAllFrees(frees);
+    return frees;
 }
 
-// A temporary of this loop is created here and freed here or below, or freed here and created
-// below (core/jitk/block.cpp:174-181 of the reference).
+// A temporary of this loop is created here and freed here or in a nested loop, or freed here and
+// created here or in a nested loop (the reference's rule, core/jitk/block.cpp:174-181).
 void LoopB::getLocalTemps(set<bh_base *> &out) const {
-    const set<bh_base *> frees = getAllFrees();
-    set_intersection(_news.begin(), _news.end(), frees.begin(), frees.end(), inserter(out, out.begin()));
-    const set<bh_base *> news = getAllNews();
-    set_intersection(_frees.begin(), _frees.end(), news.begin(), news.end(), inserter(out, out.begin()));
+    const set<bh_base *> frees_below = getAllFrees(), news_below = getAllNews();
+    for (bh_base *b : _news)
+        if (frees_below.count(b)) out.insert(b);
+    for (bh_base *b : _frees)
+        if (news_below.count(b)) out.insert(b);
 }
 set<bh_base *> LoopB::getLocalTemps() const {
-    set<bh_base *> ret;
-    getLocalTemps(ret);
-    return ret;
+    set<bh_base *> temps;
+    getLocalTemps(temps);
+    return temps;
 }
 void LoopB::getAllTemps(set<bh_base *> &out) const {
-    getLocalTemps(out);
-    for (const Block &b : _block_list)
-        if (!b.isInstr()) b.getLoop().getAllTemps(out);
+    visit_loops(*this, [&](const LoopB &l) { l.getLocalTemps(out); });
 }
 set<bh_base *> LoopB::getAllTemps() const {
-    set<bh_base *> ret;
-    getAllTemps(ret);
-    return ret;
+    set<bh_base *> temps;
+    getAllTemps(temps);
+    return temps;
 }
 set<bh_base *> LoopB::getAllNonTemps() const {
     const set<bh_base *> temps = getAllTemps();
-    set<bh_base *> ret;
-    for (const bh_base *t : getAllBases()) {
-        bh_base *b = const_cast<bh_base *>(t);
-        if (!contains(temps, b)) ret.insert(b);
-    }
-    return ret;
+    set<bh_base *> rest;
+    for (const bh_base *b : getAllBases())
+        if (!temps.count(const_cast<bh_base *>(b))) rest.insert(const_cast<bh_base *>(b));
+    return rest;
 }
 
 bool LoopB::validation() const {
