@@ -1505,8 +1505,10 @@ void emit_flat_vector(Symbols &sym, ostream &body, const CodegenOptions &opt, co
     body << "    }\n";
 }
 
-// Elements of a map small enough to run in another kernel's tail.
-constexpr int64_t kFlatTailElements = 4096;
+// Elements of a map small enough to run in another kernel's tail: a few values computed from a
+// reduction's result, such as a mean. (Maps of up to 4096 elements there made small flushes of the
+// learned-fuser workload slower: one CTA after the producer's last one is a serial step.)
+constexpr int64_t kFlatTailElements = 32;
 
 LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) {
     LaunchUnit u;
@@ -1548,7 +1550,7 @@ LaunchUnit lower_flat(const LoopB &loop, unsigned P, const CodegenOptions &opt) 
         u.V > 1 && !(heavy_body(inner) && !opt.preload_heavy) ? preloadable_views(inner, L, sym) : vector<bh_view>{};
     const string n_inner = "p.n" + to_string(sym.loop_id.at(&inner));
     const string iv = "i" + to_string(P - 1);
-    // A small map (at most kFlatTailElements elements) can also run in the tail of the kernel
+    // A tiny map (at most kFlatTailElements elements) can also run in the tail of the kernel
     // before it, by the CTA that finishes that kernel last (fuse_tails): one CTA runs every work
     // item in turn. Elementwise results do not depend on which thread computes them. (bh_tail is
     // in every map's source, so that maps of every size share one compiled kernel.)

@@ -43,16 +43,16 @@ def test_black_scholes_iteration_is_one_kernel():
 
 
 def test_small_maps_run_in_the_producers_tail_and_large_ones_do_not():
-    """A map of at most 4096 elements that reads a reduction's result runs in the reduction
-    kernel's tail; a larger one keeps its own launch. Maps of every size share one kernel source."""
+    """A map of at most 32 elements that reads a reduction's result runs in the reduction kernel's
+    tail; a larger one keeps its own launch. Maps of every size share one kernel source."""
     def prog(n):
         def p(rt):
             a = bh.empty(rt, (1 << 20,), np.float32)
             b = bh.empty(rt, (n,), np.float32)
             return [b * a.sum() + 1.0]
         return p
-    _, small = plan(prog(4096))
-    _, large = plan(prog(4097))
+    _, small = plan(prog(32))
+    _, large = plan(prog(33))
     assert [u["sched"] for u in small] == ["grid_reduce"] and small[0]["tail"], [u["sched"] for u in small]
     assert [u["sched"] for u in large] == ["grid_reduce", "flat"], [u["sched"] for u in large]
 

@@ -514,11 +514,10 @@ def test_scan1d_order_is_canonical(gpu_rt, n, dtype):
     assert np.asarray(got).tobytes() == want.tobytes()
 
 
-@pytest.mark.parametrize("n,dtype", [(1, np.float64), (1000, np.float32), (4096, np.float64), (4097, np.float32)])
+@pytest.mark.parametrize("n,dtype", [(1, np.float64), (32, np.float32), (33, np.float64), (4097, np.float32)])
 def test_small_maps_after_a_reduction_match_the_oracle(gpu_rt, oracle_rt, n, dtype):
-    """A map of at most 4096 elements that reads a reduction's result runs in the reduction
-    kernel's tail (one CTA, every work item); a larger one keeps its own launch. Both against the
-    oracle."""
+    """A map of at most 32 elements that reads a reduction's result runs in the reduction kernel's
+    tail (one CTA); a larger one keeps its own launch. Both against the oracle."""
     a_host = np.random.default_rng(n).random(1 << 20).astype(dtype)
     b_host = np.random.default_rng(n + 1).random(n).astype(dtype)
 
