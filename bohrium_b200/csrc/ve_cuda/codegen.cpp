@@ -3243,12 +3243,57 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
             pl.add(fc, "unsigned int*", "counter");
             u.scan_gate = true;
         }
+        // Prefetch (scan_prefetch): the streaming units read their unit-stride read-only inputs
+        // from a two-slot shared-memory ring per CTA, each full chunk filled by TMA bulk copies
+        // (one thread, one mbarrier per slot, bounded waits) while the CTA works on the chunk before.
+        vector<bh_view> pfv;
+        vector<int64_t> pf_off;
+        int64_t pf_bytes = 0;
+        if (phase != 1 && opt.scan_prefetch && !opt.bounds_check) {
+            vector<bh_view> cand = preloadable_views(L, L, sym);
+            const bh_view &in = acc->operand[1];
+            bool in_written = false;
+            for (const InstrPtr &i : jitk::all_instr(L))
+                if (!i->operand.empty() && !i->operand[0].isConstant() && i->operand[0].base == in.base) in_written = true;
+            if (!in.isConstant() && !sym.temps.count(in.base) && !in_written &&
+                find_if(cand.begin(), cand.end(), [&](const bh_view &v) { return v == in; }) == cand.end())
+                cand.push_back(in);
+            for (const bh_view &v : cand) {
+                if (!unit_stride_view(v, 0, sym)) continue;
+                pfv.push_back(v);
+                pf_off.push_back(pf_bytes);
+                pf_bytes += 2 * kScanTile * static_cast<int64_t>(bh_type_size(v.base->dtype()));
+            }
+            if (pf_bytes > 64 * 1024) {
+                pfv.clear();
+                pf_off.clear();
+                pf_bytes = 0;
+            }
+        }
+        const bool pf = !pfv.empty();
+        if (pf) {
+            ParamField fok{ParamField::TMA_OK};  // bulk copies allowed (not in grouped launches)
+            pl.add(fok, "bh_i64", "tma_ok");
+            ParamField ferr{ParamField::SCRATCH};
+            ferr.i64 = -1;  // the engine's error record
+            pl.add(ferr, "unsigned long long*", "err");
+        }
         stringstream body;
         Emitter em(sym, body, opt);
         body << block_scan_fn(T, "bh_block_scan", rop, ident);
-        body << "__device__ void bh_work(const P &p, bh_i64 w) {\n";
+        if (pf) {
+            body << "// bh_dynamic_shared_bytes: " << pf_bytes << "\n";
+            body << "__device__ void bh_work_x(const P &p, bh_i64 w, int slot, const unsigned char *ring) {\n";
+        } else {
+            body << "__device__ void bh_work(const P &p, bh_i64 w) {\n";
+        }
         body << "    const bh_i64 c = p.first + w;\n";
         body << pointer_locals(sym);
+        for (size_t k = 0; k < pfv.size(); ++k) {
+            const string Tv = cuda_type(pfv[k].base->dtype());
+            body << "    const " << Tv << "* rv" << k << " = (const " << Tv << "*)(ring + " << pf_off[k] << " + slot * "
+                 << kScanTile * static_cast<int64_t>(bh_type_size(pfv[k].base->dtype())) << ");\n";
+        }
         body << "    __shared__ " << T << " sm[" << 2 * (kThreads / 32) + 1 << "];\n";
         body << "    " << T << "* totals = (" << T << "*)p.scratch;\n";
         body << "    " << T << "* carries = totals + p.nchunks;\n";
@@ -3318,8 +3363,10 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
             // q + q/8, so the per-thread reads of 8 consecutive elements below hit distinct banks.
             body << "    __shared__ " << T << " stage[" << kScanTile + kScanTile / kScanPerThread << "];\n";
             body << "    const bh_i64 cbase = c * " << kScanTile << ";\n";
-            auto stage_pass = [&](bool with_inputs, const string &what) {
+            auto stage_pass_one = [&](bool with_inputs, const string &what, bool from_ring) {
                 Scope scope;
+                if (from_ring)
+                    for (size_t k = 0; k < pfv.size(); ++k) scope.repl[ViewKey(pfv[k])] = "rv" + to_string(k) + "[q]";
                 body << "#pragma unroll\n";
                 body << "    for (int k = 0; k < " << kScanPerThread << "; ++k) {\n";
                 body << "        const int q = k * " << kThreads << " + (int)threadIdx.x;\n";
@@ -3356,6 +3403,18 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
                 body << "        }\n";
                 body << "    }\n";
             };
+            // With the ring, a full chunk (slot >= 0) reads the prefetched inputs from it.
+            auto stage_pass = [&](bool with_inputs, const string &what) {
+                if (!pf) {
+                    stage_pass_one(with_inputs, what, false);
+                    return;
+                }
+                body << "    if (slot >= 0) {\n";
+                stage_pass_one(with_inputs, what, true);
+                body << "    } else {\n";
+                stage_pass_one(with_inputs, what, false);
+                body << "    }\n";
+            };
             stage_pass(true, "in");
             body << "    __syncthreads();\n";
             // Thread t folds elements 8t..8t+7 of the chunk in order. The re-scan keeps them in
@@ -3372,9 +3431,92 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
             // The block scan's first barrier orders these stage reads before any later stage write.
             body << "    " << T << " total;\n";
             body << "    const " << T << " e = bh_block_scan(s, total, sm);\n";
+            // The kernel wrappers: with the ring, bh_main runs the prefetch walk.
+            auto wrappers = [&]() -> string {
+                if (!pf) return kWrappers;
+                stringstream ws;
+                ws << "__device__ __forceinline__ void bh_work(const P &p, bh_i64 w) { bh_work_x(p, w, -1, nullptr); }\n";
+                ws << "__device__ __forceinline__ bool bh_pf_full(const P &p, bh_i64 w) { return (p.first + w + 1) * "
+                   << kScanTile << " <= " << n0 << "; }\n";
+                ws << "__device__ __forceinline__ bool bh_pf_ok(const P &p) {\n";
+                ws << pointer_locals(sym);
+                ws << "    const bh_i64 i0 = 0;\n";
+                ws << "    bool ok = p.tma_ok != 0;\n";
+                for (const bh_view &v : pfv) ws << "    ok = ok && (((unsigned long long)&" << em.array_ref(v) << ") & 15ull) == 0;\n";
+                ws << "    return ok;\n";
+                ws << "}\n";
+                ws << "__device__ __forceinline__ void bh_pf_issue(const P &p, bh_i64 w, int slot, unsigned char *ring, "
+                      "unsigned long long *bar) {\n";
+                ws << pointer_locals(sym);
+                int64_t chunk_bytes = 0;
+                for (const bh_view &v : pfv) chunk_bytes += kScanTile * static_cast<int64_t>(bh_type_size(v.base->dtype()));
+                ws << "    const bh_i64 i0 = (p.first + w) * " << kScanTile << ";\n";
+                ws << "    bh_mbar_expect_tx(bar, " << chunk_bytes << "u);\n";
+                for (size_t k = 0; k < pfv.size(); ++k) {
+                    const int64_t vb = kScanTile * static_cast<int64_t>(bh_type_size(pfv[k].base->dtype()));
+                    ws << "    bh_bulk_row(ring + " << pf_off[k] << " + slot * " << vb << ", &" << em.array_ref(pfv[k]) << ", "
+                       << vb << "u, bar);\n";
+                }
+                ws << "}\n";
+                ws << R"CUDA(__device__ void bh_main(const P &p) {
+    extern __shared__ __align__(16) unsigned char bh_dyn[];
+    if (!bh_pf_ok(p)) {
+        for (bh_i64 w = blockIdx.x; w < p.work; w += gridDim.x) bh_work(p, w);
+        return;
+    }
+    // Item i of this CTA is work item blockIdx.x + i * gridDim.x; its chunk (when full) is the
+    // (i / 2)-th copy into slot i % 2.
+    __shared__ alignas(8) unsigned long long pf_bar[2];
+    __shared__ int pf_fail;
+    if (threadIdx.x == 0) {
+        bh_mbar_init(&pf_bar[0], 1u);
+        bh_mbar_init(&pf_bar[1], 1u);
+        bh_mbar_fence_init();
+        pf_fail = 0;
+    }
+    __syncthreads();
+    const bh_i64 step = gridDim.x;
+    bh_i64 issued = 0, waited = 0;  // items [0, issued) copied, [0, waited) arrived (thread 0)
+    if (threadIdx.x == 0) {
+        for (; issued < 2; ++issued) {
+            const bh_i64 w = blockIdx.x + issued * step;
+            if (w >= p.work || !bh_pf_full(p, w)) break;
+            bh_pf_issue(p, w, (int)issued, bh_dyn, &pf_bar[issued]);
+        }
+    }
+    for (bh_i64 i = 0;; ++i) {
+        const bh_i64 w = blockIdx.x + i * step;
+        if (w >= p.work) break;
+        const int slot = (int)(i & 1);
+        const bool full = bh_pf_full(p, w);
+        if (full) {
+            if (!bh_mbar_wait(&pf_bar[slot], (unsigned)((i >> 1) & 1))) pf_fail = 1;
+            else if (threadIdx.x == 0) waited = i + 1;
+        }
+        __syncthreads();
+        if (pf_fail) break;
+        bh_work_x(p, w, full ? slot : -1, bh_dyn);
+        __syncthreads();  // every thread is done with the slot
+        const bh_i64 wn = w + 2 * step;
+        if (threadIdx.x == 0 && full && wn < p.work && bh_pf_full(p, wn)) {
+            bh_pf_issue(p, wn, slot, bh_dyn, &pf_bar[slot]);
+            issued = i + 3;
+        }
+    }
+    if (pf_fail && threadIdx.x == 0) {
+        // A chunk copy never completed: record it, and let the copies still in flight into the
+        // ring land (bounded) before the CTA leaves.
+        atomicCAS(p.err, 0ull, 0xC000000000000000ull | (unsigned long long)blockIdx.x);
+        for (bh_i64 j = waited; j < issued; ++j) bh_mbar_wait(&pf_bar[j & 1], (unsigned)((j >> 1) & 1));
+    }
+}
+)CUDA";
+                ws << kBatchWork << kKernels;
+                return ws.str();
+            };
             if (phase == 0) {
                 body << "    if (threadIdx.x == 0) totals[c] = total;\n";
-                body << "}\n" << kWrappers;
+                body << "}\n" << wrappers();
             } else {
                 if (!windowed) {
                     body << "    const " << T << "* grun = carries + p.nchunks + (p.nchunks + " << kScanTile - 1 << ") / "
@@ -3448,7 +3590,7 @@ vector<LaunchUnit> lower_scan1d(const LoopB &loop, const InstrPtr &acc, const Co
                 stage_pass(reread, "out");
                 // Stage reads of this work item before the next item's pass 1 writes.
                 body << "    __syncthreads();\n";
-                body << "}\n" << kWrappers;
+                body << "}\n" << wrappers();
             }
         }
         u.fields = pl.fields;

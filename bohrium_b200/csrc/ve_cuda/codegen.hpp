@@ -157,6 +157,7 @@ struct CodegenOptions {
     bool scan_single_pass = false; // SCAN1D as one pass with look-back (else three units; see lower_scan1d_single)
     bool scan_windows = false;     // SCAN1D units A and C one group of chunks at a time (see lower_scan1d)
     bool stage_bulk = true;        // LANE_REDUCE stencil rows staged by TMA bulk copies (else cp.async)
+    bool scan_prefetch = true;     // SCAN1D streaming units read their inputs from a TMA-filled ring
     int64_t scan_spin_cap = int64_t{1} << 22; // polls per look-back wait (negative: give up at once)
 };
 

@@ -110,6 +110,7 @@ extern "C" const char *bh_ve_cuda_dry_run(bhb_ir *handle, int compile, const cha
         if (const char *v = getenv("BH_CUDA_SCAN_SINGLE_PASS")) opt.scan_single_pass = string(v) == "true" || string(v) == "1";
         if (const char *v = getenv("BH_CUDA_SCAN_WINDOWS")) opt.scan_windows = string(v) == "true" || string(v) == "1";
         if (const char *v = getenv("BH_CUDA_STAGE_BULK")) opt.stage_bulk = string(v) == "true" || string(v) == "1";
+        if (const char *v = getenv("BH_CUDA_SCAN_PREFETCH")) opt.scan_prefetch = string(v) == "true" || string(v) == "1";
         vector<vector<cuda::LaunchUnit>> lowered(kernels.size());
         for (size_t k = 0; k < kernels.size(); ++k)
             if (!kernels[k].isSystemOnly()) lowered[k] = cuda::lower_kernel(kernels[k], opt);

@@ -117,6 +117,7 @@ EngineCUDA::EngineCUDA(component::ComponentVE &c) : comp(c) {
     cg_opt.scan_single_pass = cfg.defaultGet<bool>("scan_single_pass", false);
     cg_opt.scan_windows = cfg.defaultGet<bool>("scan_windows", false);
     cg_opt.stage_bulk = cfg.defaultGet<bool>("stage_bulk", true);
+    cg_opt.scan_prefetch = cfg.defaultGet<bool>("scan_prefetch", true);
     pdl = cfg.defaultGet<bool>("pdl", true);
     cg_opt.scan_spin_cap = cfg.defaultGet<int64_t>("scan_spin_cap", int64_t{1} << 22);
     // The GPU reduces over the outermost axis natively, so sweeps may fuse with maps at rank 0.

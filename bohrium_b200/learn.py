@@ -117,6 +117,9 @@ def evaluate(ex, seeds, model_path: str, max_elems: float = 1e8, reps: int = 5):
     learned (the learned plan where it is bit-identical and measured faster) -- with the outputs
     of all three compared bit for bit."""
     rows = []
+    # The autotuner stays off while the three engines are timed: tuning launches (variants timed
+    # on a kernel's first launches) would otherwise fall into whichever engine runs a kernel first.
+    ex.message("CUDA: autotune off")
     for seed in seeds:
         rt, dag, outs, shape = build(ex, seed, max_elems)
         times, results = {}, {}
@@ -143,6 +146,7 @@ def evaluate(ex, seeds, model_path: str, max_elems: float = 1e8, reps: int = 5):
                      "tried": stats1.get("learned_trials", 0) - stats0.get("learned_trials", 0)})
         del dag, outs, rt
     _set_fusion(ex, "lossy", GREEDY)
+    ex.message("CUDA: autotune on")
     return rows
 
 

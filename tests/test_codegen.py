@@ -229,6 +229,29 @@ def test_scan_units_stage_elements_at_coalesced_positions(dtype):
         assert "= stage[q + (q >> 3)];" in units[2]["source"]
 
 
+def test_scan_units_prefetch_their_inputs_through_a_tma_ring(monkeypatch):
+    """Units A and C read their unit-stride read-only inputs (the accumulate's own input, or the
+    array a fused input is computed from) from a two-slot shared-memory ring filled by TMA bulk
+    copies one chunk ahead; unit B has none. With scan_prefetch off, no unit has the ring."""
+    def direct(rt):
+        y = bh.empty(rt, (1_000_000,), np.float64)
+        return [bh.accumulate("ADD_ACCUMULATE", y, 0)]
+
+    def fused(rt):
+        x = bh.empty(rt, (1_000_000,), np.float32)
+        return [bh.accumulate("ADD_ACCUMULATE", x * np.float32(2), 0)]
+    for prog in (direct, fused):
+        _, units = plan(prog)
+        assert [u["sched"] for u in units] == ["scan1d"] * 3, [u["sched"] for u in units]
+        for k, u in enumerate(units):
+            ring = "bh_pf_issue" in u["source"] and "bh_bulk_row(ring" in u["source"]
+            assert ring == (k != 1), (prog.__name__, k, ring)
+    monkeypatch.setenv("BH_CUDA_SCAN_PREFETCH", "false")
+    for prog in (direct, fused):
+        _, units = plan(prog)
+        assert all("bh_pf_issue" not in u["source"] for u in units)
+
+
 def test_scan_windows_are_groups_of_chunks_sharing_two_kernels(monkeypatch):
     """A scan over 2.5 groups of chunks (2048 chunks of 2048 elements each) is units A and C for
     each group in turn: the same two compiled kernels, with the group's first chunk and chunk
