@@ -609,15 +609,18 @@ def extra_learned(bh, W, ex, rt, out, train_seeds=24, eval_seeds=12, holdout_see
     finally:
         os.unlink(path)
     res = learn.summary(rows)
-    # Inference: the learned contraction's host time (batched GPU predictions included) per plan
-    # it built, and per predicted merge candidate.
+    # Inference: the cost model's share of building the learned plans (block features, GPU
+    # inference, merge choice) per plan and per predicted block; and the whole learned plan
+    # building (contraction, lowering, NVRTC compilation of new kernels) per plan.
     preds = s1.get("learned_predictions", 0) - s0.get("learned_predictions", 0)
     fusion_s = s1.get("time_learned_fusion", 0) - s0.get("time_learned_fusion", 0)
+    choose_s = s1.get("time_learned_choose", 0) - s0.get("time_learned_choose", 0)
     plans = s1.get("learned_trials", 0) + s1.get("learned_same_plan", 0) + s1.get("learned_order_differs", 0) - (
         s0.get("learned_trials", 0) + s0.get("learned_same_plan", 0) + s0.get("learned_order_differs", 0))
     res["inference"] = {"predictions": int(preds), "plans": int(plans),
-                        "ms_per_plan": round(fusion_s * 1e3 / plans, 3) if plans else None,
-                        "us_per_prediction": round(fusion_s * 1e6 / preds, 3) if preds else None}
+                        "model_ms_per_plan": round(choose_s * 1e3 / plans, 3) if plans else None,
+                        "model_us_per_prediction": round(choose_s * 1e6 / preds, 3) if preds else None,
+                        "plan_build_ms_per_plan": round(fusion_s * 1e3 / plans, 3) if plans else None}
     res.update({"records": int(X.shape[0]), "train_loss": round(loss, 4), "holdout": holdout,
                 "collect_s": round(t1 - t0, 1),
                 "train_s": round(train_s, 2), "eval_s": round(time.perf_counter() - t2, 1),

@@ -1817,7 +1817,8 @@ string EngineCUDA::statistics() const {
        << "\nlearned_kept: " << _stats.learned_kept << "\ngreedy_kept: " << _stats.greedy_kept
        << "\nlearned_same_plan: " << _stats.learned_same << "\nlearned_order_differs: " << _stats.learned_order_differs
        << "\nlearned_predictions: " << _stats.learned_predictions
-       << "\ntime_learned_fusion: " << _stats.time_learned_fusion << "\nrecords: " << record_count() << "\n";
+       << "\ntime_learned_fusion: " << _stats.time_learned_fusion
+       << "\ntime_learned_choose: " << _stats.time_learned_choose << "\nrecords: " << record_count() << "\n";
     if (!_stats.records.empty()) {
         ss << "units:\n";
         for (const UnitRecord &r : _stats.records)

@@ -56,7 +56,8 @@ struct Stats {
     uint64_t learned_predictions = 0;
     uint64_t parallel_compiles = 0; // sources compiled ahead in parallel
     uint64_t tuned_kernels = 0, tuned_capped = 0, tune_launches = 0;
-    double time_learned_fusion = 0;
+    double time_learned_fusion = 0; // learned plans: contraction, lowering and compilation
+    double time_learned_choose = 0; // of which the cost model's merge choices (features + inference)
     double time_fusion = 0, time_codegen = 0, time_compile = 0, time_exec_host = 0;
     double time_prepare = 0, time_launch = 0; // host time: list clean-up + hashing, plan execution
     std::vector<UnitRecord> records; // filled when profiling

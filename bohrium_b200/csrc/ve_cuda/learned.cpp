@@ -168,6 +168,12 @@ void EngineCUDA::predict_us(const vector<CostFeatures> &rows, vector<float> &out
 
 int EngineCUDA::choose_merge(const vector<pair<const Block *, const Block *>> &cands) {
     if (cands.empty() || cm == nullptr) return -1;
+    const auto t0 = chrono::steady_clock::now();
+    struct Timer {  // the model's share of the learned contraction: features, inference, choice
+        double &acc;
+        chrono::steady_clock::time_point t0;
+        ~Timer() { acc += chrono::duration<double>(chrono::steady_clock::now() - t0).count(); }
+    } timer{_stats.time_learned_choose, t0};
     // Keys of every block involved and of every merged pair; predict what is not cached yet.
     vector<uint64_t> ka(cands.size()), kb(cands.size()), km(cands.size());
     vector<CostFeatures> rows;
