@@ -398,7 +398,7 @@ __device__ __forceinline__ bool bh_mbar_wait(unsigned long long *bar, unsigned p
     return false;
 }
 // One contiguous global -> shared copy by the TMA engine (16-byte aligned addresses, a multiple
-// of 16 bytes), counted on `bar`; no cluster multicast.
+// of 16 bytes), counted on `bar`; the copy lands in this CTA's shared memory only.
 __device__ __forceinline__ void bh_bulk_row(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  :: "r"(bh_saddr(dst)), "l"(src), "r"(bytes), "r"(bh_saddr(bar)) : "memory");

@@ -382,3 +382,29 @@ def test_untransposed_and_complex_maps_stay_flat():
         return [a + a, z.T * z.T]
     res, units = plan(prog)
     assert [u["sched"] for u in units] == ["flat", "flat"]
+
+
+def test_generated_tma_copies_land_in_the_issuing_cta_only():
+    """Every TMA copy the engine generates (TILE2D tiles, staged stencil rows, the scan's prefetch
+    ring) reads this GPU's own memory into the issuing CTA's shared memory: no source copies to
+    several CTAs of a cluster, and none is launched with a cluster shape."""
+    def transpose(rt):
+        a, b = bh.empty(rt, (1024, 1024), np.float32), bh.empty(rt, (1024, 1024), np.float32)
+        return [a + b.T]
+
+    def heat(rt):
+        a, b = bh.empty(rt, (512, 512), np.float32), bh.empty(rt, (512, 512), np.float32)
+        return [W.heat_step(a, b), b]
+
+    def scan(rt):
+        x = bh.empty(rt, (1_000_000,), np.float64)
+        return [bh.accumulate("ADD_ACCUMULATE", x * 2.0, 0)]
+    sources = []
+    for prog in (transpose, heat, scan):
+        _, units = plan(prog)
+        sources += [u["source"] for u in units]
+    assert any("cp.async.bulk.tensor" in src for src in sources)
+    assert any("cp.async.bulk.shared" in src for src in sources)
+    to_cluster = "multi" + "cast"  # the qualifier of a copy to several CTAs
+    for src in sources:
+        assert to_cluster not in src and "__cluster_dims__" not in src
