@@ -1,11 +1,12 @@
 """The learned engine against the greedy fuser it steers (core/jitk/graph.cpp:319-365, the
 reference's greedy contraction), on held-out DAGs of the learned-fuser workload. The model is
 trained here on this engine's own timings of other DAGs. The learned engine builds a learned plan
-for every DAG (the model predicts the merges), times it against the greedy plan and keeps it only when it is faster (by at least
-3 %), so over the held-out set it is never slower than greedy batching (within timing noise),
-any plan it keeps is faster there, and its outputs equal the greedy plan's bit for bit. (How much
-it gains is measured by bench.py's learned_fuser_random_dags, with a larger training set; a
-model trained on eight small DAGs, as here, keeps few or no learned plans.)"""
+for every DAG (the model predicts the merges), times it against the greedy plan and keeps it
+only when it is faster (by at least 3 %), so over the held-out set it is never slower than greedy
+batching (within timing noise), any plan it keeps is faster there, and its outputs equal the
+greedy plan's bit for bit. (How much it gains is measured by bench.py's
+learned_fuser_random_dags, with a larger training set; a model trained on eight small DAGs, as
+here, keeps few or no learned plans.)"""
 import numpy as np
 import pytest
 
