@@ -8,8 +8,8 @@ throughput of the flushes with the inputs resident in device memory (bytes of S,
 flush plus the result written, over the device time of the timed steps). `e2e` is the same metric
 through the C ABI with the inputs handed over from page-locked host buffers every step and the 10
 mean prices read back. `cpu_baseline` is the oracle (the restated ve/openmp engine) on the host
-cores. `extra` adds the other workloads: the plain chain, the 2-D heat stencil and the batching
-workload in its plain and grouped forms.
+cores. `extra` adds the other workloads (plain chain, heat stencil, batching, streaming block,
+axpy, transpose-add, scan, learned fuser); they are single-GPU measurements and run at N = 1 only.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--no-extra]
 
@@ -328,7 +328,9 @@ def run_ours(args, world, rank, local):
     del sets
 
     extra = {}
-    if args.extra and rank == 0:
+    # The other workloads are single-GPU measurements: they run at N = 1 only (under torchrun the
+    # other ranks would wait for rank 0 at the final barrier for the whole of them).
+    if args.extra and rank == 0 and world == 1:
         extra = run_extra(bh, W, ex, rt, peak, heat_n=args.heat_n, learned_train=args.learned_train,
                           learned_eval=args.learned_eval, learned_holdout=args.learned_holdout)
 
