@@ -408,3 +408,28 @@ def test_generated_tma_copies_land_in_the_issuing_cta_only():
     to_cluster = "multi" + "cast"  # the qualifier of a copy to several CTAs
     for src in sources:
         assert to_cluster not in src and "__cluster_dims__" not in src
+
+
+def test_small_light_grid_reductions_hold_one_variant_per_launch_mode():
+    """A light grid reduction over at most 64 tiles takes 1 tile per work item in a plain launch
+    and 4 in a grouped one: its source holds the device code for both (bh_work for plain
+    launches, bh_batch_work for grouped ones). Heavy or large reductions have one variant."""
+    from bohrium_b200 import workloads as W
+
+    def small(rt):
+        x = bh.empty(rt, (30000,), np.float32)
+        y = W.batching_chain(x)
+        return [y, y.sum(), y.max()]
+
+    def large(rt):
+        x = bh.empty(rt, (1 << 24,), np.float32)
+        y = W.batching_chain(x)
+        return [y, y.sum(), y.max()]
+    _, units = plan(small)
+    src = units[0]["source"]
+    assert "namespace bh_kp" in src and "namespace bh_kg" in src
+    assert "const bh_i64 tile0 = w * 1;" in src and "const bh_i64 tile0 = w * 4;" in src
+    assert "void bh_batch_work(const P &p, bh_i64 w) { bh_kg::bh_work(p, w); }" in src
+    assert units[0]["work"] == 15  # plain work items: one tile each
+    _, units = plan(large)
+    assert "namespace bh_kg" not in units[0]["source"]
